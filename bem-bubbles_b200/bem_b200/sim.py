@@ -1,0 +1,208 @@
+"""Host-side mirror of the reference's simulation interface, over the C ABI.
+
+``ColocSim`` follows Bem::ColocSim / Bem::LinLinSim / Bem::Simulation
+(Bem/Simulation/ColocSim.hpp:13-28, LinLinSim.hpp:19-90, Simulation.hpp:26-210): same method
+names, argument meaning and error behaviour (a vertex with x < 0 at an RK4 step raises, as the
+reference's ``std::out_of_range`` from ``test_negative`` does).  The state lives in GPU memory;
+every call crosses the C ABI with host arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _d(a):
+    return a.ctypes.data_as(L._D)
+
+
+class ColocSim:
+    """Collocation BEM simulation of gas/vapour bubbles on one GPU.
+
+    verts: (N,3) float64, trigs: (M,3) int; p_inf, epsilon, sigma, gamma as in the reference
+    constructor (Simulation.hpp:29).  ``pressurefield`` is either None (the reference's
+    default_field, 0), a tuple ``(amp, omega, phase[, kx])`` for amp*sin(kx*x + omega*t + phase)
+    evaluated on the device, or a Python callable f(x: ndarray(3), t: float) -> float evaluated
+    on the host for every vertex at every stage.
+    """
+
+    def __init__(self, verts, trigs, p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.0, pressurefield=None,
+                 device=0, solver="bicgstab", mirror=False):
+        self._L = L.load()
+        self._h = C.c_void_p()
+        p = L.Params()
+        self._L.bem_default_params(C.byref(p))
+        p.p_inf, p.epsilon, p.sigma, p.gamma = float(p_inf), float(epsilon), float(sigma), float(gamma)
+        p.mirror = int(bool(mirror))
+        p.solver = {"bicgstab": L.SOLVER_BICGSTAB, "lu": L.SOLVER_LU, "mixed": L.SOLVER_MIXED}[solver]
+        self._cb = None
+        if pressurefield is not None and not callable(pressurefield):
+            amp, omega, phase = pressurefield[:3]
+            kx = pressurefield[3] if len(pressurefield) > 3 else 0.0
+            p.field_amp, p.field_omega, p.field_phase, p.field_kx = float(amp), float(omega), float(phase), float(kx)
+        rc = self._L.bem_create(C.byref(self._h), int(device), C.byref(p))
+        if rc != L.BEM_OK:
+            raise L.BemError(rc, "bem_create failed (no CUDA device?)")
+        v = np.ascontiguousarray(verts, dtype=np.float64)
+        t = np.ascontiguousarray(trigs, dtype=np.int64)
+        self.N, self.M = len(v), len(t)
+        self._check(self._L.bem_set_mesh(self._h, self.N, _d(v), self.M, t.ctypes.data_as(L._I64)))
+        if callable(pressurefield):
+            fn = pressurefield
+
+            def _cb(xp, tt, user):
+                return float(fn(np.array([xp[0], xp[1], xp[2]]), tt))
+
+            self._cb = L.FIELD_FN(_cb)
+            self._check(self._L.bem_set_field_callback(self._h, self._cb, None))
+
+    # -------------------------------------------------------------- plumbing
+    def _check(self, rc):
+        if rc == L.BEM_OK:
+            return
+        msg = self._L.bem_last_error(self._h).decode() if self._h else ""
+        if rc == L.BEM_ERR_NEGATIVE_X:
+            raise IndexError(msg or "negative values")
+        raise L.BemError(rc, msg)
+
+    def close(self):
+        if self._h:
+            self._L.bem_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> L.Params:
+        p = L.Params()
+        self._check(self._L.bem_get_params(self._h, C.byref(p)))
+        return p
+
+    def _update(self, **kw):
+        p = self.params()
+        for k, v in kw.items():
+            setattr(p, k, v)
+        self._check(self._L.bem_set_params(self._h, C.byref(p)))
+
+    # -------------------------------------------------------------- setters (Simulation.hpp:92-167)
+    def set_phi(self, value):
+        a = np.full(self.N, float(value)) if np.isscalar(value) else np.ascontiguousarray(value, dtype=np.float64)
+        self._check(self._L.bem_set_phi(self._h, _d(a)))
+
+    def set_psi(self, value):
+        a = np.ascontiguousarray(value, dtype=np.float64)
+        self._check(self._L.bem_set_psi(self._h, _d(a)))
+
+    def get_phi(self):
+        a = np.empty(self.N)
+        self._check(self._L.bem_get_phi(self._h, _d(a)))
+        return a
+
+    def get_psi(self):
+        a = np.empty(self.N)
+        self._check(self._L.bem_get_psi(self._h, _d(a)))
+        return a
+
+    def get_vertices(self):
+        a = np.empty((self.N, 3))
+        self._check(self._L.bem_get_vertices(self._h, _d(a)))
+        return a
+
+    def set_vertices(self, v):
+        a = np.ascontiguousarray(v, dtype=np.float64)
+        self._check(self._L.bem_set_vertices(self._h, _d(a)))
+
+    def set_V_0(self, v):
+        self._check(self._L.bem_set_V0(self._h, float(v)))
+
+    def get_V_0(self):
+        a = np.zeros(1)
+        self._check(self._L.bem_get_V0(self._h, _d(a)))
+        return float(a[0])
+
+    def set_time(self, t):
+        self._check(self._L.bem_set_time(self._h, float(t)))
+
+    def get_time(self):
+        a = np.zeros(1)
+        self._check(self._L.bem_get_time(self._h, _d(a)))
+        return float(a[0])
+
+    def get_volume(self):
+        a = np.zeros(1)
+        self._check(self._L.bem_get_volume(self._h, _d(a)))
+        return float(a[0])
+
+    def set_min_dt(self, v):
+        self._update(min_dt=float(v))
+
+    def set_dp_balance(self, v):
+        self._update(dp_balance=float(v))
+
+    def set_bcgstab(self, on: bool):
+        self._update(solver=L.SOLVER_BICGSTAB if on else L.SOLVER_LU)
+
+    def set_solver(self, name: str):
+        self._update(solver={"bicgstab": L.SOLVER_BICGSTAB, "lu": L.SOLVER_LU, "mixed": L.SOLVER_MIXED}[name])
+
+    def set_mirror(self, on: bool):
+        self._update(mirror=int(bool(on)))
+
+    def stats(self) -> L.Stats:
+        s = L.Stats()
+        self._check(self._L.bem_get_stats(self._h, C.byref(s)))
+        return s
+
+    # -------------------------------------------------------------- hot path
+    def assemble_matrices(self, verts=None):
+        """ColocSim::assemble_matrices -> (G, H), column-major N x N float64."""
+        G = np.empty((self.N, self.N), order="F")
+        H = np.empty((self.N, self.N), order="F")
+        v = None if verts is None else np.ascontiguousarray(verts, dtype=np.float64)
+        self._check(self._L.bem_assemble(self._h, _d(v) if v is not None else None, _d(G), _d(H)))
+        return G, H
+
+    def solve_system(self, G, b):
+        G = np.asfortranarray(G, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.empty(self.N)
+        self._check(self._L.bem_solve_system(self._h, _d(G), _d(b), _d(x)))
+        return x
+
+    def position_t(self, pot, verts=None, return_psi=False):
+        pot = np.ascontiguousarray(pot, dtype=np.float64)
+        vel = np.empty((self.N, 3))
+        psi = np.empty(self.N)
+        v = None if verts is None else np.ascontiguousarray(verts, dtype=np.float64)
+        self._check(self._L.bem_position_t(self._h, _d(v) if v is not None else None, _d(pot), _d(vel), _d(psi)))
+        return (vel, psi) if return_psi else vel
+
+    def pot_t_multi(self, grads, t, verts=None):
+        g = np.ascontiguousarray(grads, dtype=np.float64)
+        out = np.empty(self.N)
+        v = None if verts is None else np.ascontiguousarray(verts, dtype=np.float64)
+        self._check(self._L.bem_pot_t_multi(self._h, _d(v) if v is not None else None, _d(g), float(t), _d(out)))
+        return out
+
+    def evolve_system_RK4(self, dp, fixdt=False):
+        dt = np.zeros(1)
+        self._check(self._L.bem_evolve_rk4(self._h, float(dp), int(bool(fixdt)), _d(dt)))
+        return float(dt[0])
+
+    def evolve_system(self, dp, fixdt=False):
+        dt = np.zeros(1)
+        self._check(self._L.bem_evolve_euler(self._h, float(dp), int(bool(fixdt)), _d(dt)))
+        return float(dt[0])
+
+    def evolve_rk4_steps(self, dt, steps):
+        """`steps` fixed-dt RK4 steps with no host round trip in between."""
+        self._check(self._L.bem_evolve_rk4_n(self._h, float(dt), int(steps)))
+
+    def sync(self):
+        self._check(self._L.bem_sync(self._h))

@@ -1,0 +1,338 @@
+// Dense collocation assembly of G (single layer) and H (double layer) in FP64.
+//
+// Replaces ColocSim::assemble_matrices (Bem/Simulation/ColocSim.cpp:21-110) with the per-pair
+// integrals of Integrator::integrate_Lin_coloc_local[_mir] (Bem/Integration/Integrator.cpp:237-283):
+//   * regular pairs (vertex i not on triangle t): 7-point rule on the triangle
+//     (integrate_disjoint_coloc[_mir], Integrator.hpp:471-513, kernel Integrator.hpp:116-119);
+//   * singular pairs (i on t): polar rule with the analytic radial integral and 7-point Gauss in
+//     the angle (integrate_identical_coloc[_mir], Integrator.cpp:13-89);
+//   * the "4 pi rule" diagonal H(i,i) -= 4 pi + sum_j H(i,j) (ColocSim.cpp:85-97).
+//
+// Tiling (B200): a CTA owns one column group (CG vertices, i.e. CG columns of G and H) and a block
+// of ASM_ROWS collocation rows, one row per thread.  It walks the triangles incident to its
+// vertices in increasing index order (the reference's per-column summation order), with the
+// triangle records staged in shared memory and read as broadcasts, and accumulates the CG columns
+// of its rows in shared memory.  Column writes are coalesced (column-major, consecutive rows).
+// No atomics: every entry is summed by exactly one thread in a fixed order, so the result is
+// bit-reproducible run to run.  The same pass produces the per-group partial row sums of H and
+// partial H*phi, so the 4 pi diagonal and the right-hand side need no second read of H.
+#include <math.h>
+
+#include "ctx.h"
+
+namespace bemb {
+
+// c[q][k] = w_q * basis_k(u_q, v_q) for the 7-point rule mapped to the 45-degree unit triangle
+// (u, v) = (qx + qy, qy), basis (1-u, u-v, v) (ResultTypes.hpp:111-117); u_q, v_q; Gauss-7 angle data.
+__constant__ double c_qc[7][3];
+__constant__ double c_quv[7][2];
+__constant__ double c_gcos[7], c_gsin[7], c_gw[7];
+
+// Reference tables (quadrature.hpp:30-38 gauss_7, :88-96 quadrature_7), evaluated on the host once.
+static void upload_constants() {
+    static bool done = false;
+    if (done) return;
+    const double Q[7][3] = {{0.33333333333333333, 0.33333333333333333, 0.22500000000000000 * 0.5},
+                            {0.79742698535308720, 0.10128650732345633, 0.12593918054482717 * 0.5},
+                            {0.10128650732345633, 0.79742698535308720, 0.12593918054482717 * 0.5},
+                            {0.10128650732345633, 0.10128650732345633, 0.12593918054482717 * 0.5},
+                            {0.05971587178976981, 0.47014206410511505, 0.13239415278850616 * 0.5},
+                            {0.47014206410511505, 0.05971587178976981, 0.13239415278850616 * 0.5},
+                            {0.47014206410511505, 0.47014206410511505, 0.13239415278850616 * 0.5}};
+    const double GL[7][2] = {{0.5 * (1.0 + 0.0000000000000000), 0.5 * 0.4179591836734694},
+                             {0.5 * (1.0 + 0.4058451513773972), 0.5 * 0.3818300505051189},
+                             {0.5 * (1.0 - 0.4058451513773972), 0.5 * 0.3818300505051189},
+                             {0.5 * (1.0 - 0.7415311855993945), 0.5 * 0.2797053914892766},
+                             {0.5 * (1.0 + 0.7415311855993945), 0.5 * 0.2797053914892766},
+                             {0.5 * (1.0 - 0.9491079123427585), 0.5 * 0.1294849661688697},
+                             {0.5 * (1.0 + 0.9491079123427585), 0.5 * 0.1294849661688697}};
+    double qc[7][3], quv[7][2], gc[7], gs[7], gw[7];
+    for (int q = 0; q < 7; ++q) {
+        double u = Q[q][0] + Q[q][1], v = Q[q][1], w = Q[q][2];
+        quv[q][0] = u;
+        quv[q][1] = v;
+        qc[q][0] = (1.0 - u) * w;
+        qc[q][1] = (u - v) * w;
+        qc[q][2] = v * w;
+        double th = GL[q][0] * 0.78539816339744830962;
+        gc[q] = cos(th);
+        gs[q] = sin(th);
+        gw[q] = GL[q][1];
+    }
+    cudaMemcpyToSymbol(c_qc, qc, sizeof(qc));
+    cudaMemcpyToSymbol(c_quv, quv, sizeof(quv));
+    cudaMemcpyToSymbol(c_gcos, gc, sizeof(gc));
+    cudaMemcpyToSymbol(c_gsin, gs, sizeof(gs));
+    cudaMemcpyToSymbol(c_gw, gw, sizeof(gw));
+    done = true;
+}
+
+// Per-triangle record: Interpolator (Interpolator.hpp:15-37) quantities and the 7 quadrature
+// points y_q = a + u_q*ab + v_q*bc.
+__global__ void k_triangle_records(int M, const double* __restrict__ x, const int* __restrict__ tri,
+                                   double* __restrict__ rec) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
+    double ax = x[3 * ia], ay = x[3 * ia + 1], az = x[3 * ia + 2];
+    double abx = x[3 * ib] - ax, aby = x[3 * ib + 1] - ay, abz = x[3 * ib + 2] - az;
+    double bcx = x[3 * ic] - x[3 * ib], bcy = x[3 * ic + 1] - x[3 * ib + 1], bcz = x[3 * ic + 2] - x[3 * ib + 2];
+    double nx = aby * bcz - abz * bcy, ny = abz * bcx - abx * bcz, nz = abx * bcy - aby * bcx;
+    double area = sqrt(nx * nx + ny * ny + nz * nz);
+    double ia_ = 1.0 / area;
+    double* r = rec + (size_t)t * REC;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        double u = c_quv[q][0], v = c_quv[q][1];
+        r[3 * q + 0] = (ax + u * abx) + v * bcx;
+        r[3 * q + 1] = (ay + u * aby) + v * bcy;
+        r[3 * q + 2] = (az + u * abz) + v * bcz;
+    }
+    r[21] = nx * ia_;
+    r[22] = ny * ia_;
+    r[23] = nz * ia_;
+    r[24] = area;
+    r[25] = r[26] = r[27] = 0.0;
+}
+
+// Regular 7-point rule of one (row, triangle) pair; returns area-scaled G and H basis integrals.
+template <bool MIRROR>
+__device__ __forceinline__ void regular_pair(const double* __restrict__ r, double xi0, double xi1, double xi2,
+                                             double& g0, double& g1, double& g2, double& h0, double& h1,
+                                             double& h2) {
+    const double nx = r[21], ny = r[22], nz = r[23], area = r[24];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        double yx = r[3 * q], zy = r[3 * q + 1] - xi1, zz = r[3 * q + 2] - xi2;
+        double zx = yx - xi0;
+        double yz2 = zy * zy + zz * zz;
+        double inv = rsqrt(zx * zx + yz2);
+        double dn = zx * nx + (zy * ny + zz * nz);
+        double gq = inv;
+        double hq = -dn * (inv * inv * inv);
+        if (MIRROR) {
+            // image point (-y.x, y.y, y.z) with image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
+            double mx = -yx - xi0;
+            double inv2 = rsqrt(mx * mx + yz2);
+            double dn2 = -mx * nx + (zy * ny + zz * nz);
+            gq += inv2;
+            hq += -dn2 * (inv2 * inv2 * inv2);
+        }
+        a0 = fma(c_qc[q][0], gq, a0);
+        a1 = fma(c_qc[q][1], gq, a1);
+        a2 = fma(c_qc[q][2], gq, a2);
+        b0 = fma(c_qc[q][0], hq, b0);
+        b1 = fma(c_qc[q][1], hq, b1);
+        b2 = fma(c_qc[q][2], hq, b2);
+    }
+    g0 = a0 * area;
+    g1 = a1 * area;
+    g2 = a2 * area;
+    h0 = b0 * area;
+    h1 = b1 * area;
+    h2 = b2 * area;
+}
+
+// Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  Results in the triangle's
+// original vertex order.  Reads the vertex positions from global memory (rare path).
+template <bool MIRROR>
+__device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta, int tb, int tc, int shift,
+                                           double* g, double* h) {
+    int v[3] = {ta, tb, tc};
+    int r0 = v[shift], r1 = v[(shift + 1) % 3], r2 = v[(shift + 2) % 3];
+    double ax = x[3 * r0], ay = x[3 * r0 + 1], az = x[3 * r0 + 2];
+    double abx = x[3 * r1] - ax, aby = x[3 * r1 + 1] - ay, abz = x[3 * r1 + 2] - az;
+    double bcx = x[3 * r2] - x[3 * r1], bcy = x[3 * r2 + 1] - x[3 * r1 + 1], bcz = x[3 * r2 + 2] - x[3 * r1 + 2];
+    double nx = aby * bcz - abz * bcy, ny = abz * bcx - abx * bcz, nz = abx * bcy - aby * bcx;
+    double area = sqrt(nx * nx + ny * ny + nz * nz);
+    double jac = 0.5 * area * 0.78539816339744830962;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        double cx = c_gcos[q], sx = c_gsin[q];
+        double dx = cx * abx + sx * bcx, dy = cx * aby + sx * bcy, dz = cx * abz + sx * bcz;
+        double dist = sqrt(dx * dx + dy * dy + dz * dz);
+        double of = jac * c_gw[q] / dist;
+        double fac = 1.0 / (cx * cx);
+        s0 += of * cx * fac;
+        s1 += of * (cx - sx) * fac;
+        s2 += of * sx * fac;
+    }
+    double rg[3] = {s0, s1, s2}, rh[3] = {0.0, 0.0, 0.0};
+    if (MIRROR) {
+        // regular rule over the mirrored own triangle, plain kernel, H sign flipped (Integrator.cpp:70-86)
+        double bx = ax + abx, by = ay + aby, bz = az + abz;
+        double cxp = bx + bcx, cyp = by + bcy, czp = bz + bcz;
+        double max_ = -ax, mbx = -bx, mcx = -cxp;
+        double mabx = mbx - max_, maby = by - ay, mabz = bz - az;
+        double mbcx = mcx - mbx, mbcy = cyp - by, mbcz = czp - bz;
+        double mnx = maby * mbcz - mabz * mbcy, mny = mabz * mbcx - mabx * mbcz, mnz = mabx * mbcy - maby * mbcx;
+        double marea = sqrt(mnx * mnx + mny * mny + mnz * mnz);
+        double mi = 1.0 / marea;
+        mnx *= mi;
+        mny *= mi;
+        mnz *= mi;
+        double a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            double u = c_quv[q][0], w = c_quv[q][1];
+            double zx = (max_ + u * mabx) + w * mbcx - ax;
+            double zy = (ay + u * maby) + w * mbcy - ay;
+            double zz = (az + u * mabz) + w * mbcz - az;
+            double inv = 1.0 / sqrt(zx * zx + zy * zy + zz * zz);
+            double hq = -(zx * mnx + zy * mny + zz * mnz) * inv * inv * inv;
+            a0 += c_qc[q][0] * inv;
+            a1 += c_qc[q][1] * inv;
+            a2 += c_qc[q][2] * inv;
+            b0 += c_qc[q][0] * hq;
+            b1 += c_qc[q][1] * hq;
+            b2 += c_qc[q][2] * hq;
+        }
+        rg[0] += a0 * marea;
+        rg[1] += a1 * marea;
+        rg[2] += a2 * marea;
+        rh[0] = -(b0 * marea);
+        rh[1] = -(b1 * marea);
+        rh[2] = -(b2 * marea);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        g[(k + shift) % 3] = rg[k];
+        h[(k + shift) % 3] = rh[k];
+    }
+}
+
+template <bool MIRROR>
+__global__ void __launch_bounds__(ASM_ROWS) k_assemble(int N, const double* __restrict__ x, const int* __restrict__ tri,
+                                                       const double* __restrict__ rec, const int* __restrict__ grp_off,
+                                                       const int* __restrict__ grp_tri, const int* __restrict__ grp_slot,
+                                                       const int* __restrict__ grp_vert, const double* __restrict__ phi,
+                                                       double* __restrict__ G, double* __restrict__ H,
+                                                       double* __restrict__ rowHp, double* __restrict__ bp) {
+    extern __shared__ __align__(16) double smem[];
+    double* accG = smem;                        // [CG][ASM_ROWS]
+    double* accH = accG + CG * ASM_ROWS;        // [CG][ASM_ROWS]
+    double* srec = accH + CG * ASM_ROWS;        // [ASM_TC][REC]
+    int* sinfo = reinterpret_cast<int*>(srec + ASM_TC * REC);  // [ASM_TC][4]
+    const int g = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int i = blockIdx.y * ASM_ROWS + tid;
+#pragma unroll 4
+    for (int s = 0; s < CG; ++s) {
+        accG[s * ASM_ROWS + tid] = 0.0;
+        accH[s * ASM_ROWS + tid] = 0.0;
+    }
+    double xi0 = 0.0, xi1 = 0.0, xi2 = 0.0;
+    if (i < N) {
+        xi0 = x[3 * i];
+        xi1 = x[3 * i + 1];
+        xi2 = x[3 * i + 2];
+    }
+    const int tb = grp_off[g], te = grp_off[g + 1];
+    for (int c0 = tb; c0 < te; c0 += ASM_TC) {
+        const int cnt = min(ASM_TC, te - c0);
+        __syncthreads();
+        for (int e = tid; e < cnt * (REC / 2); e += ASM_ROWS) {
+            int tt = e / (REC / 2), w = e - tt * (REC / 2);
+            const double2* src = reinterpret_cast<const double2*>(rec + (size_t)grp_tri[c0 + tt] * REC);
+            reinterpret_cast<double2*>(srec + tt * REC)[w] = src[w];
+        }
+        for (int e = tid; e < cnt; e += ASM_ROWS) {
+            int t = grp_tri[c0 + e];
+            sinfo[4 * e] = grp_slot[c0 + e];
+            sinfo[4 * e + 1] = tri[3 * t];
+            sinfo[4 * e + 2] = tri[3 * t + 1];
+            sinfo[4 * e + 3] = tri[3 * t + 2];
+        }
+        __syncthreads();
+        if (i < N) {
+            for (int tt = 0; tt < cnt; ++tt) {
+                const int4 info = reinterpret_cast<const int4*>(sinfo)[tt];
+                double gv[3], hv[3];
+                if (i == info.y || i == info.z || i == info.w) {
+                    int shift = (i == info.y) ? 0 : ((i == info.z) ? 1 : 2);
+                    singular_pair<MIRROR>(x, info.y, info.z, info.w, shift, gv, hv);
+                } else {
+                    regular_pair<MIRROR>(srec + tt * REC, xi0, xi1, xi2, gv[0], gv[1], gv[2], hv[0], hv[1], hv[2]);
+                }
+                const int code = info.x;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    int s = (code >> (6 * k)) & 63;
+                    if (s != 63) {
+                        accG[s * ASM_ROWS + tid] += gv[k];
+                        accH[s * ASM_ROWS + tid] += hv[k];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (i < N) {
+        double rs = 0.0, bs = 0.0;
+        for (int s = 0; s < CG; ++s) {
+            int v = grp_vert[g * CG + s];
+            if (v < 0) continue;
+            double gv = accG[s * ASM_ROWS + tid], hv = accH[s * ASM_ROWS + tid];
+            G[(size_t)v * N + i] = gv;
+            H[(size_t)v * N + i] = hv;
+            rs += hv;
+            bs = fma(hv, phi[v], bs);
+        }
+        rowHp[(size_t)g * N + i] = rs;
+        bp[(size_t)g * N + i] = bs;
+    }
+}
+
+// 4 pi rule and right-hand side: H(i,i) -= 4 pi - val, val = -sum_j H(i,j); b = H*phi.
+__global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
+                           const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double val = 0.0, bs = 0.0;
+    for (int g = 0; g < ngroups; ++g) {
+        val -= rowHp[(size_t)g * N + i];
+        bs += bp[(size_t)g * N + i];
+    }
+    double d = -(4.0 * 3.14159265358979323846 - val);
+    H[(size_t)i * N + i] += d;
+    if (b) b[i] = fma(d, phi[i], bs);
+}
+
+void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
+    upload_constants();
+    int M = (int)c.topo.M;
+    k_triangle_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, c.topo.tri, c.rec);
+}
+
+static size_t asm_smem() {
+    return sizeof(double) * (2 * CG * ASM_ROWS + ASM_TC * REC) + sizeof(int) * 4 * ASM_TC;
+}
+
+void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b, cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    launch_triangle_records(c, x, s);
+    dim3 grid(c.topo.ngroups, (N + ASM_ROWS - 1) / ASM_ROWS);
+    size_t sm = asm_smem();
+    if (c.prm.mirror) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            attr = true;
+        }
+        k_assemble<true><<<grid, ASM_ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off, c.topo.grp_tri,
+                                                    c.topo.grp_slot, c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            attr = true;
+        }
+        k_assemble<false><<<grid, ASM_ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off, c.topo.grp_tri,
+                                                     c.topo.grp_slot, c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
+    }
+    k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
+}
+
+}  // namespace bemb

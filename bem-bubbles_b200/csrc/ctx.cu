@@ -1,0 +1,657 @@
+// C ABI of libbem_b200.so (include/bem_b200.h): context life cycle, host-side topology
+// preprocessing, and the per-step orchestration of LinLinSim::evolve_system_RK4 / evolve_system
+// (Bem/Simulation/LinLinSim.cpp:194-284) as a sequence of device kernels on one stream.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <deque>
+#include <new>
+#include <numeric>
+#include <set>
+#include <vector>
+
+#include "ctx.h"
+
+namespace bemb {
+
+// ---------------------------------------------------------------- device memory helpers
+template <typename T>
+static int dalloc(Ctx& c, T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return c.fail(BEM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    c.allocs.push_back((void*)*p);
+    c.bytes += count * sizeof(T);
+    return BEM_OK;
+}
+
+static void free_all(Ctx& c) {
+    for (void* p : c.allocs) cudaFree(p);
+    c.allocs.clear();
+    c.bytes = 0;
+    c.topo = Topology{};
+    c.have_mesh = false;
+    c.xinv_valid = false;
+}
+
+// ---------------------------------------------------------------- topology preprocessing
+struct HostTopo {
+    std::vector<int> tri, csr_off, csr_idx, grp_off, grp_tri, grp_slot, grp_vert, part_of_vert, part_off,
+        part_tidx, tri_rot;
+    int ngroups = 0, nparts = 0;
+};
+
+static int build_topology(int64_t N, int64_t M, const int64_t* trigs, HostTopo& h, std::string& err) {
+    h.tri.resize((size_t)(3 * M));
+    for (int64_t j = 0; j < 3 * M; ++j) {
+        if (trigs[j] < 0 || trigs[j] >= N) {
+            err = "triangle index out of range";
+            return BEM_ERR_ARG;
+        }
+        h.tri[(size_t)j] = (int)trigs[j];
+    }
+    // vertex -> triangles (increasing triangle order, Mesh.cpp:75-84)
+    h.csr_off.assign((size_t)N + 1, 0);
+    for (int64_t j = 0; j < 3 * M; ++j) h.csr_off[(size_t)h.tri[(size_t)j] + 1]++;
+    for (int64_t i = 0; i < N; ++i) h.csr_off[(size_t)i + 1] += h.csr_off[(size_t)i];
+    h.csr_idx.assign((size_t)(3 * M), 0);
+    std::vector<int> fill(h.csr_off.begin(), h.csr_off.end() - 1);
+    for (int64_t j = 0; j < M; ++j)
+        for (int k = 0; k < 3; ++k) h.csr_idx[(size_t)fill[(size_t)h.tri[(size_t)(3 * j + k)]]++] = (int)j;
+    for (int64_t i = 0; i < N; ++i)
+        if (h.csr_off[(size_t)i + 1] == h.csr_off[(size_t)i]) {
+            err = "vertex " + std::to_string(i) + " belongs to no triangle";
+            return BEM_ERR_ARG;
+        }
+    // vertex adjacency
+    std::vector<std::vector<int>> nbr((size_t)N);
+    for (int64_t j = 0; j < M; ++j)
+        for (int k = 0; k < 3; ++k) {
+            int a = h.tri[(size_t)(3 * j + k)];
+            nbr[(size_t)a].push_back(h.tri[(size_t)(3 * j + (k + 1) % 3)]);
+            nbr[(size_t)a].push_back(h.tri[(size_t)(3 * j + (k + 2) % 3)]);
+        }
+    for (auto& v : nbr) {
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+    }
+    // loose parts, in order of their smallest vertex (split_by_loose_parts, Mesh.cpp:382-440)
+    h.part_of_vert.assign((size_t)N, -1);
+    int np = 0;
+    for (int64_t s = 0; s < N; ++s) {
+        if (h.part_of_vert[(size_t)s] >= 0) continue;
+        std::vector<int> st{(int)s};
+        h.part_of_vert[(size_t)s] = np;
+        while (!st.empty()) {
+            int v = st.back();
+            st.pop_back();
+            for (int u : nbr[(size_t)v])
+                if (h.part_of_vert[(size_t)u] < 0) {
+                    h.part_of_vert[(size_t)u] = np;
+                    st.push_back(u);
+                }
+        }
+        ++np;
+    }
+    h.nparts = np;
+    h.part_off.assign((size_t)np + 1, 0);
+    for (int64_t j = 0; j < M; ++j) h.part_off[(size_t)h.part_of_vert[(size_t)h.tri[(size_t)(3 * j)]] + 1]++;
+    for (int p = 0; p < np; ++p) h.part_off[(size_t)p + 1] += h.part_off[(size_t)p];
+    h.part_tidx.assign((size_t)M, 0);
+    std::vector<int> pf(h.part_off.begin(), h.part_off.end() - 1);
+    h.tri_rot.assign((size_t)(3 * M), 0);
+    for (int64_t j = 0; j < M; ++j) {
+        const int* t = &h.tri[(size_t)(3 * j)];
+        h.part_tidx[(size_t)pf[(size_t)h.part_of_vert[(size_t)t[0]]]++] = (int)j;
+        int r = 0;
+        if (t[1] > t[r]) r = 1;
+        if (t[2] > t[r]) r = 2;
+        for (int k = 0; k < 3; ++k) h.tri_rot[(size_t)(3 * j + k)] = t[(r + k) % 3];
+    }
+    // assembly column groups: breadth-first patches of at most CG vertices
+    std::vector<int> grp((size_t)N, -1), slot((size_t)N, -1);
+    std::vector<std::vector<int>> members;
+    for (int64_t s = 0; s < N; ++s) {
+        if (grp[(size_t)s] >= 0) continue;
+        const int gid = (int)members.size();
+        members.emplace_back();
+        std::deque<int> q{(int)s};
+        std::vector<char> queued;
+        std::set<int> inq{(int)s};
+        while (!q.empty() && (int)members.back().size() < CG) {
+            int v = q.front();
+            q.pop_front();
+            if (grp[(size_t)v] >= 0) continue;
+            grp[(size_t)v] = gid;
+            slot[(size_t)v] = (int)members.back().size();
+            members.back().push_back(v);
+            for (int u : nbr[(size_t)v])
+                if (grp[(size_t)u] < 0 && !inq.count(u)) {
+                    inq.insert(u);
+                    q.push_back(u);
+                }
+        }
+    }
+    h.ngroups = (int)members.size();
+    h.grp_off.assign((size_t)h.ngroups + 1, 0);
+    h.grp_vert.assign((size_t)h.ngroups * CG, -1);
+    for (int g = 0; g < h.ngroups; ++g) {
+        std::vector<int> tl;
+        for (int v : members[(size_t)g]) {
+            h.grp_vert[(size_t)g * CG + slot[(size_t)v]] = v;
+            for (int e = h.csr_off[(size_t)v]; e < h.csr_off[(size_t)v + 1]; ++e) tl.push_back(h.csr_idx[(size_t)e]);
+        }
+        std::sort(tl.begin(), tl.end());
+        tl.erase(std::unique(tl.begin(), tl.end()), tl.end());
+        for (int t : tl) {
+            int code = 0;
+            for (int k = 0; k < 3; ++k) {
+                int v = h.tri[(size_t)(3 * t + k)];
+                int sl = (grp[(size_t)v] == g) ? slot[(size_t)v] : 63;
+                code |= sl << (6 * k);
+            }
+            h.grp_tri.push_back(t);
+            h.grp_slot.push_back(code);
+        }
+        h.grp_off[(size_t)g + 1] = (int)h.grp_tri.size();
+    }
+    return BEM_OK;
+}
+
+template <typename T>
+static int upload(Ctx& c, T** dst, const std::vector<T>& src) {
+    int rc = dalloc(c, dst, src.size());
+    if (rc) return rc;
+    BEM_CUDA(c, cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return BEM_OK;
+}
+
+// ---------------------------------------------------------------- small kernels
+__global__ void k_set_dt(DevScalars* sc, double dt) { sc->dt = dt; }
+__global__ void k_set_time(DevScalars* sc, double t) { sc->time = t; }
+__global__ void k_set_V0(DevScalars* sc, double v) { sc->V0 = v; }
+__global__ void k_copy_vol(DevScalars* sc, const double* vol) { sc->V0 = vol[0]; }
+__global__ void k_total_volume(const double* vol, int np, double* out) {
+    double s = 0.0;
+    for (int p = 0; p < np; ++p) s += vol[p];
+    *out = s;
+}
+
+// ---------------------------------------------------------------- stage building blocks
+static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    switch (c.prm.solver) {
+        case BEM_SOLVER_LU:
+            return lu_solve(c, A, b, x, s);
+        case BEM_SOLVER_MIXED:
+            return mixed_solve(c, A, b, x, s);
+        default:
+            return bicgstab(c, A, b, x, s);
+    }
+}
+
+// LinLinSim::position_t (LinLinSim.cpp:26-83)
+static int position_t(Ctx& c, const double* x, const double* pot, double* vel, cudaStream_t s) {
+    launch_assemble(c, x, pot, c.G, c.H, c.b, s);
+    int rc = solve(c, c.G, c.b, c.psil, s);
+    if (rc) return rc;
+    launch_velocity_prep(c, x, pot, s);
+    launch_velocity(c, c.psil, vel, s);
+    return BEM_OK;
+}
+
+// Field values for the callback form: positions back to the host, one call per vertex.
+static int eval_field_callback(Ctx& c, const double* x, cudaStream_t s) {
+    const int64_t N = c.topo.N;
+    std::vector<double> hx((size_t)(3 * N)), hf((size_t)N);
+    double t = 0.0;
+    BEM_CUDA(c, cudaMemcpyAsync(hx.data(), x, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaMemcpyAsync(&t, &c.sc->time, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < N; ++i) hf[(size_t)i] = c.field_cb(&hx[(size_t)(3 * i)], t, c.field_user);
+    BEM_CUDA(c, cudaMemcpyAsync(c.fieldv, hf.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    return BEM_OK;
+}
+
+// LinLinSim::pot_t_multi (LinLinSim.cpp:98-120)
+static int pot_t_multi(Ctx& c, const double* x, const double* vel, double* out, cudaStream_t s) {
+    const double* fv = nullptr;
+    if (c.field_cb) {
+        int rc = eval_field_callback(c, x, s);
+        if (rc) return rc;
+        fv = c.fieldv;
+    }
+    launch_pot_t(c, x, vel, fv, out, s);
+    return BEM_OK;
+}
+
+static int check_negative(Ctx& c, cudaStream_t s) {
+    int f = 0;
+    BEM_CUDA(c, cudaMemsetAsync(c.flag + 1, 0, sizeof(int), s));
+    launch_any_negative(c, c.x, c.flag + 1, s);
+    BEM_CUDA(c, cudaMemcpyAsync(&f, c.flag + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    if (f) return c.fail(BEM_ERR_NEGATIVE_X, "negative values");  // test_negative, LinLinSim.cpp:148-159
+    return BEM_OK;
+}
+
+// One RK4 step on the device state (LinLinSim.cpp:194-257); no host synchronisation unless an
+// iterative solver polls, a field callback is set, or dt is adaptive and requested back.
+static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
+    const int64_t N = c.topo.N;
+    BEM_CUDA(c, cudaMemcpyAsync(c.x1, c.x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
+    BEM_CUDA(c, cudaMemcpyAsync(c.p1, c.phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    int rc = position_t(c, c.x1, c.p1, c.k1, s);
+    if (rc) return rc;
+    if ((rc = pot_t_multi(c, c.x1, c.k1, c.kp1, s))) return rc;
+    if (fixdt)
+        k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
+    else
+        launch_get_dt(c, c.k1, c.kp1, dp, s);
+    const double* dtp = &c.sc->dt;
+    launch_axpy3(3 * N, c.x1, dtp, 0.5, c.k1, c.xs, s);
+    launch_axpy3(N, c.p1, dtp, 0.5, c.kp1, c.ps, s);
+    if ((rc = position_t(c, c.xs, c.ps, c.k2, s))) return rc;
+    if ((rc = pot_t_multi(c, c.xs, c.k2, c.kp2, s))) return rc;
+    launch_axpy3(3 * N, c.x1, dtp, 0.5, c.k2, c.xs, s);
+    launch_axpy3(N, c.p1, dtp, 0.5, c.kp2, c.ps, s);
+    if ((rc = position_t(c, c.xs, c.ps, c.k3, s))) return rc;
+    if ((rc = pot_t_multi(c, c.xs, c.k3, c.kp3, s))) return rc;
+    launch_axpy3(3 * N, c.x1, dtp, 1.0, c.k3, c.xs, s);
+    launch_axpy3(N, c.p1, dtp, 1.0, c.kp3, c.ps, s);
+    if ((rc = position_t(c, c.xs, c.ps, c.k4, s))) return rc;
+    if ((rc = pot_t_multi(c, c.xs, c.k4, c.kp4, s))) return rc;
+    launch_rk4_final(c, s);
+    return BEM_OK;
+}
+
+static int euler_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
+    int rc = position_t(c, c.x, c.phi, c.k1, s);
+    if (rc) return rc;
+    if ((rc = pot_t_multi(c, c.x, c.k1, c.kp1, s))) return rc;
+    if (fixdt)
+        k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
+    else
+        launch_get_dt(c, c.k1, c.kp1, dp, s);
+    launch_euler_final(c, c.k1, c.kp1, s);
+    return BEM_OK;
+}
+
+static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
+    Topology& t = c.topo;
+    t.N = N;
+    t.M = M;
+    t.ngroups = h.ngroups;
+    t.nparts = h.nparts;
+    t.h_part_of_vert = h.part_of_vert;
+    int rc;
+    if ((rc = upload(c, &t.tri, h.tri)) || (rc = upload(c, &t.csr_off, h.csr_off)) ||
+        (rc = upload(c, &t.csr_idx, h.csr_idx)) || (rc = upload(c, &t.grp_off, h.grp_off)) ||
+        (rc = upload(c, &t.grp_tri, h.grp_tri)) || (rc = upload(c, &t.grp_slot, h.grp_slot)) ||
+        (rc = upload(c, &t.grp_vert, h.grp_vert)) || (rc = upload(c, &t.part_of_vert, h.part_of_vert)) ||
+        (rc = upload(c, &t.part_off, h.part_off)) || (rc = upload(c, &t.part_tidx, h.part_tidx)) ||
+        (rc = upload(c, &t.tri_rot, h.tri_rot)))
+        return rc;
+    const size_t n = (size_t)N, m = (size_t)M, nn = n * n;
+    const int ncs = 64;
+    double** vec3s[] = {&c.x, &c.x1, &c.xs, &c.k1, &c.k2, &c.k3, &c.k4, &c.vn};
+    for (auto p : vec3s)
+        if ((rc = dalloc(c, p, 3 * n))) return rc;
+    double** vecs[] = {&c.phi, &c.psi, &c.b, &c.psil, &c.kap, &c.fieldv, &c.p1, &c.ps, &c.kp1, &c.kp2,
+                       &c.kp3, &c.kp4, &c.r, &c.r0, &c.pv, &c.vv, &c.yv, &c.zv, &c.sv, &c.tv, &c.invd};
+    for (auto p : vecs)
+        if ((rc = dalloc(c, p, n))) return rc;
+    if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (rc = dalloc(c, &c.LU, nn)) ||
+        (rc = dalloc(c, &c.rec, m * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) || (rc = dalloc(c, &c.tg, 3 * m)) ||
+        (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, (size_t)h.ngroups * n)) ||
+        (rc = dalloc(c, &c.bp, (size_t)h.ngroups * n)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
+        (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
+        (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
+        (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)))
+        return rc;
+    if (c.prm.solver == BEM_SOLVER_MIXED) {
+        if ((rc = dalloc(c, &c.Xinv, nn)) || (rc = dalloc(c, &c.Tw, nn)) || (rc = dalloc(c, &c.G32, nn)) ||
+            (rc = dalloc(c, &c.V, n * (size_t)(c.gmres_m + 1))) || (rc = dalloc(c, &c.Z, n * (size_t)c.gmres_m)))
+            return rc;
+    }
+    BEM_CUDA(c, cudaMemset(c.cnt, 0, sizeof(unsigned) * ((n + 255) / 256 + 1)));
+    BEM_CUDA(c, cudaMemset(c.phi, 0, sizeof(double) * n));
+    BEM_CUDA(c, cudaMemset(c.psi, 0, sizeof(double) * n));
+    BEM_CUDA(c, cudaMemset(c.psil, 0, sizeof(double) * n));
+    return BEM_OK;
+}
+
+static int ensure_mixed_buffers(Ctx& c) {
+    if (c.Xinv || !c.have_mesh) return BEM_OK;
+    const size_t n = (size_t)c.topo.N, nn = n * n;
+    int rc;
+    if ((rc = dalloc(c, &c.Xinv, nn)) || (rc = dalloc(c, &c.Tw, nn)) || (rc = dalloc(c, &c.G32, nn)) ||
+        (rc = dalloc(c, &c.V, n * (size_t)(c.gmres_m + 1))) || (rc = dalloc(c, &c.Z, n * (size_t)c.gmres_m)))
+        return rc;
+    return BEM_OK;
+}
+
+}  // namespace bemb
+
+using namespace bemb;
+
+struct bem_ctx : public Ctx {};
+
+#define CTX_GUARD(ctx)                    \
+    if (!(ctx)) return BEM_ERR_ARG;       \
+    cudaSetDevice((ctx)->device)
+#define NEED_MESH(ctx) \
+    if (!(ctx)->have_mesh) return (ctx)->fail(BEM_ERR_STATE, "no mesh set")
+
+extern "C" {
+
+void bem_default_params(bem_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->p_inf = 1.0;
+    p->epsilon = 1.0;
+    p->sigma = 0.0;
+    p->gamma = 1.0;
+    p->min_dt = -1.0;
+    p->dp_balance = 3.0;
+    p->nopen_eps = 1e-2;
+    p->mirror = 0;
+    p->solver = BEM_SOLVER_BICGSTAB;
+    p->mixed_tol = 1e-12;
+    p->max_iters = 0;
+}
+
+int bem_create(bem_ctx** out, int device, const bem_params* p) {
+    if (!out) return BEM_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return BEM_ERR_CUDA;
+    if (device < 0 || device >= ndev) return BEM_ERR_ARG;
+    bem_ctx* c = new (std::nothrow) bem_ctx();
+    if (!c) return BEM_ERR_NOMEM;
+    c->device = device;
+    if (p)
+        c->prm = *p;
+    else
+        bem_default_params(&c->prm);
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc((void**)&c->sc, sizeof(DevScalars)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_sc, sizeof(DevScalars)) != cudaSuccess ||
+        cudaMalloc((void**)&c->flag, 4 * sizeof(int)) != cudaSuccess) {
+        delete c;
+        return BEM_ERR_CUDA;
+    }
+    cudaMemset(c->sc, 0, sizeof(DevScalars));
+    cudaMemset(c->flag, 0, 4 * sizeof(int));
+    *out = c;
+    return BEM_OK;
+}
+
+int bem_destroy(bem_ctx* c) {
+    if (!c) return BEM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(*c);
+    cudaFree(c->sc);
+    cudaFree(c->flag);
+    cudaFreeHost(c->h_sc);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return BEM_OK;
+}
+
+const char* bem_last_error(const bem_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int bem_set_params(bem_ctx* c, const bem_params* p) {
+    CTX_GUARD(c);
+    if (!p) return c->fail(BEM_ERR_ARG, "null params");
+    const bool to_mixed = p->solver == BEM_SOLVER_MIXED && c->prm.solver != BEM_SOLVER_MIXED;
+    if (p->mirror != c->prm.mirror) c->xinv_valid = false;
+    c->prm = *p;
+    if (to_mixed) return ensure_mixed_buffers(*c);
+    return BEM_OK;
+}
+
+int bem_get_params(const bem_ctx* c, bem_params* p) {
+    if (!c || !p) return BEM_ERR_ARG;
+    *p = c->prm;
+    return BEM_OK;
+}
+
+int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const int64_t* trigs) {
+    CTX_GUARD(c);
+    if (N < 3 || M < 1 || !verts || !trigs) return c->fail(BEM_ERR_ARG, "bad mesh arguments");
+    if (N > (int64_t)1 << 20) return c->fail(BEM_ERR_ARG, "mesh too large for dense storage");
+    cudaStreamSynchronize(c->stream);
+    free_all(*c);
+    HostTopo h;
+    int rc = build_topology(N, M, trigs, h, c->err);
+    if (rc) return rc;
+    if ((rc = alloc_mesh(*c, N, M, h))) return rc;
+    BEM_CUDA(*c, cudaMemcpy(c->x, verts, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+    c->have_mesh = true;
+    // Simulation ctor: V_0 = volume(initial) (Simulation.hpp:42), time = 0
+    cudaStream_t s = c->stream;
+    k_set_time<<<1, 1, 0, s>>>(c->sc, 0.0);
+    launch_part_volumes(*c, c->x, c->vol, s);
+    k_total_volume<<<1, 1, 0, s>>>(c->vol, c->topo.nparts, c->vol + c->topo.nparts);
+    k_copy_vol<<<1, 1, 0, s>>>(c->sc, c->vol + c->topo.nparts);
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    return BEM_OK;
+}
+
+int bem_num_verts(const bem_ctx* c, int64_t* n) {
+    if (!c || !n) return BEM_ERR_ARG;
+    *n = c->topo.N;
+    return BEM_OK;
+}
+
+#define COPY_IN(dst, src, count)                                                                      \
+    do {                                                                                              \
+        if (!(src)) return c->fail(BEM_ERR_ARG, "null pointer");                                      \
+        BEM_CUDA(*c, cudaMemcpyAsync((dst), (src), sizeof(double) * (count), cudaMemcpyHostToDevice, c->stream)); \
+        BEM_CUDA(*c, cudaStreamSynchronize(c->stream));                                              \
+    } while (0)
+#define COPY_OUT(dst, src, count)                                                                     \
+    do {                                                                                              \
+        if (!(dst)) return c->fail(BEM_ERR_ARG, "null pointer");                                      \
+        BEM_CUDA(*c, cudaMemcpyAsync((dst), (src), sizeof(double) * (count), cudaMemcpyDeviceToHost, c->stream)); \
+        BEM_CUDA(*c, cudaStreamSynchronize(c->stream));                                              \
+    } while (0)
+
+int bem_set_vertices(bem_ctx* c, const double* v) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    COPY_IN(c->x, v, 3 * c->topo.N);
+    return BEM_OK;
+}
+int bem_get_vertices(bem_ctx* c, double* v) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    COPY_OUT(v, c->x, 3 * c->topo.N);
+    return BEM_OK;
+}
+int bem_set_phi(bem_ctx* c, const double* v) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    COPY_IN(c->phi, v, c->topo.N);
+    return BEM_OK;
+}
+int bem_get_phi(bem_ctx* c, double* v) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    COPY_OUT(v, c->phi, c->topo.N);
+    return BEM_OK;
+}
+int bem_set_psi(bem_ctx* c, const double* v) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    COPY_IN(c->psi, v, c->topo.N);
+    return BEM_OK;
+}
+int bem_get_psi(bem_ctx* c, double* v) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    COPY_OUT(v, c->psi, c->topo.N);
+    return BEM_OK;
+}
+int bem_set_time(bem_ctx* c, double t) {
+    CTX_GUARD(c);
+    k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return BEM_OK;
+}
+int bem_get_time(bem_ctx* c, double* t) {
+    CTX_GUARD(c);
+    COPY_OUT(t, &c->sc->time, 1);
+    return BEM_OK;
+}
+int bem_set_V0(bem_ctx* c, double v) {
+    CTX_GUARD(c);
+    k_set_V0<<<1, 1, 0, c->stream>>>(c->sc, v);
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return BEM_OK;
+}
+int bem_get_V0(bem_ctx* c, double* v) {
+    CTX_GUARD(c);
+    COPY_OUT(v, &c->sc->V0, 1);
+    return BEM_OK;
+}
+int bem_get_volume(bem_ctx* c, double* vol) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    // volume(mesh) over the whole mesh in triangle order (Mesh.cpp:206-218)
+    launch_part_volumes(*c, c->x, c->vol, c->stream);
+    k_total_volume<<<1, 1, 0, c->stream>>>(c->vol, c->topo.nparts, c->vol + c->topo.nparts);
+    COPY_OUT(vol, c->vol + c->topo.nparts, 1);
+    return BEM_OK;
+}
+int bem_set_field_callback(bem_ctx* c, bem_field_fn fn, void* user) {
+    CTX_GUARD(c);
+    c->field_cb = fn;
+    c->field_user = user;
+    return BEM_OK;
+}
+
+int bem_assemble(bem_ctx* c, const double* verts, double* G, double* H) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const int64_t N = c->topo.N;
+    const double* x = c->x;
+    if (verts) {
+        COPY_IN(c->xs, verts, 3 * N);
+        x = c->xs;
+    }
+    BEM_CUDA(*c, cudaMemsetAsync(c->p1, 0, sizeof(double) * N, c->stream));
+    launch_assemble(*c, x, c->p1, c->G, c->H, nullptr, c->stream);
+    BEM_CUDA(*c, cudaGetLastError());
+    if (G) COPY_OUT(G, c->G, N * N);
+    if (H) COPY_OUT(H, c->H, N * N);
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return BEM_OK;
+}
+
+int bem_solve_system(bem_ctx* c, const double* G, const double* b, double* x) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const int64_t N = c->topo.N;
+    if (!G || !b || !x) return c->fail(BEM_ERR_ARG, "null pointer");
+    COPY_IN(c->G, G, N * N);
+    COPY_IN(c->b, b, N);
+    int rc = solve(*c, c->G, c->b, c->psil, c->stream);
+    if (rc) return rc;
+    COPY_OUT(x, c->psil, N);
+    return BEM_OK;
+}
+
+int bem_position_t(bem_ctx* c, const double* verts, const double* pot, double* vel, double* psi_l) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const int64_t N = c->topo.N;
+    if (!pot || !vel) return c->fail(BEM_ERR_ARG, "null pointer");
+    const double* x = c->x;
+    if (verts) {
+        COPY_IN(c->xs, verts, 3 * N);
+        x = c->xs;
+    }
+    COPY_IN(c->ps, pot, N);
+    int rc = position_t(*c, x, c->ps, c->k1, c->stream);
+    if (rc) return rc;
+    BEM_CUDA(*c, cudaGetLastError());
+    COPY_OUT(vel, c->k1, 3 * N);
+    if (psi_l) COPY_OUT(psi_l, c->psil, N);
+    return BEM_OK;
+}
+
+int bem_pot_t_multi(bem_ctx* c, const double* verts, const double* grads, double t, double* out) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const int64_t N = c->topo.N;
+    if (!grads || !out) return c->fail(BEM_ERR_ARG, "null pointer");
+    const double* x = c->x;
+    if (verts) {
+        COPY_IN(c->xs, verts, 3 * N);
+        x = c->xs;
+    }
+    COPY_IN(c->k1, grads, 3 * N);
+    double t_saved = 0.0;
+    COPY_OUT(&t_saved, &c->sc->time, 1);
+    k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
+    int rc = pot_t_multi(*c, x, c->k1, c->kp1, c->stream);
+    k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t_saved);
+    if (rc) return rc;
+    BEM_CUDA(*c, cudaGetLastError());
+    COPY_OUT(out, c->kp1, N);
+    return BEM_OK;
+}
+
+int bem_evolve_rk4(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    int rc = check_negative(*c, c->stream);
+    if (rc) return rc;
+    if ((rc = rk4_step(*c, dp, fixdt != 0, c->stream))) return rc;
+    BEM_CUDA(*c, cudaGetLastError());
+    if (dt_out) COPY_OUT(dt_out, &c->sc->dt, 1);
+    return check_negative(*c, c->stream);
+}
+
+int bem_evolve_rk4_n(bem_ctx* c, double dt, int32_t steps) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    int rc = check_negative(*c, c->stream);
+    if (rc) return rc;
+    for (int k = 0; k < steps; ++k)
+        if ((rc = rk4_step(*c, dt, true, c->stream))) return rc;
+    BEM_CUDA(*c, cudaGetLastError());
+    return check_negative(*c, c->stream);
+}
+
+int bem_evolve_euler(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    int rc = euler_step(*c, dp, fixdt != 0, c->stream);
+    if (rc) return rc;
+    BEM_CUDA(*c, cudaGetLastError());
+    if (dt_out) COPY_OUT(dt_out, &c->sc->dt, 1);
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return BEM_OK;
+}
+
+int bem_get_stats(bem_ctx* c, bem_stats* s) {
+    if (!c || !s) return BEM_ERR_ARG;
+    *s = c->stats;
+    return BEM_OK;
+}
+
+int bem_sync(bem_ctx* c) {
+    CTX_GUARD(c);
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return BEM_OK;
+}
+
+}  // extern "C"

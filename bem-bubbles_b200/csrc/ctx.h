@@ -1,0 +1,90 @@
+// Context object behind the opaque bem_ctx handle: parameters, device-resident state and
+// every device work buffer of one simulation.
+#pragma once
+
+#include <string>
+
+#include "internal.h"
+
+namespace bemb {
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bem_params prm{};
+    std::string err;
+    Topology topo;
+    bool have_mesh = false;
+
+    // host pressure-field callback (reference: real(*pressurefield)(vec3, real))
+    bem_field_fn field_cb = nullptr;
+    void* field_user = nullptr;
+
+    // ---- device state (mesh.verts, phi, psi) and scalars
+    double* x = nullptr;    // N*3
+    double* phi = nullptr;  // N
+    double* psi = nullptr;  // N
+    DevScalars* sc = nullptr;
+    DevScalars* h_sc = nullptr;  // pinned mirror
+
+    // ---- per-stage work
+    double* G = nullptr;       // N*N column-major
+    double* H = nullptr;       // N*N column-major
+    double* b = nullptr;       // N
+    double* psil = nullptr;    // N, solved dphi/dn of the current stage
+    double* rec = nullptr;     // M*REC triangle records (quadrature points, normal, area)
+    double* tn = nullptr;      // M*3 triangle unit normals (Mesh.cpp formula)
+    double* tg = nullptr;      // M*3 tangential gradients of the stage potential
+    double* rowHp = nullptr;   // ngroups*N partial row sums of H
+    double* bp = nullptr;      // ngroups*N partial H*phi
+    double* vol = nullptr;     // nparts volumes
+    double* kap = nullptr;     // N mean curvature (sigma != 0)
+    double* tk = nullptr;      // M per-triangle mean curvature
+    double* fieldv = nullptr;  // N per-vertex field values (callback mode)
+    int* flag = nullptr;       // device int flags
+
+    // RK4 buffers
+    double *x1 = nullptr, *xs = nullptr, *k1 = nullptr, *k2 = nullptr, *k3 = nullptr, *k4 = nullptr;
+    double *p1 = nullptr, *ps = nullptr, *kp1 = nullptr, *kp2 = nullptr, *kp3 = nullptr, *kp4 = nullptr;
+    double* vn = nullptr;  // N*3 vertex normals
+
+    // ---- solver work
+    double* part = nullptr;        // GEMV partials, up to 64*N
+    unsigned* cnt = nullptr;       // GEMV completion counters
+    double* red = nullptr;         // reduction partials (VBLK * 8)
+    double *r = nullptr, *r0 = nullptr, *pv = nullptr, *vv = nullptr, *yv = nullptr, *zv = nullptr,
+           *sv = nullptr, *tv = nullptr, *invd = nullptr;
+    // LU
+    double* LU = nullptr;  // N*N
+    int* piv = nullptr;    // N
+    // mixed: approximate inverse (FP32), Krylov basis
+    float* Xinv = nullptr;     // N*N column-major
+    float* Tw = nullptr;       // N*N work for the Newton-Schulz refresh
+    float* G32 = nullptr;      // N*N FP32 copy of G for the refresh GEMMs
+    double* V = nullptr;       // N*(m+1) Krylov basis
+    double* Z = nullptr;       // N*m preconditioned directions
+    double* hcol = nullptr;    // (m+2) Hessenberg column / dot results
+    bool xinv_valid = false;
+    int gmres_m = 30;
+
+    // statistics
+    bem_stats stats{};
+
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+};
+
+// Record a CUDA error in the context and map it to a status.
+#define BEM_CUDA(c, call)                                                              \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return (c).fail(BEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+}  // namespace bemb

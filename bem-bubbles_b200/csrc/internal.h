@@ -1,0 +1,88 @@
+// Internal declarations shared by the CUDA translation units of libbem_b200.so.
+// Nothing here crosses the C ABI (include/bem_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/bem_b200.h"
+
+namespace bemb {
+
+// Column-group width of the assembly tiles: each CTA owns CG columns (vertices) of G and H.
+constexpr int CG = 32;
+// Rows per assembly CTA (one row per thread).
+constexpr int ASM_ROWS = 128;
+// Triangle records staged per chunk in shared memory.
+constexpr int ASM_TC = 32;
+// Doubles per triangle record: 7 quadrature points (21), unit normal (3), area (1), pad (3).
+constexpr int REC = 28;
+// Fixed block count of the vector kernels, so reductions have a fixed, deterministic shape.
+constexpr int VBLK = 128;
+constexpr int VTHR = 256;
+
+// Topology-derived, device-resident tables (rebuilt only when the triangle list changes).
+struct Topology {
+    int64_t N = 0, M = 0;
+    int* tri = nullptr;          // M*3 int32, reference vertex order
+    int* csr_off = nullptr;      // N+1, vertex -> incident triangles (increasing index)
+    int* csr_idx = nullptr;      // 3M
+    int ngroups = 0;             // assembly column groups
+    int* grp_off = nullptr;      // ngroups+1 into grp_tri
+    int* grp_tri = nullptr;      // triangles incident to the group's vertices, increasing
+    int* grp_slot = nullptr;     // per grp_tri entry: 3 x 6-bit owned-slot codes (63 = not owned)
+    int* grp_vert = nullptr;     // ngroups*CG vertex of each slot, -1 padding
+    int nparts = 0;              // loose parts (bubbles)
+    int* part_of_vert = nullptr; // N
+    int* part_off = nullptr;     // nparts+1 into part_tidx
+    int* part_tidx = nullptr;    // triangle ids grouped by part, increasing inside a part
+    int* tri_rot = nullptr;      // M*3: triangles rotated so the largest vertex id comes first,
+                                 // the vertex order split_by_loose_parts leaves (Mesh.cpp:410-426)
+    std::vector<int> h_part_of_vert;
+};
+
+// Control block of the iterative solvers and RK4 scalars, resident on the device.
+struct DevScalars {
+    double time;      // simulation time
+    double dt;        // current step
+    double V0;        // reference volume of the gas law
+    double field;     // far-field pressure at the step-start time (x-independent family)
+    // BiCGSTAB / GMRES scalars
+    double rho, alpha, w, beta, r0_sq, rhs_sq, tol2, rr;
+    int32_t iters, restarts, done, restart_flag, maxit, nonconv;
+    int32_t pad[2];
+};
+
+struct Ctx;
+
+// assemble.cu
+void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s);
+void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b,
+                     cudaStream_t s);
+
+// stage.cu
+void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s);
+void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s);
+void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* field_host, double* out,
+                  cudaStream_t s);
+void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s);
+void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k,
+                  double* out, cudaStream_t s);
+void launch_rk4_final(Ctx& c, cudaStream_t s);
+void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStream_t s);
+void launch_vertex_normals(Ctx& c, const double* x, double* out, cudaStream_t s);
+void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cudaStream_t s);
+void launch_any_negative(Ctx& c, const double* x, int* flag, cudaStream_t s);
+void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s);
+
+// linalg.cu
+void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part,
+          unsigned* counters);
+int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+
+}  // namespace bemb

@@ -1,0 +1,929 @@
+// Dense solvers for G psi = H phi (Simulation::solve_system, Bem/Simulation/Simulation.cpp:40-71).
+//
+//   * BiCGSTAB (the reference default, Simulation.hpp:38): Jacobi preconditioner, zero start,
+//     tolerance DBL_EPSILON on the recursive residual, at most 2N iterations, restart of the shadow
+//     residual when rho vanishes -- the documented Eigen 3.4 BiCGSTAB<MatrixXd> behaviour.  All
+//     scalars live on the device; the host only polls the done flag every few iterations.
+//   * LU with row partial pivoting (PartialPivLU): right-looking blocked factorisation in FP64.
+//   * MIXED: FP64 GMRES on G, right-preconditioned by an FP32 approximate inverse X ~ G^-1 kept
+//     across stages and steps and refreshed by Newton-Schulz (X <- X(2I - G X)) when the Krylov
+//     iteration count grows.  The answer is the FP64 G's solution to the relative residual
+//     `mixed_tol` (checked on the true residual), whatever the quality of X.
+//
+// GEMV on the column-major N x N matrices is HBM-bound: a 2-D grid (row blocks x column splits),
+// fixed-order reduction of the column-split partials by the last CTA of each row block.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "ctx.h"
+
+namespace bemb {
+
+constexpr int GV_ROWS = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum n partials in a fixed order; result valid in every thread of the block.
+__device__ double block_reduce_partials(const double* __restrict__ p, int n) {
+    __shared__ double s_out;
+    if (threadIdx.x < 32) {
+        double a = 0.0;
+        for (int k = threadIdx.x; k < n; k += 32) a += p[k];
+        a = warp_sum(a);
+        if (threadIdx.x == 0) s_out = a;
+    }
+    __syncthreads();
+    double r = s_out;
+    __syncthreads();
+    return r;
+}
+
+// Deterministic block sum of per-thread values (blockDim.x a multiple of 32, <= 1024).
+__device__ double block_sum(double v) {
+    __shared__ double s_w[32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s_w[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = (lane < (int)(blockDim.x >> 5)) ? s_w[lane] : 0.0;
+        r = warp_sum(r);
+        if (lane == 0) s_w[0] = r;
+    }
+    __syncthreads();
+    r = s_w[0];
+    __syncthreads();
+    return r;
+}
+
+// y = A x; A column-major (T = double or float), x and y FP64.  grid (row blocks, column splits).
+// Optional fused dots of the result: d1 = y.u, d2 = y.w partials per row block.
+template <typename T>
+__global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, const T* __restrict__ A, const double* __restrict__ x,
+                                                  double* __restrict__ y, double* __restrict__ part,
+                                                  unsigned* __restrict__ cnt, const int* __restrict__ gate,
+                                                  int gate_val, const double* __restrict__ u,
+                                                  double* __restrict__ du, const double* __restrict__ w,
+                                                  double* __restrict__ dw) {
+    if (gate && *gate != gate_val) return;
+    const int rb = blockIdx.x, cs = blockIdx.y, ncs = gridDim.y;
+    const int i = rb * GV_ROWS + threadIdx.x;
+    const int chunk = (n + ncs - 1) / ncs;
+    const int c0 = cs * chunk, c1 = min(n, c0 + chunk);
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    if (i < n) {
+        const T* col = A + (size_t)c0 * n + i;
+        int j = c0;
+        for (; j + 3 < c1; j += 4) {
+            T a0 = col[0], a1 = col[(size_t)n], a2 = col[2 * (size_t)n], a3 = col[3 * (size_t)n];
+            acc0 = fma((double)a0, __ldg(x + j), acc0);
+            acc1 = fma((double)a1, __ldg(x + j + 1), acc1);
+            acc2 = fma((double)a2, __ldg(x + j + 2), acc2);
+            acc3 = fma((double)a3, __ldg(x + j + 3), acc3);
+            col += 4 * (size_t)n;
+        }
+        for (; j < c1; ++j) {
+            acc0 = fma((double)col[0], __ldg(x + j), acc0);
+            col += n;
+        }
+        part[(size_t)cs * n + i] = (acc0 + acc1) + (acc2 + acc3);
+    }
+    __threadfence();
+    __shared__ unsigned s_ticket;
+    __syncthreads();
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&cnt[rb], 1u);
+    __syncthreads();
+    if (s_ticket != (unsigned)(ncs - 1)) return;
+    // last CTA of this row block: fixed-order sum of the column-split partials
+    __threadfence();
+    double yi = 0.0;
+    if (i < n) {
+        for (int k = 0; k < ncs; ++k) yi += __ldcg(part + (size_t)k * n + i);
+        y[i] = yi;
+    }
+    if (du) {
+        double v = (i < n) ? yi * u[i] : 0.0;
+        v = block_sum(v);
+        if (threadIdx.x == 0) du[rb] = v;
+    }
+    if (dw) {
+        double v = (i < n) ? yi * w[i] : 0.0;
+        v = block_sum(v);
+        if (threadIdx.x == 0) dw[rb] = v;
+    }
+    if (threadIdx.x == 0) cnt[rb] = 0u;
+}
+
+static int gemv_splits(int n) {
+    int rb = (n + GV_ROWS - 1) / GV_ROWS;
+    int cs = std::max(1, std::min(64, (4 * 148 + rb - 1) / rb));
+    cs = std::min(cs, std::max(1, n / 16));
+    return cs;
+}
+
+template <typename T>
+static void gemv_t(int n, const T* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt,
+                   const int* gate = nullptr, int gate_val = 0, const double* u = nullptr, double* du = nullptr,
+                   const double* w = nullptr, double* dw = nullptr) {
+    dim3 grid((n + GV_ROWS - 1) / GV_ROWS, gemv_splits(n));
+    k_gemv<T><<<grid, GV_ROWS, 0, s>>>(n, A, x, y, part, cnt, gate, gate_val, u, du, w, dw);
+}
+
+void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt) {
+    gemv_t<double>((int)n, A, x, y, s, part, cnt);
+}
+
+// ------------------------------------------------------------------------------------------------
+// BiCGSTAB
+// ------------------------------------------------------------------------------------------------
+constexpr double DEPS = 2.220446049250313080847e-16;
+
+// partial-sum slots inside Ctx::red (VBLK each)
+enum { RS_RR = 0, RS_R0R = 1, RS_R0V = 2, RS_TT = 3, RS_TS = 4, RS_BB = 5, RS_N = 6 };
+
+__global__ void k_bicg_init(int n, const double* __restrict__ A, const double* __restrict__ b,
+                            double* __restrict__ x, double* __restrict__ r, double* __restrict__ r0,
+                            double* __restrict__ p, double* __restrict__ v, double* __restrict__ invd,
+                            double* __restrict__ red) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = A[(size_t)i * n + i];
+        invd[i] = (d != 0.0) ? 1.0 / d : 1.0;
+        x[i] = 0.0;
+        r[i] = b[i];
+        r0[i] = b[i];
+        p[i] = 0.0;
+        v[i] = 0.0;
+        s += b[i] * b[i];
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) {
+        red[RS_BB * VBLK + blockIdx.x] = s;
+        red[RS_RR * VBLK + blockIdx.x] = s;
+        red[RS_R0R * VBLK + blockIdx.x] = s;
+    }
+}
+
+__global__ void k_bicg_init_scalars(DevScalars* sc, const double* __restrict__ red, int maxit) {
+    double bb = block_reduce_partials(red + RS_BB * VBLK, VBLK);
+    if (threadIdx.x == 0) {
+        sc->rhs_sq = bb;
+        sc->r0_sq = bb;
+        sc->rho = 1.0;
+        sc->alpha = 1.0;
+        sc->w = 1.0;
+        sc->tol2 = DEPS * DEPS * bb;
+        sc->iters = 0;
+        sc->restarts = 0;
+        sc->done = (bb == 0.0) ? 1 : 0;
+        sc->restart_flag = 0;
+        sc->maxit = maxit;
+        sc->nonconv = 0;
+    }
+}
+
+// Loop test, rho, restart decision and beta (one CTA).
+__global__ void k_bicg_begin(DevScalars* sc, const double* __restrict__ red) {
+    double rr = block_reduce_partials(red + RS_RR * VBLK, VBLK);
+    double r0r = block_reduce_partials(red + RS_R0R * VBLK, VBLK);
+    if (threadIdx.x != 0 || sc->done) return;
+    sc->rr = rr;
+    if (!(rr > sc->tol2) || sc->iters >= sc->maxit) {
+        sc->done = 1;
+        sc->nonconv = (rr > sc->tol2) ? 1 : 0;
+        return;
+    }
+    double rho_old = sc->rho;
+    sc->beta = rho_old;  // kept for the restart path
+    if (fabs(r0r) < DEPS * DEPS * sc->r0_sq) {
+        sc->restart_flag = 1;
+        return;
+    }
+    sc->restart_flag = 0;
+    sc->rho = r0r;
+    sc->beta = (r0r / rho_old) * (sc->alpha / sc->w);
+}
+
+// restart: r = b - t (t = A x), r0 = r, partial r.r
+__global__ void k_bicg_restart_update(int n, const DevScalars* sc, const double* __restrict__ b,
+                                      const double* __restrict__ t, double* __restrict__ r, double* __restrict__ r0,
+                                      double* __restrict__ red) {
+    if (sc->done || !sc->restart_flag) return;
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double ri = b[i] - t[i];
+        r[i] = ri;
+        r0[i] = ri;
+        s += ri * ri;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) red[RS_RR * VBLK + blockIdx.x] = s;
+}
+
+__global__ void k_bicg_restart_scalars(DevScalars* sc, const double* __restrict__ red) {
+    double rr = block_reduce_partials(red + RS_RR * VBLK, VBLK);
+    if (threadIdx.x != 0 || sc->done || !sc->restart_flag) return;
+    double rho_old = sc->beta;
+    sc->rho = rr;
+    sc->r0_sq = rr;
+    if (sc->restarts++ == 0) sc->iters = 0;
+    sc->beta = (rr / rho_old) * (sc->alpha / sc->w);
+    sc->restart_flag = 0;
+}
+
+// p = r + beta (p - w v); y = invd .* p
+__global__ void k_bicg_p(int n, const DevScalars* sc, const double* __restrict__ r, double* __restrict__ p,
+                         const double* __restrict__ v, const double* __restrict__ invd, double* __restrict__ y) {
+    if (sc->done) return;
+    const double beta = sc->beta, w = sc->w;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double pi = r[i] + beta * (p[i] - w * v[i]);
+        p[i] = pi;
+        y[i] = invd[i] * pi;
+    }
+}
+
+// alpha = rho / (r0 . v); s = r - alpha v; z = invd .* s
+__global__ void k_bicg_s(int n, int nrb, DevScalars* sc, const double* __restrict__ red_r0v,
+                         const double* __restrict__ r, const double* __restrict__ v, const double* __restrict__ invd,
+                         double* __restrict__ s, double* __restrict__ z) {
+    if (sc->done) return;
+    double r0v = block_reduce_partials(red_r0v, nrb);
+    const double alpha = sc->rho / r0v;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->alpha = alpha;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double si = r[i] - alpha * v[i];
+        s[i] = si;
+        z[i] = invd[i] * si;
+    }
+}
+
+// w = (t.s)/(t.t); x += alpha y + w z; r = s - w t; partials r.r and r0.r; iteration count
+__global__ void k_bicg_xr(int n, int nrb, DevScalars* sc, const double* __restrict__ red_tt,
+                          const double* __restrict__ red_ts, const double* __restrict__ y,
+                          const double* __restrict__ z, const double* __restrict__ s, const double* __restrict__ t,
+                          const double* __restrict__ r0, double* __restrict__ x, double* __restrict__ r,
+                          double* __restrict__ red) {
+    if (sc->done) return;
+    double tt = block_reduce_partials(red_tt, nrb);
+    double ts = block_reduce_partials(red_ts, nrb);
+    const double w = (tt > 0.0) ? ts / tt : 0.0;
+    const double alpha = sc->alpha;
+    double a = 0.0, b = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] += alpha * y[i] + w * z[i];
+        double ri = s[i] - w * t[i];
+        r[i] = ri;
+        a += ri * ri;
+        b += r0[i] * ri;
+    }
+    a = block_sum(a);
+    b = block_sum(b);
+    if (threadIdx.x == 0) {
+        red[RS_RR * VBLK + blockIdx.x] = a;
+        red[RS_R0R * VBLK + blockIdx.x] = b;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->w = w;
+        sc->iters += 1;
+    }
+}
+
+int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
+    double* red = c.red;
+    // GEMV dot partial slots (one per row block) after the VBLK-sized vector slots
+    double* g_r0v = red + RS_N * VBLK;
+    double* g_tt = g_r0v + nrb;
+    double* g_ts = g_tt + nrb;
+    const int maxit = c.prm.max_iters > 0 ? c.prm.max_iters : 2 * n;
+    k_bicg_init<<<VBLK, VTHR, 0, s>>>(n, A, b, x, c.r, c.r0, c.pv, c.vv, c.invd, red);
+    k_bicg_init_scalars<<<1, 32, 0, s>>>(c.sc, red, maxit);
+    int* done_dev = &c.sc->done;
+    int* rflag_dev = &c.sc->restart_flag;
+    const int batch = 4;
+    for (int it0 = 0;; it0 += batch) {
+        for (int k = 0; k < batch; ++k) {
+            k_bicg_begin<<<1, 32, 0, s>>>(c.sc, red);
+            // restart path (inactive unless the flag is set)
+            gemv_t<double>(n, A, x, c.tv, s, c.part, c.cnt, rflag_dev, 1);
+            k_bicg_restart_update<<<VBLK, VTHR, 0, s>>>(n, c.sc, b, c.tv, c.r, c.r0, red);
+            k_bicg_restart_scalars<<<1, 32, 0, s>>>(c.sc, red);
+            k_bicg_p<<<VBLK, VTHR, 0, s>>>(n, c.sc, c.r, c.pv, c.vv, c.invd, c.yv);
+            gemv_t<double>(n, A, c.yv, c.vv, s, c.part, c.cnt, done_dev, 0, c.r0, g_r0v);
+            k_bicg_s<<<VBLK, VTHR, 0, s>>>(n, nrb, c.sc, g_r0v, c.r, c.vv, c.invd, c.sv, c.zv);
+            gemv_t<double>(n, A, c.zv, c.tv, s, c.part, c.cnt, done_dev, 0, c.tv, g_tt, c.sv, g_ts);
+            k_bicg_xr<<<VBLK, VTHR, 0, s>>>(n, nrb, c.sc, g_tt, g_ts, c.yv, c.zv, c.sv, c.tv, c.r0, x, c.r, red);
+        }
+        BEM_CUDA(c, cudaMemcpyAsync(c.h_sc, c.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+        BEM_CUDA(c, cudaStreamSynchronize(s));
+        if (c.h_sc->done) break;
+        if (it0 > 4 * maxit + 64) return c.fail(BEM_ERR_NOT_CONVERGED, "BiCGSTAB: loop guard");
+    }
+    c.stats.last_iters = c.h_sc->iters;
+    c.stats.last_rel_residual = c.h_sc->rhs_sq > 0 ? sqrt(c.h_sc->rr / c.h_sc->rhs_sq) : 0.0;
+    c.stats.solves++;
+    return BEM_OK;
+}
+
+
+// ------------------------------------------------------------------------------------------------
+// LU with row partial pivoting (FP64), right-looking, panel width LU_NB
+// ------------------------------------------------------------------------------------------------
+constexpr int LU_NB = 64;
+
+// Panel factorisation of columns [k0, k0+nb), rows [k0, n), one CTA: pivot search (largest
+// |entry|, first row on ties), row swap inside the panel, column scaling, rank-1 panel update.
+__global__ void __launch_bounds__(1024) k_lu_panel(int n, int k0, int nb, double* __restrict__ A,
+                                                   int* __restrict__ piv, int* __restrict__ sing) {
+    __shared__ double s_v[32];
+    __shared__ int s_i[32];
+    __shared__ int s_p;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int j = k0; j < k0 + nb; ++j) {
+        double best = -1.0;
+        int bi = n;
+        for (int i = j + tid; i < n; i += blockDim.x) {
+            double v = fabs(A[(size_t)j * n + i]);
+            if (v > best) {
+                best = v;
+                bi = i;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            s_v[wid] = best;
+            s_i[wid] = bi;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            best = (lane < (int)(blockDim.x >> 5)) ? s_v[lane] : -2.0;
+            bi = (lane < (int)(blockDim.x >> 5)) ? s_i[lane] : n;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (lane == 0) s_p = (bi < n) ? bi : j;
+        }
+        __syncthreads();
+        const int p = s_p;
+        if (tid == 0) piv[j] = p;
+        if (p != j)
+            for (int c = k0 + tid; c < k0 + nb; c += blockDim.x) {
+                double t = A[(size_t)c * n + j];
+                A[(size_t)c * n + j] = A[(size_t)c * n + p];
+                A[(size_t)c * n + p] = t;
+            }
+        __syncthreads();
+        const double d = A[(size_t)j * n + j];
+        if (d != 0.0) {
+            for (int i = j + 1 + tid; i < n; i += blockDim.x) A[(size_t)j * n + i] /= d;
+        } else if (tid == 0) {
+            *sing = 1;
+        }
+        __syncthreads();
+        const int ncols = k0 + nb - j - 1, nrows = n - j - 1;
+        for (int e = tid; e < ncols * nrows; e += blockDim.x) {
+            int cc = e / nrows, rr = e - cc * nrows;
+            int c = j + 1 + cc, i = j + 1 + rr;
+            A[(size_t)c * n + i] -= A[(size_t)j * n + i] * A[(size_t)c * n + j];
+        }
+        __syncthreads();
+    }
+}
+
+// Apply the panel's row interchanges to every column outside the panel.
+__global__ void k_lu_laswp(int n, int k0, int nb, double* __restrict__ A, const int* __restrict__ piv) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || (c >= k0 && c < k0 + nb)) return;
+    double* col = A + (size_t)c * n;
+    for (int j = k0; j < k0 + nb; ++j) {
+        int p = piv[j];
+        if (p != j) {
+            double t = col[j];
+            col[j] = col[p];
+            col[p] = t;
+        }
+    }
+}
+
+// U12 = L11^-1 A12: one warp per column right of the panel, two panel rows per lane.
+__global__ void k_lu_trsm(int n, int k0, int nb, double* __restrict__ A) {
+    __shared__ double L[LU_NB][LU_NB + 1];
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+        int r = e % nb, c = e / nb;
+        L[r][c] = A[(size_t)(k0 + c) * n + k0 + r];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int col = k0 + nb + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (col >= n) return;
+    double* a = A + (size_t)col * n + k0;
+    double v0 = (lane < nb) ? a[lane] : 0.0, v1 = (lane + 32 < nb) ? a[lane + 32] : 0.0;
+    for (int k = 0; k < nb; ++k) {
+        double xk = (k < 32) ? __shfl_sync(0xffffffffu, v0, k) : __shfl_sync(0xffffffffu, v1, k - 32);
+        if (lane > k && lane < nb) v0 -= L[lane][k] * xk;
+        if (lane + 32 > k && lane + 32 < nb) v1 -= L[lane + 32][k] * xk;
+    }
+    if (lane < nb) a[lane] = v0;
+    if (lane + 32 < nb) a[lane + 32] = v1;
+}
+
+// A22 -= L21 * U12 with 64x64 output tiles, K = nb <= 64 in chunks of 32, FP64 FMA (SIMT).
+__global__ void __launch_bounds__(256) k_lu_gemm(int n, int k0, int nb, double* __restrict__ A) {
+    __shared__ double sa[32][64 + 1];  // [k][row]
+    __shared__ double sb[32][64 + 1];  // [k][col]
+    const int r0 = k0 + nb + blockIdx.x * 64, c0 = k0 + nb + blockIdx.y * 64;
+    const int tid = threadIdx.x;
+    const int tr = (tid % 16) * 4, tc = (tid / 16) * 4;
+    double acc[4][4] = {};
+    for (int kc = 0; kc < nb; kc += 32) {
+        const int kn = min(32, nb - kc);
+        __syncthreads();
+        for (int e = tid; e < kn * 64; e += 256) {
+            int k = e / 64, r = e % 64;
+            int gr = r0 + r;
+            sa[k][r] = (gr < n) ? A[(size_t)(k0 + kc + k) * n + gr] : 0.0;
+            int gc = c0 + r;
+            sb[k][r] = (gc < n) ? A[(size_t)gc * n + k0 + kc + k] : 0.0;
+        }
+        __syncthreads();
+        for (int k = 0; k < kn; ++k) {
+            double a[4], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[q] = sa[k][tr + q];
+                b[q] = sb[k][tc + q];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+#pragma unroll
+                for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+        }
+    }
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+        int gc = c0 + tc + y;
+        if (gc >= n) continue;
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+            int gr = r0 + tr + x;
+            if (gr < n) A[(size_t)gc * n + gr] -= acc[x][y];
+        }
+    }
+}
+
+// x = P b (the recorded interchanges in order), then L y = x (unit lower), U x = y; one CTA,
+// x kept in shared memory when it fits.
+__global__ void __launch_bounds__(1024) k_lu_substitute(int n, const double* __restrict__ A,
+                                                        const int* __restrict__ piv, const double* __restrict__ b,
+                                                        double* __restrict__ x) {
+    extern __shared__ double sx[];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n; i += blockDim.x) sx[i] = b[i];
+    __syncthreads();
+    if (tid == 0)
+        for (int j = 0; j < n; ++j) {
+            int p = piv[j];
+            if (p != j) {
+                double t = sx[j];
+                sx[j] = sx[p];
+                sx[p] = t;
+            }
+        }
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        const double xj = sx[j];
+        if (xj != 0.0)
+            for (int i = j + 1 + tid; i < n; i += blockDim.x) sx[i] -= A[(size_t)j * n + i] * xj;
+        __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; --j) {
+        if (tid == 0) sx[j] /= A[(size_t)j * n + j];
+        __syncthreads();
+        const double xj = sx[j];
+        if (xj != 0.0)
+            for (int i = tid; i < j; i += blockDim.x) sx[i] -= A[(size_t)j * n + i] * xj;
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += blockDim.x) x[i] = sx[i];
+}
+
+int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    if ((size_t)n * sizeof(double) > 200 * 1024)
+        return c.fail(BEM_ERR_ARG, "LU solver: N too large for the single-CTA substitution (N <= 25600)");
+    BEM_CUDA(c, cudaMemcpyAsync(c.LU, A, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s));
+    BEM_CUDA(c, cudaMemsetAsync(c.flag, 0, sizeof(int), s));
+    for (int k0 = 0; k0 < n; k0 += LU_NB) {
+        const int nb = std::min(LU_NB, n - k0);
+        k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
+        k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
+        const int rest = n - k0 - nb;
+        if (rest > 0) {
+            k_lu_trsm<<<(rest + 7) / 8, 256, 0, s>>>(n, k0, nb, c.LU);
+            dim3 g((rest + 63) / 64, (rest + 63) / 64);
+            k_lu_gemm<<<g, 256, 0, s>>>(n, k0, nb, c.LU);
+        }
+    }
+    size_t sm = sizeof(double) * (size_t)n;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_lu_substitute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+    }
+    k_lu_substitute<<<1, 1024, sm, s>>>(n, c.LU, c.piv, b, x);
+    int sing = 0;
+    BEM_CUDA(c, cudaMemcpyAsync(&sing, c.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    c.stats.solves++;
+    c.stats.last_iters = 0;
+    if (sing) return c.fail(BEM_ERR_SINGULAR, "LU: zero pivot (singular G)");
+    return BEM_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// MIXED: FP64 GMRES right-preconditioned by an FP32 approximate inverse X, Newton-Schulz refresh
+// ------------------------------------------------------------------------------------------------
+
+__global__ void k_to_f32(int64_t nn, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// |G| column sums (norm-1 candidates) and row sums (norm-inf candidates)
+__global__ void k_abs_colsum(int n, const double* __restrict__ A, double* __restrict__ cs) {
+    int j = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += fabs(A[(size_t)j * n + i]);
+    s = block_sum(s);
+    if (threadIdx.x == 0) cs[j] = s;
+}
+__global__ void k_abs_rowsum(int n, const double* __restrict__ A, double* __restrict__ rs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += fabs(A[(size_t)j * n + i]);
+    rs[i] = s;
+}
+__global__ void k_max_two(int n, const double* __restrict__ a, const double* __restrict__ b, double* out) {
+    __shared__ double sa[1024], sb[1024];
+    double ma = 0.0, mb = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        ma = fmax(ma, a[i]);
+        mb = fmax(mb, b[i]);
+    }
+    sa[threadIdx.x] = ma;
+    sb[threadIdx.x] = mb;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sa[threadIdx.x] = fmax(sa[threadIdx.x], sa[threadIdx.x + w]);
+            sb[threadIdx.x] = fmax(sb[threadIdx.x], sb[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = 1.0 / (sa[0] * sb[0]);
+}
+// X0 = alpha * G^T (FP32), the classical Newton-Schulz start (Ben-Israel & Cohen 1966)
+__global__ void k_scaled_transpose(int n, const double* __restrict__ A, const double* __restrict__ alpha,
+                                   float* __restrict__ X) {
+    __shared__ double tile[32][33];
+    int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        int i = bx + threadIdx.x, j = by + k;
+        tile[k][threadIdx.x] = (i < n && j < n) ? A[(size_t)j * n + i] : 0.0;
+    }
+    __syncthreads();
+    const double a = *alpha;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        int i = by + threadIdx.x, j = bx + k;  // X(i,j) = G(j,i)
+        if (i < n && j < n) X[(size_t)j * n + i] = (float)(a * tile[threadIdx.x][k]);
+    }
+}
+
+// C = A * B, N x N column-major FP32, SIMT tiles 128x128x8, 8x8 per thread.
+__global__ void __launch_bounds__(256) k_sgemm(int n, const float* __restrict__ A, const float* __restrict__ B,
+                                               float* __restrict__ C) {
+    __shared__ float As[8][128];
+    __shared__ float Bs[8][128];
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * 128, j0 = blockIdx.y * 128;
+    const int tx = tid % 16, ty = tid / 16;
+    float acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = 0.f;
+    for (int k0 = 0; k0 < n; k0 += 8) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            int idx = tid + 256 * e;  // 0..1023
+            int r = idx % 128, k = idx / 128;
+            int gi = i0 + r, gk = k0 + k;
+            As[k][r] = (gi < n && gk < n) ? A[(size_t)gk * n + gi] : 0.f;
+            int kk = idx % 8, c = idx / 8;
+            int gj = j0 + c, gk2 = k0 + kk;
+            Bs[kk][c] = (gj < n && gk2 < n) ? B[(size_t)gj * n + gk2] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float a[8], b[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                a[q] = As[k][tx + 16 * q];
+                b[q] = Bs[k][ty + 16 * q];
+            }
+#pragma unroll
+            for (int x = 0; x < 8; ++x)
+#pragma unroll
+                for (int y = 0; y < 8; ++y) acc[x][y] = fmaf(a[x], b[y], acc[x][y]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int y = 0; y < 8; ++y) {
+        int gj = j0 + ty + 16 * y;
+        if (gj >= n) continue;
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+            int gi = i0 + tx + 16 * x;
+            if (gi < n) C[(size_t)gj * n + gi] = acc[x][y];
+        }
+    }
+}
+
+// Xn = 2 X - P ; and partial ||I - T||_F^2 of the T = G X just used
+__global__ void k_ns_combine(int64_t nn, const float* __restrict__ X, const float* __restrict__ P,
+                             float* __restrict__ Xn) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x)
+        Xn[i] = 2.f * X[i] - P[i];
+}
+__global__ void k_eye_resid(int n, const float* __restrict__ T, double* __restrict__ part) {
+    double s = 0.0;
+    const int64_t nn = (int64_t)n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t j = e / n, i = e - j * n;
+        double d = (i == j ? 1.0 : 0.0) - (double)T[e];
+        s += d * d;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+__global__ void k_sum_partials(const double* __restrict__ p, int np, double* out) {
+    double v = block_reduce_partials(p, np);
+    if (threadIdx.x == 0) *out = v;
+}
+
+static void sgemm(int n, const float* A, const float* B, float* C, cudaStream_t s) {
+    dim3 g((n + 127) / 128, (n + 127) / 128);
+    k_sgemm<<<g, 256, 0, s>>>(n, A, B, C);
+}
+
+// One Newton-Schulz step X <- X (2I - G X); returns ||I - G X_old||_F / sqrt(n) (host value).
+static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
+    const int n = (int)c.topo.N;
+    const int64_t nn = (int64_t)n * n;
+    sgemm(n, c.G32, c.Xinv, c.Tw, s);  // T = G X
+    k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
+    k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
+    float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
+    sgemm(n, c.Xinv, c.Tw, P, s);      // P = X T
+    k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
+    double v = 0.0;
+    BEM_CUDA(c, cudaMemcpyAsync(&v, c.red + VBLK, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    *eres = sqrt(v / n);
+    return BEM_OK;
+}
+
+static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_scratch) {
+    const int n = (int)c.topo.N;
+    const int64_t nn = (int64_t)n * n;
+    k_to_f32<<<4 * 148, 256, 0, s>>>(nn, A, c.G32);
+    if (from_scratch || !c.xinv_valid) {
+        double* cs = c.red + 2 * VBLK;  // scratch of size >= 2n is not guaranteed here: use r/r0
+        k_abs_colsum<<<n, 256, 0, s>>>(n, A, c.r);
+        k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, A, c.r0);
+        k_max_two<<<1, 1024, 0, s>>>(n, c.r, c.r0, cs);
+        dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
+        k_scaled_transpose<<<tg, tb, 0, s>>>(n, A, cs, c.Xinv);
+        double e = 1.0;
+        int it = 0;
+        for (; it < 60; ++it) {
+            int rc = ns_step(c, s, &e);
+            if (rc) return rc;
+            if (e < 1e-4) break;
+        }
+        c.xinv_valid = true;
+    } else {
+        double e = 0.0;
+        int rc = ns_step(c, s, &e);
+        if (rc) return rc;
+        if (!(e < 0.9)) {  // diverging (stale X too far off): start over
+            c.xinv_valid = false;
+            return refresh_inverse(c, A, s, true);
+        }
+    }
+    c.stats.precond_refresh++;
+    return BEM_OK;
+}
+
+// h[k] partials of V_k . w for k <= j (one partial per block per k)
+__global__ void k_multidot(int n, int nv, const double* __restrict__ V, const double* __restrict__ w,
+                           double* __restrict__ part) {
+    for (int k = 0; k < nv; ++k) {
+        double s = 0.0;
+        const double* v = V + (size_t)k * n;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i] * w[i];
+        s = block_sum(s);
+        if (threadIdx.x == 0) part[k * VBLK + blockIdx.x] = s;
+    }
+}
+// h[k] (+)= sum of partials, one warp per k
+__global__ void k_multidot_final(int nv, const double* __restrict__ part, double* __restrict__ h, int accumulate) {
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k >= nv) return;
+    double a = 0.0;
+    for (int b = lane; b < VBLK; b += 32) a += part[k * VBLK + b];
+    a = warp_sum(a);
+    if (lane == 0) h[k] = accumulate ? h[k] + a : a;
+}
+// w -= sum_k V_k h[k]; partial ||w||^2 (slot nv*VBLK)
+__global__ void k_orth_update(int n, int nv, const double* __restrict__ V, const double* __restrict__ h,
+                              double* __restrict__ w, double* __restrict__ part) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double wi = w[i];
+        for (int k = 0; k < nv; ++k) wi -= V[(size_t)k * n + i] * h[k];
+        w[i] = wi;
+        s += wi * wi;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+// hn = sqrt(sum partials); V_next = w / hn; h[nv] = hn
+__global__ void k_normalize(int n, const double* __restrict__ part, const double* __restrict__ w,
+                            double* __restrict__ vnext, double* __restrict__ hslot) {
+    double nrm2 = block_reduce_partials(part, VBLK);
+    double hn = sqrt(nrm2);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *hslot = hn;
+    double inv = (hn > 0.0) ? 1.0 / hn : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) vnext[i] = w[i] * inv;
+}
+__global__ void k_scale(int n, const double* __restrict__ a, double f, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * f;
+}
+// x += Z y
+__global__ void k_combine(int n, int k, const double* __restrict__ Z, const double* __restrict__ y,
+                          double* __restrict__ x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = x[i];
+        for (int q = 0; q < k; ++q) s += Z[(size_t)q * n + i] * y[q];
+        x[i] = s;
+    }
+}
+// r = b - t; partial ||r||^2 and ||b||^2
+__global__ void k_resid(int n, const double* __restrict__ b, const double* __restrict__ t, double* __restrict__ r,
+                        double* __restrict__ part) {
+    double s = 0.0, bb = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double ri = b[i] - t[i];
+        r[i] = ri;
+        s += ri * ri;
+        bb += b[i] * b[i];
+    }
+    s = block_sum(s);
+    bb = block_sum(bb);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        part[VBLK + blockIdx.x] = bb;
+    }
+}
+__global__ void k_resid_final(const double* __restrict__ part, double* out) {
+    double a = block_reduce_partials(part, VBLK);
+    double b = block_reduce_partials(part + VBLK, VBLK);
+    if (threadIdx.x == 0) {
+        out[0] = a;
+        out[1] = b;
+    }
+}
+
+int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    const int m = c.gmres_m;
+    const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
+    if (!c.xinv_valid) {
+        int rc = refresh_inverse(c, A, s, true);
+        if (rc) return rc;
+    }
+    double* hp = c.red;                    // partial slots: up to (m+1)*VBLK
+    double* hh = c.hcol;                   // device h column (m+2)
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), hcol(m + 2);
+    BEM_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+    int total_it = 0;
+    double relres = 1.0;
+    for (int cycle = 0; cycle < 20; ++cycle) {
+        // r = b - G x
+        gemv_t<double>(n, A, x, c.tv, s, c.part, c.cnt);
+        k_resid<<<VBLK, VTHR, 0, s>>>(n, b, c.tv, c.r, hp);
+        k_resid_final<<<1, 32, 0, s>>>(hp, hh);
+        double rb[2];
+        BEM_CUDA(c, cudaMemcpyAsync(rb, hh, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        BEM_CUDA(c, cudaStreamSynchronize(s));
+        const double bnorm = sqrt(rb[1]);
+        const double beta = sqrt(rb[0]);
+        if (bnorm == 0.0) {
+            relres = 0.0;
+            break;
+        }
+        relres = beta / bnorm;
+        if (relres <= tol) break;
+        // V0 = r / beta
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;
+        k_scale<<<VBLK, VTHR, 0, s>>>(n, c.r, 1.0 / beta, c.V);
+        for (int j = 0; j < m; ++j) {
+            double* vj = c.V + (size_t)j * n;
+            double* zj = c.Z + (size_t)j * n;
+            gemv_t<float>(n, c.Xinv, vj, zj, s, c.part, c.cnt);  // z = X v
+            gemv_t<double>(n, A, zj, c.tv, s, c.part, c.cnt);    // w = G z
+            k_multidot<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, c.tv, hp);
+            k_multidot_final<<<1, 32 * (j + 1), 0, s>>>(j + 1, hp, hh, 0);
+            k_orth_update<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, hh, c.tv, hp + (size_t)(m + 1) * VBLK);
+            // second Gram-Schmidt pass (CGS2)
+            k_multidot<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, c.tv, hp);
+            k_multidot_final<<<1, 32 * (j + 1), 0, s>>>(j + 1, hp, hh + (m + 2), 0);
+            k_orth_update<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, hh + (m + 2), c.tv, hp + (size_t)(m + 1) * VBLK);
+            k_normalize<<<VBLK, VTHR, 0, s>>>(n, hp + (size_t)(m + 1) * VBLK, c.tv, c.V + (size_t)(j + 1) * n,
+                                              hh + j + 1);
+            std::vector<double> h2(m + 2);
+            BEM_CUDA(c, cudaMemcpyAsync(hcol.data(), hh, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, s));
+            BEM_CUDA(c, cudaMemcpyAsync(h2.data(), hh + (m + 2), sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
+            BEM_CUDA(c, cudaStreamSynchronize(s));
+            for (int q = 0; q <= j; ++q) hcol[q] += h2[q];
+            // Givens rotations on the new Hessenberg column
+            for (int q = 0; q < j; ++q) {
+                double t = cs[q] * hcol[q] + sn[q] * hcol[q + 1];
+                hcol[q + 1] = -sn[q] * hcol[q] + cs[q] * hcol[q + 1];
+                hcol[q] = t;
+            }
+            double den = hypot(hcol[j], hcol[j + 1]);
+            cs[j] = (den > 0) ? hcol[j] / den : 1.0;
+            sn[j] = (den > 0) ? hcol[j + 1] / den : 0.0;
+            hcol[j] = den;
+            hcol[j + 1] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            for (int q = 0; q <= j; ++q) H[(size_t)q * m + j] = hcol[q];
+            k = j + 1;
+            ++total_it;
+            if (fabs(g[j + 1]) / bnorm <= 0.5 * tol) break;
+        }
+        // y = R^-1 g
+        std::vector<double> y(k);
+        for (int q = k - 1; q >= 0; --q) {
+            double acc = g[q];
+            for (int r = q + 1; r < k; ++r) acc -= H[(size_t)q * m + r] * y[r];
+            y[q] = acc / H[(size_t)q * m + q];
+        }
+        BEM_CUDA(c, cudaMemcpyAsync(hh, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+        k_combine<<<VBLK, VTHR, 0, s>>>(n, k, c.Z, hh, x);
+    }
+    c.stats.solves++;
+    c.stats.last_iters = total_it;
+    c.stats.last_rel_residual = relres;
+    if (relres > tol) return c.fail(BEM_ERR_NOT_CONVERGED, "mixed GMRES did not reach the tolerance");
+    // keep the inverse fresh: refresh when the Krylov iteration count grows
+    if (total_it > 6) {
+        int rc = refresh_inverse(c, A, s, false);
+        if (rc) return rc;
+    }
+    return BEM_OK;
+}
+
+}  // namespace bemb

@@ -1,0 +1,396 @@
+// Per-stage pointwise work of LinLinSim (Bem/Simulation/LinLinSim.cpp) on the device:
+// surface velocities (position_t), Bernoulli Dphi/Dt per bubble (pot_t_multi), vertex normals,
+// adaptive dt, the RK4 / Euler combination and the wall treatment (nopenetration).
+// All O(N) or O(M); memory-bound and tiny next to assembly and solve.
+#include <math.h>
+
+#include "ctx.h"
+
+namespace bemb {
+
+struct d3 {
+    double x, y, z;
+};
+__device__ __forceinline__ d3 ld3(const double* p, int i) { return {p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+__device__ __forceinline__ void st3(double* p, int i, d3 v) {
+    p[3 * i] = v.x;
+    p[3 * i + 1] = v.y;
+    p[3 * i + 2] = v.z;
+}
+__device__ __forceinline__ d3 sub(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 cross(d3 a, d3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// generate_triangle_normals (Mesh.cpp:130-138) and generate_tangent_gradients (LinLinSim.cpp:288-305)
+__global__ void k_velocity_prep(int M, const double* __restrict__ x, const int* __restrict__ tri,
+                                const double* __restrict__ pot, double* __restrict__ tn, double* __restrict__ tg) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    int a = tri[3 * t], b = tri[3 * t + 1], c = tri[3 * t + 2];
+    d3 A = ld3(x, a), B = ld3(x, b), C = ld3(x, c);
+    d3 n = cross(sub(B, A), sub(C, A));
+    double inv = 1.0 / sqrt(dot(n, n));
+    st3(tn, t, {n.x * inv, n.y * inv, n.z * inv});
+    d3 ab = sub(B, A), bc = sub(C, B);
+    d3 m = cross(ab, bc);
+    double i2 = 1.0 / dot(m, m);
+    m = {m.x * i2, m.y * i2, m.z * i2};
+    double s1 = pot[c] - pot[b], s2 = pot[a] - pot[b];
+    d3 u = cross(m, ab), v = cross(m, bc);
+    st3(tg, t, {s1 * u.x + s2 * v.x, s1 * u.y + s2 * v.y, s1 * u.z + s2 * v.z});
+}
+
+// vertex gradient = mean over incident triangles of (tangent gradient + psi_i * normal)
+// (LinLinSim.cpp:48-59)
+__global__ void k_velocity(int N, const int* __restrict__ off, const int* __restrict__ idx,
+                           const double* __restrict__ tn, const double* __restrict__ tg,
+                           const double* __restrict__ psil, double* __restrict__ vel) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double gx = 0, gy = 0, gz = 0, num = 0;
+    const double p = psil[i];
+    for (int e = off[i]; e < off[i + 1]; ++e) {
+        int t = idx[e];
+        gx += tg[3 * t] + p * tn[3 * t];
+        gy += tg[3 * t + 1] + p * tn[3 * t + 1];
+        gz += tg[3 * t + 2] + p * tn[3 * t + 2];
+        num += 1.0;
+    }
+    double s = 1.0 / num;
+    st3(vel, i, {gx * s, gy * s, gz * s});
+}
+
+// Part volumes: one CTA per loose part, fixed-shape tree reduction (Mesh.cpp:206-218).
+__global__ void k_part_volume(const double* __restrict__ x, const int* __restrict__ off,
+                              const int* __restrict__ tidx, const int* __restrict__ ptri, double* __restrict__ vol) {
+    __shared__ double red[256];
+    const int p = blockIdx.x;
+    double acc = 0.0;
+    for (int e = off[p] + threadIdx.x; e < off[p + 1]; e += 256) {
+        const int t = tidx[e];
+        d3 a = ld3(x, ptri[3 * t]), b = ld3(x, ptri[3 * t + 1]), c = ld3(x, ptri[3 * t + 2]);
+        acc += dot(cross(a, b), c) / 6.0;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) vol[p] = red[0];
+}
+
+// potential_t (Simulation.cpp:73-75) per vertex:
+// 2 sigma kappa + |grad|^2/2 + p_inf - epsilon (V0/V_part)^gamma + p_field(x, t_stepstart)
+__global__ void k_pot_t(int N, const double* __restrict__ x, const double* __restrict__ vel,
+                        const int* __restrict__ part, const double* __restrict__ vol,
+                        const double* __restrict__ kap, const double* __restrict__ fieldv,
+                        const DevScalars* __restrict__ sc, double p_inf, double eps_gas, double sigma,
+                        double gamma, double famp, double fkx, double fomega, double fphase, double t_host,
+                        int use_dev_time, double* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    d3 g = ld3(vel, i);
+    double V = vol[part[i]];
+    double t = use_dev_time ? sc->time : t_host;
+    double f;
+    if (fieldv)
+        f = fieldv[i];
+    else
+        f = famp * sin(fkx * x[3 * i] + fomega * t + fphase);
+    double k = kap ? kap[i] : 0.0;
+    out[i] = 2.0 * sigma * k + 0.5 * dot(g, g) + p_inf - eps_gas * pow(sc->V0 / V, gamma) + f;
+}
+
+// Max-1999 vertex normals (Mesh.cpp:141-163)
+__global__ void k_vertex_normals(int N, const double* __restrict__ x, const int* __restrict__ tri,
+                                 const int* __restrict__ off, const int* __restrict__ idx, double* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double nx = 0, ny = 0, nz = 0;
+    for (int e = off[i]; e < off[i + 1]; ++e) {
+        int t = idx[e];
+        int a = tri[3 * t], b = tri[3 * t + 1], c = tri[3 * t + 2];
+        if (i == b) {
+            int o = a;
+            a = b;
+            b = c;
+            c = o;
+        } else if (i == c) {
+            int o = a;
+            a = c;
+            c = b;
+            b = o;
+        }
+        d3 A = ld3(x, a);
+        d3 B = sub(ld3(x, b), A), C = sub(ld3(x, c), A);
+        d3 n = cross(B, C);
+        double s = 1.0 / (dot(B, B) * dot(C, C));
+        nx += n.x * s;
+        ny += n.y * s;
+        nz += n.z * s;
+    }
+    double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+    st3(out, i, {nx * inv, ny * inv, nz * inv});
+}
+
+// out = a + (coef * scale) * k, coef from device memory (the step dt), elementwise.
+__global__ void k_axpy_dev(int64_t n, const double* __restrict__ a, const double* __restrict__ coef, double scale,
+                           const double* __restrict__ k, double* __restrict__ out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = a[i] + (scale * *coef) * k[i];
+}
+
+// RK4 combination, phi update and nopenetration (LinLinSim.cpp:236-253, 162-190).
+// avg = (k1 + 2k2 + 2k3 + k4)/6 is left in k1 for the psi update.
+__global__ void k_rk4_final(int N, const double* __restrict__ x1, double* __restrict__ k1,
+                            const double* __restrict__ k2, const double* __restrict__ k3,
+                            const double* __restrict__ k4, const double* __restrict__ p1,
+                            const double* __restrict__ q1, const double* __restrict__ q2,
+                            const double* __restrict__ q3, const double* __restrict__ q4,
+                            DevScalars* __restrict__ sc, double eps, double* __restrict__ x,
+                            double* __restrict__ phi) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double dt = sc->dt;
+    double av[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        int j = 3 * i + c;
+        av[c] = (((k1[j] + 2.0 * k2[j]) + 2.0 * k3[j]) + k4[j]) * (1.0 / 6.0);
+        x[j] = x1[j] + dt * av[c];
+    }
+    phi[i] = p1[i] + (dt / 6.0) * (((q1[i] + 2.0 * q2[i]) + 2.0 * q3[i]) + q4[i]);
+    double cx = av[0];
+    if (cx * dt < 0.0) {
+        bool flag = false;
+        double xpos = x1[3 * i];
+        if (xpos < eps) {
+            x[3 * i] = xpos * exp(cx / xpos * dt);
+            flag = true;
+        } else {
+            double te = (eps - xpos) / cx;
+            if (fabs(te) < fabs(dt)) {
+                x[3 * i] = eps * exp(cx / eps * (dt - te));
+                flag = true;
+            }
+        }
+        if (flag) av[0] = (x[3 * i] - xpos) / dt;
+    }
+    k1[3 * i] = av[0];
+    k1[3 * i + 1] = av[1];
+    k1[3 * i + 2] = av[2];
+}
+
+__global__ void k_psi_from_avg(int N, const double* __restrict__ avg, const double* __restrict__ vn,
+                               double* __restrict__ psi, DevScalars* __restrict__ sc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) sc->time += sc->dt;
+    if (i >= N) return;
+    psi[i] = avg[3 * i] * vn[3 * i] + avg[3 * i + 1] * vn[3 * i + 1] + avg[3 * i + 2] * vn[3 * i + 2];
+}
+
+__global__ void k_euler_final(int N, const double* __restrict__ vel, const double* __restrict__ potd,
+                              DevScalars* __restrict__ sc, double* __restrict__ x, double* __restrict__ phi) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double dt = sc->dt;
+    if (i < N) {
+        for (int c = 0; c < 3; ++c) x[3 * i + c] = x[3 * i + c] + vel[3 * i + c] * dt;
+        phi[i] = phi[i] + dt * potd[i];
+    }
+}
+
+__global__ void k_euler_time(DevScalars* sc) { sc->time += sc->dt; }
+
+// Simulation::get_dt (Simulation.cpp:77-92): one CTA, deterministic max-reductions.
+__global__ void k_get_dt(int N, const double* __restrict__ vel, const double* __restrict__ potd, double dp,
+                         double dp_balance, double min_dt, DevScalars* __restrict__ sc) {
+    __shared__ double mp[1024], mv[1024];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        a = fmax(fabs(potd[i]), a);
+        d3 v = ld3(vel, i);
+        b = fmax(dot(v, v), b);
+    }
+    mp[threadIdx.x] = a;
+    mv[threadIdx.x] = b;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            mp[threadIdx.x] = fmax(mp[threadIdx.x], mp[threadIdx.x + w]);
+            mv[threadIdx.x] = fmax(mv[threadIdx.x], mv[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double dt = dp / (mp[0] + dp_balance * sqrt(mv[0]));
+        if (min_dt > 0.0) dt = fmin(dt, min_dt);
+        sc->dt = dt;
+    }
+}
+
+__global__ void k_any_negative(int N, const double* __restrict__ x, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N && x[3 * i] < 0.0) *flag = 1;
+}
+
+// Per-triangle curvature tensor (Rusinkiewicz least squares as written in Mesh.cpp:256-319):
+// 6x3 system solved with complete pivoting, mean curvature 0.5*(x0+x2); averaged to vertices.
+__global__ void k_tri_curvature(int M, const double* __restrict__ x, const int* __restrict__ tri,
+                                const double* __restrict__ vn, double* __restrict__ tk) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
+    d3 e0 = sub(ld3(x, ib), ld3(x, ia)), e1 = sub(ld3(x, ic), ld3(x, ib)), e2 = sub(ld3(x, ia), ld3(x, ic));
+    double iu = 1.0 / sqrt(dot(e0, e0));
+    d3 u = {e0.x * iu, e0.y * iu, e0.z * iu};
+    d3 nr = cross(e0, e1);
+    double inr = 1.0 / sqrt(dot(nr, nr));
+    nr = {nr.x * inr, nr.y * inr, nr.z * inr};
+    d3 v = cross(nr, u);
+    double A[6][3] = {{dot(e0, u), dot(e0, v), 0.0}, {0.0, dot(e0, u), dot(e0, v)},
+                      {dot(e1, u), dot(e1, v), 0.0}, {0.0, dot(e1, u), dot(e1, v)},
+                      {dot(e2, u), dot(e2, v), 0.0}, {0.0, dot(e2, u), dot(e2, v)}};
+    d3 na = ld3(vn, ia), nb = ld3(vn, ib), nc = ld3(vn, ic);
+    double rhs[6] = {dot(sub(nb, na), u), dot(sub(nb, na), v), dot(sub(nc, nb), u),
+                     dot(sub(nc, nb), v), dot(sub(na, nc), u), dot(sub(na, nc), v)};
+    int rowp[6] = {0, 1, 2, 3, 4, 5}, colq[3] = {0, 1, 2};
+    int rank = 3;
+    double maxpiv = 0.0;
+    bool degenerate = false;
+    for (int k = 0; k < 3; ++k) {
+        int pr = k, pc = k;
+        double best = -1.0;
+        for (int j = k; j < 3; ++j)
+            for (int i = k; i < 6; ++i) {
+                double a = fabs(A[i][j]);
+                if (a > best) {
+                    best = a;
+                    pr = i;
+                    pc = j;
+                }
+            }
+        if (best == 0.0) {
+            rank = k;
+            degenerate = true;
+            break;
+        }
+        maxpiv = fmax(maxpiv, best);
+        if (pr != k) {
+            for (int j = 0; j < 3; ++j) {
+                double tmp = A[k][j];
+                A[k][j] = A[pr][j];
+                A[pr][j] = tmp;
+            }
+            int tmp = rowp[k];
+            rowp[k] = rowp[pr];
+            rowp[pr] = tmp;
+        }
+        if (pc != k) {
+            for (int i = 0; i < 6; ++i) {
+                double tmp = A[i][k];
+                A[i][k] = A[i][pc];
+                A[i][pc] = tmp;
+            }
+            int tmp = colq[k];
+            colq[k] = colq[pc];
+            colq[pc] = tmp;
+        }
+        double piv = A[k][k];
+        for (int i = k + 1; i < 6; ++i) A[i][k] /= piv;
+        for (int j = k + 1; j < 3; ++j)
+            for (int i = k + 1; i < 6; ++i) A[i][j] -= A[i][k] * A[k][j];
+    }
+    if (!degenerate) {
+        double thr = 2.220446049250313e-16 * 3.0;
+        int r = 0;
+        for (int k = 0; k < 3; ++k)
+            if (fabs(A[k][k]) > thr * maxpiv) ++r;
+        rank = r;
+    }
+    double c[6], sol[3] = {0, 0, 0};
+    for (int i = 0; i < 6; ++i) c[i] = rhs[rowp[i]];
+    for (int j = 0; j < 3; ++j)
+        for (int i = j + 1; i < 3; ++i) c[i] -= A[i][j] * c[j];
+    for (int j = rank - 1; j >= 0; --j) {
+        c[j] /= A[j][j];
+        for (int i = 0; i < j; ++i) c[i] -= A[i][j] * c[j];
+    }
+    for (int i = 0; i < rank; ++i) sol[colq[i]] = c[i];
+    tk[t] = 0.5 * (sol[0] + sol[2]);
+}
+
+__global__ void k_vertex_avg(int N, const int* __restrict__ off, const int* __restrict__ idx,
+                             const double* __restrict__ tk, double* __restrict__ kap) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = 0.0, w = 0.0;
+    for (int e = off[i]; e < off[i + 1]; ++e) {
+        s += tk[idx[e]];
+        w += 1.0;
+    }
+    kap[i] = s / w;
+}
+
+static inline int nb(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s) {
+    k_velocity_prep<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri, pot, c.tn, c.tg);
+}
+void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s) {
+    k_velocity<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tn, c.tg, psil,
+                                                  vel);
+}
+void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s) {
+    k_part_volume<<<c.topo.nparts, 256, 0, s>>>(x, c.topo.part_off, c.topo.part_tidx, c.topo.tri_rot, vol);
+}
+void launch_vertex_normals(Ctx& c, const double* x, double* out, cudaStream_t s) {
+    k_vertex_normals<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, c.topo.tri, c.topo.csr_off,
+                                                        c.topo.csr_idx, out);
+}
+void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s) {
+    // curvatures are computed on the loose parts, whose triangles carry the split's rotation
+    launch_vertex_normals(c, x, c.vn, s);
+    k_tri_curvature<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri_rot, c.vn, c.tk);
+    k_vertex_avg<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tk, kap);
+}
+void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* field_dev, double* out,
+                  cudaStream_t s) {
+    launch_part_volumes(c, x, c.vol, s);
+    const double* kap = nullptr;
+    if (c.prm.sigma != 0.0) {
+        launch_curvature(c, x, c.kap, s);
+        kap = c.kap;
+    }
+    k_pot_t<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, vel, c.topo.part_of_vert, c.vol, kap, field_dev,
+                                               c.sc, c.prm.p_inf, c.prm.epsilon, c.prm.sigma, c.prm.gamma,
+                                               c.prm.field_amp, c.prm.field_kx, c.prm.field_omega,
+                                               c.prm.field_phase, 0.0, 1, out);
+}
+void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k, double* out,
+                  cudaStream_t s) {
+    k_axpy_dev<<<nb(n, 256), 256, 0, s>>>(n, a, coef_dev, scale, k, out);
+}
+void launch_rk4_final(Ctx& c, cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    k_rk4_final<<<nb(N, 128), 128, 0, s>>>(N, c.x1, c.k1, c.k2, c.k3, c.k4, c.p1, c.kp1, c.kp2, c.kp3, c.kp4, c.sc,
+                                           c.prm.nopen_eps, c.x, c.phi);
+    launch_vertex_normals(c, c.x, c.vn, s);
+    k_psi_from_avg<<<nb(N, 128), 128, 0, s>>>(N, c.k1, c.vn, c.psi, c.sc);
+}
+void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    k_euler_final<<<nb(N, 128), 128, 0, s>>>(N, vel, potd, c.sc, c.x, c.phi);
+    k_euler_time<<<1, 1, 0, s>>>(c.sc);
+}
+void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cudaStream_t s) {
+    k_get_dt<<<1, 1024, 0, s>>>((int)c.topo.N, vel, potd, dp, c.prm.dp_balance, c.prm.min_dt, c.sc);
+}
+void launch_any_negative(Ctx& c, const double* x, int* flag, cudaStream_t s) {
+    k_any_negative<<<nb(c.topo.N, 256), 256, 0, s>>>((int)c.topo.N, x, flag);
+}
+
+}  // namespace bemb

@@ -1,0 +1,138 @@
+/* bem_b200 -- C ABI of the B200 (sm_100a) implementation of the bem-bubbles per-step hot path:
+ * collocation influence-matrix assembly, the dense solve for dphi/dn, and the RK4 / Euler update
+ * of vertex positions and surface potential.
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or torch types cross this boundary.
+ * One context owns one simulation state (mesh, phi, psi, time, parameters) resident in GPU memory,
+ * plus all device work buffers.  Calls on one context are serialised by the caller; distinct
+ * contexts may be used from different threads.  Every function returns a bem_status; the text of
+ * the last error of a context is available from bem_last_error().
+ *
+ * Host array layouts follow the reference's containers:
+ *   vertices  N x 3 float64, row-major (std::vector<vec3>, Bem/basic/Bem.hpp:15)
+ *   triangles M x 3 int64   (std::vector<Triplet>, Bem/basic/Triplet.hpp)
+ *   scalars   N float64     (PotVec / Eigen::VectorXd)
+ *   matrices  N x N float64, column-major (Eigen::MatrixXd)
+ */
+#ifndef BEM_B200_H
+#define BEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bem_ctx bem_ctx;
+
+typedef enum {
+    BEM_OK = 0,
+    BEM_ERR_ARG = 1,          /* bad argument (null pointer, size mismatch, index out of range) */
+    BEM_ERR_CUDA = 2,         /* CUDA runtime error */
+    BEM_ERR_NEGATIVE_X = 3,   /* a vertex has x < 0: the reference throws std::out_of_range
+                                 (LinLinSim::test_negative, Bem/Simulation/LinLinSim.cpp:148-159) */
+    BEM_ERR_SINGULAR = 4,     /* zero pivot in the LU factorisation */
+    BEM_ERR_NOT_CONVERGED = 5,/* iterative solver hit its iteration cap above tolerance */
+    BEM_ERR_NOMEM = 6,        /* device allocation failed */
+    BEM_ERR_STATE = 7         /* call order: no mesh set yet */
+} bem_status;
+
+typedef enum {
+    BEM_SOLVER_BICGSTAB = 0,  /* the reference default (Simulation.hpp:38, Simulation.cpp:49-53) */
+    BEM_SOLVER_LU = 1,        /* PartialPivLU (Simulation.cpp:57-60) */
+    BEM_SOLVER_MIXED = 2      /* FP64 GMRES preconditioned by a low-precision inverse of G */
+} bem_solver;
+
+/* Physical and numerical parameters (Simulation ctor, Bem/Simulation/Simulation.hpp:29-54;
+ * LinLinSim ctor, LinLinSim.hpp:22-27).  The far-field pressure of the reference is an arbitrary
+ * function pointer real(*)(vec3 x, real t); here it is the family
+ *     p_field(x, t) = field_amp * sin(field_kx * x.x + field_omega * t + field_phase)
+ * evaluated on the device, or a host callback (bem_set_field_callback). */
+typedef struct {
+    double p_inf;        /* default 1 */
+    double epsilon;      /* gas-pressure coefficient, default 1 */
+    double sigma;        /* surface tension, default 0 */
+    double gamma;        /* polytropic exponent, default 1 */
+    double field_amp, field_kx, field_omega, field_phase;
+    double min_dt;       /* Simulation::set_min_dt, default -1 (off) */
+    double dp_balance;   /* Simulation::set_dp_balance, default 3 */
+    double nopen_eps;    /* LinLinSim::eps (nopenetration wall distance), default 1e-2 */
+    int32_t mirror;      /* image in the wall x = 0 (LinLinSim.hpp:13 MIRROR_MESH) */
+    int32_t solver;      /* bem_solver */
+    double mixed_tol;    /* relative residual target of BEM_SOLVER_MIXED, default 1e-12 */
+    int32_t max_iters;   /* iteration cap for the iterative solvers, 0 = reference default (2N) */
+    int32_t reserved;
+} bem_params;
+
+/* Fill *p with the reference's defaults. */
+void bem_default_params(bem_params* p);
+
+/* Create a context on CUDA device `device`.  Replaces the construction of Bem::ColocSim /
+ * Bem::LinLinSim / Bem::Simulation (ColocSim.hpp:16, LinLinSim.hpp:22, Simulation.hpp:29). */
+int bem_create(bem_ctx** out, int device, const bem_params* p);
+int bem_destroy(bem_ctx* ctx);
+const char* bem_last_error(const bem_ctx* ctx);
+int bem_set_params(bem_ctx* ctx, const bem_params* p);
+int bem_get_params(const bem_ctx* ctx, bem_params* p);
+
+/* Set the mesh (topology + positions).  As in the Simulation ctor, V_0 := volume(mesh),
+ * phi := 0, psi := 0 (Simulation.hpp:42, LinLinSim.hpp:28-29).  Replaces `Mesh mesh` set-up. */
+int bem_set_mesh(bem_ctx* ctx, int64_t n_verts, const double* verts, int64_t n_trigs, const int64_t* trigs);
+int bem_num_verts(const bem_ctx* ctx, int64_t* n);
+/* mesh.verts read/write (public member Simulation::mesh, Simulation.hpp:202) */
+int bem_set_vertices(bem_ctx* ctx, const double* verts);
+int bem_get_vertices(bem_ctx* ctx, double* verts);
+/* set_phi / get_phi / set_psi / get_psi (Simulation.hpp:92-143) */
+int bem_set_phi(bem_ctx* ctx, const double* phi);
+int bem_get_phi(bem_ctx* ctx, double* phi);
+int bem_set_psi(bem_ctx* ctx, const double* psi);
+int bem_get_psi(bem_ctx* ctx, double* psi);
+/* set_time/get_time, set_V_0 (Simulation.hpp:106-126) */
+int bem_set_time(bem_ctx* ctx, double t);
+int bem_get_time(bem_ctx* ctx, double* t);
+int bem_set_V0(bem_ctx* ctx, double v0);
+int bem_get_V0(bem_ctx* ctx, double* v0);
+/* get_volume: volume(mesh) (Simulation.hpp:128-130, Mesh.cpp:206-218) */
+int bem_get_volume(bem_ctx* ctx, double* vol);
+
+/* Host callback form of the reference's pressure-field function pointer (Simulation.hpp:186):
+ * when set, it is evaluated on the host for every vertex at every RK4 stage (positions are copied
+ * back for it), instead of the device-evaluated sine family.  Pass NULL to clear. */
+typedef double (*bem_field_fn)(const double x[3], double t, void* user);
+int bem_set_field_callback(bem_ctx* ctx, bem_field_fn fn, void* user);
+
+/* ColocSim::assemble_matrices (Bem/Simulation/ColocSim.cpp:21-110) for the given vertex positions
+ * (NULL = the context's mesh).  G and H are host N x N column-major outputs; either may be NULL. */
+int bem_assemble(bem_ctx* ctx, const double* verts, double* G, double* H);
+/* Simulation::solve_system (Simulation.cpp:40-71): x = G^{-1} b with the context's solver. */
+int bem_solve_system(bem_ctx* ctx, const double* G, const double* b, double* x);
+/* LinLinSim::position_t (LinLinSim.cpp:26-83): vertex velocities for positions `verts` (NULL = mesh)
+ * and potential `pot`.  psi_l (the solved dphi/dn) may be NULL. */
+int bem_position_t(bem_ctx* ctx, const double* verts, const double* pot, double* vel, double* psi_l);
+/* LinLinSim::pot_t_multi (LinLinSim.cpp:98-120): Dphi/Dt per vertex for positions `verts`
+ * (NULL = mesh), vertex velocities `grads` and time t. */
+int bem_pot_t_multi(bem_ctx* ctx, const double* verts, const double* grads, double t, double* out);
+/* LinLinSim::evolve_system_RK4 (LinLinSim.cpp:194-257) and evolve_system (Euler, :260-284) on the
+ * device-resident state.  fixdt != 0: dt = dp; else the adaptive Simulation::get_dt (Simulation.cpp:77-92).
+ * *dt_out (may be NULL) receives the step taken.  BEM_ERR_NEGATIVE_X mirrors test_negative. */
+int bem_evolve_rk4(bem_ctx* ctx, double dp, int32_t fixdt, double* dt_out);
+int bem_evolve_euler(bem_ctx* ctx, double dp, int32_t fixdt, double* dt_out);
+/* `steps` RK4 steps with fixed dt without host synchronisation in between. */
+int bem_evolve_rk4_n(bem_ctx* ctx, double dt, int32_t steps);
+
+/* Solver statistics of the most recent solve. */
+typedef struct {
+    int64_t solves;           /* solves since creation */
+    int32_t last_iters;       /* iterations of the last iterative solve */
+    int32_t precond_refresh;  /* refreshes of the mixed path's approximate inverse */
+    double last_rel_residual; /* final relative residual of the last iterative solve */
+} bem_stats;
+int bem_get_stats(bem_ctx* ctx, bem_stats* s);
+
+/* Synchronise the context's stream. */
+int bem_sync(bem_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEM_B200_H */

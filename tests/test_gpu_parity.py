@@ -1,0 +1,204 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Small cases compare against the golden vectors produced by the reference's own code
+(tests/golden/ref_cases.npz) and against the oracle (the bit-exact C restatement) on the same
+seeded inputs; full-size cases check size-independent properties (the 4 pi row-sum rule, the
+analytic sphere solution, agreement of the three solvers).
+
+Tolerance: relative error max|gpu - ref| / max|ref| <= 1e-10, the FP64 path's parity bar.  The
+GPU contracts multiply-adds into FMAs and uses the hardware reciprocal square root, so the
+agreement is at the 1e-15 level per entry rather than bit-exact.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from bem_b200 import mesh
+from bem_b200.sim import ColocSim
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_cases.npz"))
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _field():
+    p_inf, eps, sigma, gamma, amp, omega, phase = GOLD["field"]
+    return dict(p_inf=p_inf, epsilon=eps, sigma=sigma, gamma=gamma), (amp, omega, phase)
+
+
+@pytest.mark.parametrize("name", ["one", "two"])
+@pytest.mark.parametrize("mirror", [0, 1])
+def test_assembly_matches_reference(name, mirror):
+    v, f = GOLD[f"{name}_verts"], GOLD[f"{name}_trigs"]
+    sim = ColocSim(v, f, mirror=bool(mirror))
+    G, H = sim.assemble_matrices()
+    assert rel(G, GOLD[f"{name}_G_m{mirror}"]) < 1e-13
+    assert rel(H, GOLD[f"{name}_H_m{mirror}"]) < 1e-13
+
+
+def test_assembly_nu10_matches_oracle_and_is_reproducible():
+    v, f = mesh.bubble(10, 1.0, (2.0, 0.0, 0.0))
+    sim = ColocSim(v, f)
+    G, H = sim.assemble_matrices()
+    G2, H2 = sim.assemble_matrices()
+    assert G.tobytes() == G2.tobytes() and H.tobytes() == H2.tobytes()  # no atomics: bit-reproducible
+    Go, Ho = O.assemble(v, f)
+    assert rel(G, Go) < 1e-13 and rel(H, Ho) < 1e-13
+
+
+def test_assembly_full_size_four_pi_rule():
+    # N = 4002 (icosphere nu=20): sum_j H(i,j) = -4 pi for every row (ColocSim.cpp:85-97)
+    v, f = mesh.bubble(20, 1.0, (2.0, 0.0, 0.0))
+    sim = ColocSim(v, f)
+    G, H = sim.assemble_matrices()
+    assert np.max(np.abs(H.sum(axis=1) + 4 * np.pi)) < 1e-10
+    assert np.all(np.isfinite(G)) and np.all(np.diag(G) > 0)
+
+
+@pytest.mark.parametrize("solver", ["lu", "bicgstab", "mixed"])
+def test_solvers_match_reference(solver):
+    for name in ("one", "two"):
+        v, f, phi = GOLD[f"{name}_verts"], GOLD[f"{name}_trigs"], GOLD[f"{name}_phi"]
+        sim = ColocSim(v, f, solver=solver)
+        G, H = sim.assemble_matrices()
+        x = sim.solve_system(G, H @ phi)
+        assert rel(x, GOLD[f"{name}_psiLU_m0"]) < TOL, solver
+
+
+def test_sphere_known_answer_full_size():
+    # constant phi on a sphere of radius R: dphi/dn -> -phi/R (exterior Dirichlet problem)
+    v, f = mesh.bubble(20, 1.0, (2.0, 0.0, 0.0))
+    sim = ColocSim(v, f, solver="lu")
+    vel, psi = sim.position_t(np.full(len(v), 0.7), return_psi=True)
+    assert abs(psi.mean() + 0.7) < 2e-3
+    sim.set_solver("mixed")
+    _, psi_m = sim.position_t(np.full(len(v), 0.7), return_psi=True)
+    sim.set_solver("bicgstab")
+    _, psi_b = sim.position_t(np.full(len(v), 0.7), return_psi=True)
+    assert rel(psi_m, psi) < 1e-9 and rel(psi_b, psi) < 1e-9
+
+
+def test_position_and_pot_t_match_reference():
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    phys, fld = _field()
+    sim = ColocSim(v, f, pressurefield=fld, solver="lu", **phys)
+    sim.set_V_0(float(GOLD["two_V0"][0]))
+    vel = sim.position_t(phi)
+    assert rel(vel, GOLD["two_vel"]) < TOL
+    assert rel(sim.pot_t_multi(vel, 0.3), GOLD["two_pot_t"]) < TOL
+    sim_s = ColocSim(v, f, pressurefield=fld, solver="lu", **dict(phys, sigma=0.3))
+    sim_s.set_V_0(float(GOLD["two_V0"][0]))
+    assert rel(sim_s.pot_t_multi(vel, 0.3), GOLD["two_pot_t_sigma"]) < TOL
+
+
+def _record(sim):
+    return np.r_[sim.get_vertices().ravel(), sim.get_phi(), sim.get_psi(), sim.get_time()]
+
+
+def test_rk4_fixed_dt_matches_reference():
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    phys, fld = _field()
+    sim = ColocSim(v, f, pressurefield=fld, solver="lu", **phys)
+    sim.set_V_0(float(GOLD["two_V0"][0]))
+    sim.set_phi(phi)
+    for s in range(3):
+        sim.evolve_system_RK4(1e-2, fixdt=True)
+        assert rel(_record(sim), GOLD["two_rk4"][s]) < TOL
+
+
+def test_rk4_adaptive_bicgstab_matches_reference():
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    phys, fld = _field()
+    sim = ColocSim(v, f, pressurefield=fld, solver="bicgstab", **phys)
+    sim.set_V_0(float(GOLD["two_V0"][0]))
+    sim.set_phi(phi)
+    for s in range(2):
+        sim.evolve_system_RK4(0.05, fixdt=False)
+        assert rel(_record(sim), GOLD["two_rk4_adapt"][s]) < TOL
+
+
+def test_rk4_mixed_solver_matches_reference():
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    phys, fld = _field()
+    sim = ColocSim(v, f, pressurefield=fld, solver="mixed", **phys)
+    sim.set_V_0(float(GOLD["two_V0"][0]))
+    sim.set_phi(phi)
+    for s in range(3):
+        sim.evolve_system_RK4(1e-2, fixdt=True)
+        assert rel(_record(sim), GOLD["two_rk4"][s]) < 1e-9
+
+
+def test_euler_matches_reference():
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    phys, fld = _field()
+    sim = ColocSim(v, f, pressurefield=fld, solver="lu", **phys)
+    sim.set_V_0(float(GOLD["two_V0"][0]))
+    sim.set_phi(phi)
+    N = len(v)
+    for s in range(2):
+        sim.evolve_system(1e-2, fixdt=True)
+        got = np.r_[sim.get_vertices().ravel(), sim.get_phi()]
+        assert rel(got, GOLD["two_euler"][s][: 4 * N]) < TOL
+
+
+def test_wall_image_and_nopenetration_match_reference():
+    v, f = GOLD["wall_verts"], GOLD["wall_trigs"]
+    sim = ColocSim(v, f, p_inf=1.0, epsilon=0.0, sigma=0.0, gamma=1.0, solver="lu", mirror=True)
+    sim.set_phi(np.full(len(v), 0.6))
+    for s in range(2):
+        sim.evolve_system_RK4(2e-2, fixdt=True)
+        assert rel(_record(sim), GOLD["wall_rk4"][s]) < TOL
+
+
+def test_config1_shape_matches_reference():
+    a = mesh.bubble(7, 1.0, (2.5, 0, 0))
+    b = mesh.bubble(7, 1.0, (5.5, 0, 0))
+    v, f = mesh.join([a, b])
+    n = len(a[0])
+    phi = np.r_[np.full(n, -0.5), np.full(n, 0.5)]
+    sim = ColocSim(v, f, p_inf=1.0, epsilon=0.0, sigma=0.0, gamma=1.0, solver="lu")
+    sim.set_phi(phi)
+    for s in range(2):
+        sim.evolve_system_RK4(1e-3, fixdt=True)
+        assert rel(_record(sim), GOLD["c1_rk4"][s]) < TOL
+
+
+def test_field_callback_equals_device_field():
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    phys, (amp, omega, phase) = _field()
+    dev = ColocSim(v, f, pressurefield=(amp, omega, phase), solver="lu", **phys)
+    host = ColocSim(v, f, pressurefield=lambda x, t: amp * np.sin(omega * t + phase), solver="lu", **phys)
+    for s in (dev, host):
+        s.set_phi(phi)
+        s.set_time(0.4)
+        s.evolve_system_RK4(1e-2, fixdt=True)
+    assert rel(_record(dev), _record(host)) < 1e-13
+
+
+def test_negative_x_raises_like_reference():
+    v, f = mesh.bubble(2, 1.0, (0.5, 0.0, 0.0))
+    sim = ColocSim(v, f)
+    with pytest.raises(IndexError):
+        sim.evolve_system_RK4(1e-3, fixdt=True)
+
+
+def test_mixed_precision_error_headline_size():
+    # N = 4002 (config 2 mesh with the seeded 1% radial perturbation): psi of the mixed path
+    # against the FP64 LU path at <= 1e-8 relative
+    v, f = mesh.bubble(20, 1.0, (0.0, 0.0, 0.0))
+    rng = np.random.default_rng(0)
+    v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None] + np.array([2.0, 0.0, 0.0])
+    phi = 0.1 * np.sin(3 * v[:, 2])
+    ref = ColocSim(v, f, solver="lu")
+    _, psi_ref = ref.position_t(phi, return_psi=True)
+    mix = ColocSim(v, f, solver="mixed")
+    _, psi_mix = mix.position_t(phi, return_psi=True)
+    assert rel(psi_mix, psi_ref) <= 1e-8
