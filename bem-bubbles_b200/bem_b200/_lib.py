@@ -42,6 +42,11 @@ class Stats(C.Structure):
                 ("last_rel_residual", C.c_double)]
 
 
+class Profile(C.Structure):
+    _fields_ = [("assemble_ms", C.c_double), ("assemble_launches", C.c_int64), ("solve_ms", C.c_double),
+                ("solve_calls", C.c_int64), ("kernel_launches", C.c_int64)]
+
+
 FIELD_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_double, C.c_void_p)
 
 # name -> (restype, argtypes)
@@ -75,6 +80,11 @@ SIGNATURES = {
     "bem_evolve_rk4_n": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "bem_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "bem_sync": (C.c_int, [C.c_void_p]),
+    "bem_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "bem_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
+    "bem_reset_profile": (C.c_int, [C.c_void_p]),
+    "bem_measure_fma_peaks": (C.c_int, [C.c_int, _D, _D]),
+    "bem_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
 }
 
 _lib = None

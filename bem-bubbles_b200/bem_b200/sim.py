@@ -206,3 +206,29 @@ class ColocSim:
 
     def sync(self):
         self._check(self._L.bem_sync(self._h))
+
+    def stream_handle(self) -> int:
+        h = C.c_void_p()
+        self._check(self._L.bem_get_stream(self._h, C.byref(h)))
+        return h.value or 0
+
+    def set_profiling(self, on: bool):
+        self._check(self._L.bem_set_profiling(self._h, int(bool(on))))
+
+    def reset_profile(self):
+        self._check(self._L.bem_reset_profile(self._h))
+
+    def profile(self) -> L.Profile:
+        p = L.Profile()
+        self._check(self._L.bem_get_profile(self._h, C.byref(p)))
+        return p
+
+
+def measure_fma_peaks(device=0):
+    """(FP64, FP32) FMA throughput of `device` in TFLOP/s from the library's FMA-loop kernels."""
+    lib = L.load()
+    a, b = np.zeros(1), np.zeros(1)
+    rc = lib.bem_measure_fma_peaks(int(device), _d(a), _d(b))
+    if rc != L.BEM_OK:
+        raise L.BemError(rc, "bem_measure_fma_peaks failed")
+    return float(a[0]), float(b[0])

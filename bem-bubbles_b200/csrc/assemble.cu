@@ -303,7 +303,7 @@ __global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp,
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
     upload_constants();
     int M = (int)c.topo.M;
-    k_triangle_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, c.topo.tri, c.rec);
+    KLAUNCH(), k_triangle_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, c.topo.tri, c.rec);
 }
 
 static size_t asm_smem() {
@@ -315,13 +315,19 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
     launch_triangle_records(c, x, s);
     dim3 grid(c.topo.ngroups, (N + ASM_ROWS - 1) / ASM_ROWS);
     size_t sm = asm_smem();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c.prof) {
+        e0 = c.take_event();
+        e1 = c.take_event();
+        cudaEventRecord(e0, s);
+    }
     if (c.prm.mirror) {
         static bool attr = false;
         if (!attr) {
             cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             attr = true;
         }
-        k_assemble<true><<<grid, ASM_ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off, c.topo.grp_tri,
+        KLAUNCH(), k_assemble<true><<<grid, ASM_ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off, c.topo.grp_tri,
                                                     c.topo.grp_slot, c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
     } else {
         static bool attr = false;
@@ -329,10 +335,14 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
             cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             attr = true;
         }
-        k_assemble<false><<<grid, ASM_ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off, c.topo.grp_tri,
+        KLAUNCH(), k_assemble<false><<<grid, ASM_ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off, c.topo.grp_tri,
                                                      c.topo.grp_slot, c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
     }
-    k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
+    if (c.prof) {
+        cudaEventRecord(e1, s);
+        c.ev_asm.emplace_back(e0, e1);
+    }
+    KLAUNCH(), k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
 }
 
 }  // namespace bemb

@@ -15,6 +15,8 @@
 
 namespace bemb {
 
+std::atomic<long long> g_kernel_launches{0};
+
 // ---------------------------------------------------------------- device memory helpers
 template <typename T>
 static int dalloc(Ctx& c, T** p, size_t count) {
@@ -182,7 +184,7 @@ __global__ void k_total_volume(const double* vol, int np, double* out) {
 }
 
 // ---------------------------------------------------------------- stage building blocks
-static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+static int solve_impl(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     switch (c.prm.solver) {
         case BEM_SOLVER_LU:
             return lu_solve(c, A, b, x, s);
@@ -191,6 +193,21 @@ static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream
         default:
             return bicgstab(c, A, b, x, s);
     }
+}
+
+static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c.prof) {
+        e0 = c.take_event();
+        e1 = c.take_event();
+        cudaEventRecord(e0, s);
+    }
+    int rc = solve_impl(c, A, b, x, s);
+    if (c.prof) {
+        cudaEventRecord(e1, s);
+        c.ev_solve.emplace_back(e0, e1);
+    }
+    return rc;
 }
 
 // LinLinSim::position_t (LinLinSim.cpp:26-83)
@@ -249,7 +266,7 @@ static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
     if (rc) return rc;
     if ((rc = pot_t_multi(c, c.x1, c.k1, c.kp1, s))) return rc;
     if (fixdt)
-        k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
+        KLAUNCH(), k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
     else
         launch_get_dt(c, c.k1, c.kp1, dp, s);
     const double* dtp = &c.sc->dt;
@@ -274,7 +291,7 @@ static int euler_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
     if (rc) return rc;
     if ((rc = pot_t_multi(c, c.x, c.k1, c.kp1, s))) return rc;
     if (fixdt)
-        k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
+        KLAUNCH(), k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
     else
         launch_get_dt(c, c.k1, c.kp1, dp, s);
     launch_euler_final(c, c.k1, c.kp1, s);
@@ -436,10 +453,10 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     c->have_mesh = true;
     // Simulation ctor: V_0 = volume(initial) (Simulation.hpp:42), time = 0
     cudaStream_t s = c->stream;
-    k_set_time<<<1, 1, 0, s>>>(c->sc, 0.0);
+    KLAUNCH(), k_set_time<<<1, 1, 0, s>>>(c->sc, 0.0);
     launch_part_volumes(*c, c->x, c->vol, s);
-    k_total_volume<<<1, 1, 0, s>>>(c->vol, c->topo.nparts, c->vol + c->topo.nparts);
-    k_copy_vol<<<1, 1, 0, s>>>(c->sc, c->vol + c->topo.nparts);
+    KLAUNCH(), k_total_volume<<<1, 1, 0, s>>>(c->vol, c->topo.nparts, c->vol + c->topo.nparts);
+    KLAUNCH(), k_copy_vol<<<1, 1, 0, s>>>(c->sc, c->vol + c->topo.nparts);
     BEM_CUDA(*c, cudaStreamSynchronize(s));
     return BEM_OK;
 }
@@ -501,7 +518,7 @@ int bem_get_psi(bem_ctx* c, double* v) {
 }
 int bem_set_time(bem_ctx* c, double t) {
     CTX_GUARD(c);
-    k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
+    KLAUNCH(), k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
 }
@@ -512,7 +529,7 @@ int bem_get_time(bem_ctx* c, double* t) {
 }
 int bem_set_V0(bem_ctx* c, double v) {
     CTX_GUARD(c);
-    k_set_V0<<<1, 1, 0, c->stream>>>(c->sc, v);
+    KLAUNCH(), k_set_V0<<<1, 1, 0, c->stream>>>(c->sc, v);
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
 }
@@ -526,7 +543,7 @@ int bem_get_volume(bem_ctx* c, double* vol) {
     NEED_MESH(c);
     // volume(mesh) over the whole mesh in triangle order (Mesh.cpp:206-218)
     launch_part_volumes(*c, c->x, c->vol, c->stream);
-    k_total_volume<<<1, 1, 0, c->stream>>>(c->vol, c->topo.nparts, c->vol + c->topo.nparts);
+    KLAUNCH(), k_total_volume<<<1, 1, 0, c->stream>>>(c->vol, c->topo.nparts, c->vol + c->topo.nparts);
     COPY_OUT(vol, c->vol + c->topo.nparts, 1);
     return BEM_OK;
 }
@@ -600,9 +617,9 @@ int bem_pot_t_multi(bem_ctx* c, const double* verts, const double* grads, double
     COPY_IN(c->k1, grads, 3 * N);
     double t_saved = 0.0;
     COPY_OUT(&t_saved, &c->sc->time, 1);
-    k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
+    KLAUNCH(), k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
     int rc = pot_t_multi(*c, x, c->k1, c->kp1, c->stream);
-    k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t_saved);
+    KLAUNCH(), k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t_saved);
     if (rc) return rc;
     BEM_CUDA(*c, cudaGetLastError());
     COPY_OUT(out, c->kp1, N);
@@ -653,5 +670,116 @@ int bem_sync(bem_ctx* c) {
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
 }
+
+int bem_get_stream(bem_ctx* c, void** stream) {
+    if (!c || !stream) return BEM_ERR_ARG;
+    *stream = (void*)c->stream;
+    return BEM_OK;
+}
+
+static int drain_profile(Ctx& c) {
+    BEM_CUDA(c, cudaStreamSynchronize(c.stream));
+    for (auto& pr : c.ev_asm) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, pr.first, pr.second);
+        c.prof_acc.assemble_ms += ms;
+        c.prof_acc.assemble_launches++;
+        c.ev_pool.push_back(pr.first);
+        c.ev_pool.push_back(pr.second);
+    }
+    for (auto& pr : c.ev_solve) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, pr.first, pr.second);
+        c.prof_acc.solve_ms += ms;
+        c.prof_acc.solve_calls++;
+        c.ev_pool.push_back(pr.first);
+        c.ev_pool.push_back(pr.second);
+    }
+    c.ev_asm.clear();
+    c.ev_solve.clear();
+    return BEM_OK;
+}
+
+int bem_set_profiling(bem_ctx* c, int32_t on) {
+    CTX_GUARD(c);
+    int rc = drain_profile(*c);
+    c->prof = on != 0;
+    return rc;
+}
+
+int bem_reset_profile(bem_ctx* c) {
+    CTX_GUARD(c);
+    int rc = drain_profile(*c);
+    c->prof_acc = bem_profile{};
+    c->launches_at_reset = g_kernel_launches.load();
+    return rc;
+}
+
+int bem_get_profile(bem_ctx* c, bem_profile* out) {
+    CTX_GUARD(c);
+    if (!out) return BEM_ERR_ARG;
+    int rc = drain_profile(*c);
+    *out = c->prof_acc;
+    out->kernel_launches = g_kernel_launches.load() - c->launches_at_reset;
+    return rc;
+}
+
+}  // extern "C"
+
+// FMA-loop throughput kernels for the roofline denominators: 8 independent FMA chains per thread.
+template <typename T>
+__global__ void k_fma_loop(T* out, int iters, T seed) {
+    T a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+      a7 = a0 + 7;
+    const T m = (T)0.999999, k = (T)1e-7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = a0 * m + k;
+            a1 = a1 * m + k;
+            a2 = a2 * m + k;
+            a3 = a3 * m + k;
+            a4 = a4 * m + k;
+            a5 = a5 * m + k;
+            a6 = a6 * m + k;
+            a7 = a7 * m + k;
+        }
+    }
+    T s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (s == (T)-12345) out[0] = s;  // keeps the chains live
+}
+
+template <typename T>
+static double fma_tflops(int sms, int iters) {
+    T* buf = nullptr;
+    cudaMalloc(&buf, sizeof(T));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sms * 8, threads = 256;
+    k_fma_loop<T><<<blocks, threads>>>(buf, 8, (T)1);  // warm-up
+    cudaEventRecord(e0);
+    k_fma_loop<T><<<blocks, threads>>>(buf, iters, (T)1);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    const double fmas = (double)blocks * threads * iters * 16.0 * 8.0;
+    return 2.0 * fmas / (ms * 1e-3) / 1e12;
+}
+
+extern "C" int bem_measure_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops) {
+    if (cudaSetDevice(device) != cudaSuccess) return BEM_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (fp64_tflops) *fp64_tflops = fma_tflops<double>(sms, 4096);
+    if (fp32_tflops) *fp32_tflops = fma_tflops<float>(sms, 8192);
+    return cudaGetLastError() == cudaSuccess ? BEM_OK : BEM_ERR_CUDA;
+}
+
+extern "C" {
 
 }  // extern "C"

@@ -3,6 +3,8 @@
 #pragma once
 
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "internal.h"
 
@@ -69,6 +71,23 @@ struct Ctx {
 
     // statistics
     bem_stats stats{};
+
+    // device-time profiling (CUDA events on the context's stream)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_asm, ev_solve;
+    bem_profile prof_acc{};
+    long long launches_at_reset = 0;
+    cudaEvent_t take_event() {
+        if (ev_pool.empty()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
 
     size_t bytes = 0;
     std::vector<void*> allocs;

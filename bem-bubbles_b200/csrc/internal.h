@@ -5,12 +5,17 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
 #include "../../include/bem_b200.h"
 
 namespace bemb {
+
+// Kernel launches issued by this library (all contexts), for the bench's launch count.
+extern std::atomic<long long> g_kernel_launches;
+#define KLAUNCH() (::bemb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed))
 
 // Column-group width of the assembly tiles: each CTA owns CG columns (vertices) of G and H.
 constexpr int CG = 32;

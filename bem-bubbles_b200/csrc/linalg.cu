@@ -133,7 +133,7 @@ static void gemv_t(int n, const T* A, const double* x, double* y, cudaStream_t s
                    const int* gate = nullptr, int gate_val = 0, const double* u = nullptr, double* du = nullptr,
                    const double* w = nullptr, double* dw = nullptr) {
     dim3 grid((n + GV_ROWS - 1) / GV_ROWS, gemv_splits(n));
-    k_gemv<T><<<grid, GV_ROWS, 0, s>>>(n, A, x, y, part, cnt, gate, gate_val, u, du, w, dw);
+    KLAUNCH(), k_gemv<T><<<grid, GV_ROWS, 0, s>>>(n, A, x, y, part, cnt, gate, gate_val, u, du, w, dw);
 }
 
 void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt) {
@@ -306,23 +306,23 @@ int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
     double* g_tt = g_r0v + nrb;
     double* g_ts = g_tt + nrb;
     const int maxit = c.prm.max_iters > 0 ? c.prm.max_iters : 2 * n;
-    k_bicg_init<<<VBLK, VTHR, 0, s>>>(n, A, b, x, c.r, c.r0, c.pv, c.vv, c.invd, red);
-    k_bicg_init_scalars<<<1, 32, 0, s>>>(c.sc, red, maxit);
+    KLAUNCH(), k_bicg_init<<<VBLK, VTHR, 0, s>>>(n, A, b, x, c.r, c.r0, c.pv, c.vv, c.invd, red);
+    KLAUNCH(), k_bicg_init_scalars<<<1, 32, 0, s>>>(c.sc, red, maxit);
     int* done_dev = &c.sc->done;
     int* rflag_dev = &c.sc->restart_flag;
     const int batch = 4;
     for (int it0 = 0;; it0 += batch) {
         for (int k = 0; k < batch; ++k) {
-            k_bicg_begin<<<1, 32, 0, s>>>(c.sc, red);
+            KLAUNCH(), k_bicg_begin<<<1, 32, 0, s>>>(c.sc, red);
             // restart path (inactive unless the flag is set)
             gemv_t<double>(n, A, x, c.tv, s, c.part, c.cnt, rflag_dev, 1);
-            k_bicg_restart_update<<<VBLK, VTHR, 0, s>>>(n, c.sc, b, c.tv, c.r, c.r0, red);
-            k_bicg_restart_scalars<<<1, 32, 0, s>>>(c.sc, red);
-            k_bicg_p<<<VBLK, VTHR, 0, s>>>(n, c.sc, c.r, c.pv, c.vv, c.invd, c.yv);
+            KLAUNCH(), k_bicg_restart_update<<<VBLK, VTHR, 0, s>>>(n, c.sc, b, c.tv, c.r, c.r0, red);
+            KLAUNCH(), k_bicg_restart_scalars<<<1, 32, 0, s>>>(c.sc, red);
+            KLAUNCH(), k_bicg_p<<<VBLK, VTHR, 0, s>>>(n, c.sc, c.r, c.pv, c.vv, c.invd, c.yv);
             gemv_t<double>(n, A, c.yv, c.vv, s, c.part, c.cnt, done_dev, 0, c.r0, g_r0v);
-            k_bicg_s<<<VBLK, VTHR, 0, s>>>(n, nrb, c.sc, g_r0v, c.r, c.vv, c.invd, c.sv, c.zv);
+            KLAUNCH(), k_bicg_s<<<VBLK, VTHR, 0, s>>>(n, nrb, c.sc, g_r0v, c.r, c.vv, c.invd, c.sv, c.zv);
             gemv_t<double>(n, A, c.zv, c.tv, s, c.part, c.cnt, done_dev, 0, c.tv, g_tt, c.sv, g_ts);
-            k_bicg_xr<<<VBLK, VTHR, 0, s>>>(n, nrb, c.sc, g_tt, g_ts, c.yv, c.zv, c.sv, c.tv, c.r0, x, c.r, red);
+            KLAUNCH(), k_bicg_xr<<<VBLK, VTHR, 0, s>>>(n, nrb, c.sc, g_tt, g_ts, c.yv, c.zv, c.sv, c.tv, c.r0, x, c.r, red);
         }
         BEM_CUDA(c, cudaMemcpyAsync(c.h_sc, c.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
         BEM_CUDA(c, cudaStreamSynchronize(s));
@@ -539,13 +539,13 @@ int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
     BEM_CUDA(c, cudaMemsetAsync(c.flag, 0, sizeof(int), s));
     for (int k0 = 0; k0 < n; k0 += LU_NB) {
         const int nb = std::min(LU_NB, n - k0);
-        k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
-        k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
+        KLAUNCH(), k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
+        KLAUNCH(), k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
         const int rest = n - k0 - nb;
         if (rest > 0) {
-            k_lu_trsm<<<(rest + 7) / 8, 256, 0, s>>>(n, k0, nb, c.LU);
+            KLAUNCH(), k_lu_trsm<<<(rest + 7) / 8, 256, 0, s>>>(n, k0, nb, c.LU);
             dim3 g((rest + 63) / 64, (rest + 63) / 64);
-            k_lu_gemm<<<g, 256, 0, s>>>(n, k0, nb, c.LU);
+            KLAUNCH(), k_lu_gemm<<<g, 256, 0, s>>>(n, k0, nb, c.LU);
         }
     }
     size_t sm = sizeof(double) * (size_t)n;
@@ -554,7 +554,7 @@ int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
         cudaFuncSetAttribute(k_lu_substitute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         attr = true;
     }
-    k_lu_substitute<<<1, 1024, sm, s>>>(n, c.LU, c.piv, b, x);
+    KLAUNCH(), k_lu_substitute<<<1, 1024, sm, s>>>(n, c.LU, c.piv, b, x);
     int sing = 0;
     BEM_CUDA(c, cudaMemcpyAsync(&sing, c.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));
@@ -700,7 +700,7 @@ __global__ void k_sum_partials(const double* __restrict__ p, int np, double* out
 
 static void sgemm(int n, const float* A, const float* B, float* C, cudaStream_t s) {
     dim3 g((n + 127) / 128, (n + 127) / 128);
-    k_sgemm<<<g, 256, 0, s>>>(n, A, B, C);
+    KLAUNCH(), k_sgemm<<<g, 256, 0, s>>>(n, A, B, C);
 }
 
 // One Newton-Schulz step X <- X (2I - G X); returns ||I - G X_old||_F / sqrt(n) (host value).
@@ -708,11 +708,11 @@ static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
     sgemm(n, c.G32, c.Xinv, c.Tw, s);  // T = G X
-    k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
-    k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
+    KLAUNCH(), k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
+    KLAUNCH(), k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
     float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
     sgemm(n, c.Xinv, c.Tw, P, s);      // P = X T
-    k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
+    KLAUNCH(), k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
     double v = 0.0;
     BEM_CUDA(c, cudaMemcpyAsync(&v, c.red + VBLK, sizeof(double), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));
@@ -723,14 +723,14 @@ static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
 static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_scratch) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
-    k_to_f32<<<4 * 148, 256, 0, s>>>(nn, A, c.G32);
+    KLAUNCH(), k_to_f32<<<4 * 148, 256, 0, s>>>(nn, A, c.G32);
     if (from_scratch || !c.xinv_valid) {
         double* cs = c.red + 2 * VBLK;  // scratch of size >= 2n is not guaranteed here: use r/r0
-        k_abs_colsum<<<n, 256, 0, s>>>(n, A, c.r);
-        k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, A, c.r0);
-        k_max_two<<<1, 1024, 0, s>>>(n, c.r, c.r0, cs);
+        KLAUNCH(), k_abs_colsum<<<n, 256, 0, s>>>(n, A, c.r);
+        KLAUNCH(), k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, A, c.r0);
+        KLAUNCH(), k_max_two<<<1, 1024, 0, s>>>(n, c.r, c.r0, cs);
         dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
-        k_scaled_transpose<<<tg, tb, 0, s>>>(n, A, cs, c.Xinv);
+        KLAUNCH(), k_scaled_transpose<<<tg, tb, 0, s>>>(n, A, cs, c.Xinv);
         double e = 1.0;
         int it = 0;
         for (; it < 60; ++it) {
@@ -849,8 +849,8 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     for (int cycle = 0; cycle < 20; ++cycle) {
         // r = b - G x
         gemv_t<double>(n, A, x, c.tv, s, c.part, c.cnt);
-        k_resid<<<VBLK, VTHR, 0, s>>>(n, b, c.tv, c.r, hp);
-        k_resid_final<<<1, 32, 0, s>>>(hp, hh);
+        KLAUNCH(), k_resid<<<VBLK, VTHR, 0, s>>>(n, b, c.tv, c.r, hp);
+        KLAUNCH(), k_resid_final<<<1, 32, 0, s>>>(hp, hh);
         double rb[2];
         BEM_CUDA(c, cudaMemcpyAsync(rb, hh, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
         BEM_CUDA(c, cudaStreamSynchronize(s));
@@ -866,20 +866,20 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int k = 0;
-        k_scale<<<VBLK, VTHR, 0, s>>>(n, c.r, 1.0 / beta, c.V);
+        KLAUNCH(), k_scale<<<VBLK, VTHR, 0, s>>>(n, c.r, 1.0 / beta, c.V);
         for (int j = 0; j < m; ++j) {
             double* vj = c.V + (size_t)j * n;
             double* zj = c.Z + (size_t)j * n;
             gemv_t<float>(n, c.Xinv, vj, zj, s, c.part, c.cnt);  // z = X v
             gemv_t<double>(n, A, zj, c.tv, s, c.part, c.cnt);    // w = G z
-            k_multidot<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, c.tv, hp);
-            k_multidot_final<<<1, 32 * (j + 1), 0, s>>>(j + 1, hp, hh, 0);
-            k_orth_update<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, hh, c.tv, hp + (size_t)(m + 1) * VBLK);
+            KLAUNCH(), k_multidot<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, c.tv, hp);
+            KLAUNCH(), k_multidot_final<<<1, 32 * (j + 1), 0, s>>>(j + 1, hp, hh, 0);
+            KLAUNCH(), k_orth_update<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, hh, c.tv, hp + (size_t)(m + 1) * VBLK);
             // second Gram-Schmidt pass (CGS2)
-            k_multidot<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, c.tv, hp);
-            k_multidot_final<<<1, 32 * (j + 1), 0, s>>>(j + 1, hp, hh + (m + 2), 0);
-            k_orth_update<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, hh + (m + 2), c.tv, hp + (size_t)(m + 1) * VBLK);
-            k_normalize<<<VBLK, VTHR, 0, s>>>(n, hp + (size_t)(m + 1) * VBLK, c.tv, c.V + (size_t)(j + 1) * n,
+            KLAUNCH(), k_multidot<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, c.tv, hp);
+            KLAUNCH(), k_multidot_final<<<1, 32 * (j + 1), 0, s>>>(j + 1, hp, hh + (m + 2), 0);
+            KLAUNCH(), k_orth_update<<<VBLK, VTHR, 0, s>>>(n, j + 1, c.V, hh + (m + 2), c.tv, hp + (size_t)(m + 1) * VBLK);
+            KLAUNCH(), k_normalize<<<VBLK, VTHR, 0, s>>>(n, hp + (size_t)(m + 1) * VBLK, c.tv, c.V + (size_t)(j + 1) * n,
                                               hh + j + 1);
             std::vector<double> h2(m + 2);
             BEM_CUDA(c, cudaMemcpyAsync(hcol.data(), hh, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, s));
@@ -912,7 +912,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
             y[q] = acc / H[(size_t)q * m + q];
         }
         BEM_CUDA(c, cudaMemcpyAsync(hh, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-        k_combine<<<VBLK, VTHR, 0, s>>>(n, k, c.Z, hh, x);
+        KLAUNCH(), k_combine<<<VBLK, VTHR, 0, s>>>(n, k, c.Z, hh, x);
     }
     c.stats.solves++;
     c.stats.last_iters = total_it;

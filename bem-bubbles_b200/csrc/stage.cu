@@ -338,24 +338,24 @@ __global__ void k_vertex_avg(int N, const int* __restrict__ off, const int* __re
 static inline int nb(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s) {
-    k_velocity_prep<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri, pot, c.tn, c.tg);
+    KLAUNCH(), k_velocity_prep<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri, pot, c.tn, c.tg);
 }
 void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s) {
-    k_velocity<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tn, c.tg, psil,
+    KLAUNCH(), k_velocity<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tn, c.tg, psil,
                                                   vel);
 }
 void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s) {
-    k_part_volume<<<c.topo.nparts, 256, 0, s>>>(x, c.topo.part_off, c.topo.part_tidx, c.topo.tri_rot, vol);
+    KLAUNCH(), k_part_volume<<<c.topo.nparts, 256, 0, s>>>(x, c.topo.part_off, c.topo.part_tidx, c.topo.tri_rot, vol);
 }
 void launch_vertex_normals(Ctx& c, const double* x, double* out, cudaStream_t s) {
-    k_vertex_normals<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, c.topo.tri, c.topo.csr_off,
+    KLAUNCH(), k_vertex_normals<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, c.topo.tri, c.topo.csr_off,
                                                         c.topo.csr_idx, out);
 }
 void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s) {
     // curvatures are computed on the loose parts, whose triangles carry the split's rotation
     launch_vertex_normals(c, x, c.vn, s);
-    k_tri_curvature<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri_rot, c.vn, c.tk);
-    k_vertex_avg<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tk, kap);
+    KLAUNCH(), k_tri_curvature<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri_rot, c.vn, c.tk);
+    KLAUNCH(), k_vertex_avg<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tk, kap);
 }
 void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* field_dev, double* out,
                   cudaStream_t s) {
@@ -365,32 +365,32 @@ void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* fiel
         launch_curvature(c, x, c.kap, s);
         kap = c.kap;
     }
-    k_pot_t<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, vel, c.topo.part_of_vert, c.vol, kap, field_dev,
+    KLAUNCH(), k_pot_t<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, vel, c.topo.part_of_vert, c.vol, kap, field_dev,
                                                c.sc, c.prm.p_inf, c.prm.epsilon, c.prm.sigma, c.prm.gamma,
                                                c.prm.field_amp, c.prm.field_kx, c.prm.field_omega,
                                                c.prm.field_phase, 0.0, 1, out);
 }
 void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k, double* out,
                   cudaStream_t s) {
-    k_axpy_dev<<<nb(n, 256), 256, 0, s>>>(n, a, coef_dev, scale, k, out);
+    KLAUNCH(), k_axpy_dev<<<nb(n, 256), 256, 0, s>>>(n, a, coef_dev, scale, k, out);
 }
 void launch_rk4_final(Ctx& c, cudaStream_t s) {
     const int N = (int)c.topo.N;
-    k_rk4_final<<<nb(N, 128), 128, 0, s>>>(N, c.x1, c.k1, c.k2, c.k3, c.k4, c.p1, c.kp1, c.kp2, c.kp3, c.kp4, c.sc,
+    KLAUNCH(), k_rk4_final<<<nb(N, 128), 128, 0, s>>>(N, c.x1, c.k1, c.k2, c.k3, c.k4, c.p1, c.kp1, c.kp2, c.kp3, c.kp4, c.sc,
                                            c.prm.nopen_eps, c.x, c.phi);
     launch_vertex_normals(c, c.x, c.vn, s);
-    k_psi_from_avg<<<nb(N, 128), 128, 0, s>>>(N, c.k1, c.vn, c.psi, c.sc);
+    KLAUNCH(), k_psi_from_avg<<<nb(N, 128), 128, 0, s>>>(N, c.k1, c.vn, c.psi, c.sc);
 }
 void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStream_t s) {
     const int N = (int)c.topo.N;
-    k_euler_final<<<nb(N, 128), 128, 0, s>>>(N, vel, potd, c.sc, c.x, c.phi);
-    k_euler_time<<<1, 1, 0, s>>>(c.sc);
+    KLAUNCH(), k_euler_final<<<nb(N, 128), 128, 0, s>>>(N, vel, potd, c.sc, c.x, c.phi);
+    KLAUNCH(), k_euler_time<<<1, 1, 0, s>>>(c.sc);
 }
 void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cudaStream_t s) {
-    k_get_dt<<<1, 1024, 0, s>>>((int)c.topo.N, vel, potd, dp, c.prm.dp_balance, c.prm.min_dt, c.sc);
+    KLAUNCH(), k_get_dt<<<1, 1024, 0, s>>>((int)c.topo.N, vel, potd, dp, c.prm.dp_balance, c.prm.min_dt, c.sc);
 }
 void launch_any_negative(Ctx& c, const double* x, int* flag, cudaStream_t s) {
-    k_any_negative<<<nb(c.topo.N, 256), 256, 0, s>>>((int)c.topo.N, x, flag);
+    KLAUNCH(), k_any_negative<<<nb(c.topo.N, 256), 256, 0, s>>>((int)c.topo.N, x, flag);
 }
 
 }  // namespace bemb

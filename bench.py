@@ -1,0 +1,337 @@
+"""Benchmark of the BEM hot path on B200: RK4 steps/s of one N=4002 bubble.
+
+Workload (the headline configuration): one bubble, icosphere nu=20 (N=4002 vertices, M=8000
+triangles), R0=1 centred at (2,0,0), 1% radial perturbation N(0, 0.01^2) per vertex (seed 0),
+phi=0, p_inf=1, epsilon=1, gamma=1.4, sigma=0, far-field pressure -0.8*sin(2*pi*t/5), dt=5e-3,
+fixed step, no wall image.  A "step" is one RK4 step (4 stages of assembly + solve + update).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solver mixed|bicgstab|lu]
+
+ours: the mixed-precision path (FP64 assembly, FP64 GMRES, FP32 approximate-inverse preconditioner)
+through libbem_b200.so.  value = device time of K steps with the state resident in HBM (CUDA events
+on the library's stream, max over ranks); e2e = the same K steps through the C ABI with host
+buffers, the step's state copied in from pinned memory and the result copied back every step.
+reference: the reference's own CPU code (oracle/_ref, built from the reference sources) on the
+host cores, one RK4 stage per timed step.  With --gpus N > 1 every rank runs an independent replica
+(the path does not shard: replicas only); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "bem-bubbles_b200"))
+
+METRIC = "RK4 steps/s at N=4002: mixed-precision vs FP64 GPU at <=1e-8 rel dphi/dn error"
+NU, DT = 20, 5e-3
+PHYS = dict(p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.4)
+FIELD = (-0.8, 2.0 * np.pi / 5.0, 0.0)
+
+
+def workload():
+    from bem_b200 import mesh
+
+    v, f = mesh.bubble(NU, 1.0, (0.0, 0.0, 0.0))
+    rng = np.random.default_rng(0)
+    v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None] + np.array([2.0, 0.0, 0.0])
+    return v, f
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def read_traffic():
+    """DRAM bytes per assembly launch from the committed ncu summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "assemble_nu20_ncu.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_stages(stages, threads, timeout=900):
+    """Seconds of each of `stages` RK4 stages of the reference's own code (oracle/_ref)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if not O.ref_available(False):
+        return None
+    v, f = workload()
+    env_threads = dict(threads=threads)
+    out = O.ref_run("stages", v, f, np.zeros(len(v)), steps=stages, lu=0, V0=O.volume(v, f),
+                    amp=FIELD[0], omega=FIELD[1], phase=FIELD[2], **PHYS, **env_threads)
+    return out
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    secs = cpu_reference_stages(args.warmup + args.steps, threads)
+    if secs is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference checkout absent at build time)"}))
+        return 0
+    t = np.asarray(secs[args.warmup:])
+    stage_s = float(t.mean())
+    value = 1.0 / (4.0 * stage_s)
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 4.0 * stage_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "single bubble icosphere nu=20 (N=4002, M=8000), RK4 dt=5e-3, oscillating far field",
+                   "solver": "BiCGSTAB (reference default)", "sample": "one RK4 stage per timed step"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} RK4 stages at N=4002 (4 stages = 1 step), reference code "
+                                   f"(oracle/_ref) with OpenMP on {threads} threads"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    ws, rank, local = dist_env()
+    import torch
+
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+
+    from bem_b200.sim import ColocSim, measure_fma_peaks
+
+    v, f = workload()
+    N, M = len(v), len(f)
+    sim = ColocSim(v, f, pressurefield=FIELD, solver=args.solver, device=device, **PHYS)
+    sim.set_phi(0.0)
+    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=device)
+
+    # warm-up (also builds the preconditioner once)
+    for _ in range(args.warmup):
+        sim.evolve_rk4_steps(DT, 1)
+    sim.sync()
+
+    # accuracy of the mixed path against the FP64 path on the current (non-trivial) state
+    phi_now = sim.get_phi()
+    ref_solver = "bicgstab"
+    sim.set_solver(ref_solver)
+    _, psi64 = sim.position_t(phi_now, return_psi=True)
+    fp64_steps = 2
+    st_x, st_phi, st_psi, st_t = sim.get_vertices(), sim.get_phi(), sim.get_psi(), sim.get_time()
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev_a.record(ext)
+    sim.evolve_rk4_steps(DT, fp64_steps)
+    ev_b.record(ext)
+    ev_b.synchronize()
+    fp64_ms_per_step = ev_a.elapsed_time(ev_b) / fp64_steps
+    # restore the state and switch back
+    sim.set_vertices(st_x)
+    sim.set_phi(st_phi)
+    sim.set_psi(st_psi)
+    sim.set_time(st_t)
+    sim.set_solver(args.solver)
+    _, psimx = sim.position_t(phi_now, return_psi=True)
+    psi_err = float(np.max(np.abs(psimx - psi64)) / max(np.max(np.abs(psi64)), 1e-300))
+
+    # ---- timed region: K steps, state resident in HBM
+    fp64_peak, fp32_peak = measure_fma_peaks(device)
+    sim.set_profiling(True)
+    sim.reset_profile()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    sim.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        e0.record(ext)
+        sim.evolve_rk4_steps(DT, args.steps)
+        e1.record(ext)
+        e1.synchronize()
+    torch.cuda.synchronize(device)
+    elapsed_ms = e0.elapsed_time(e1)
+    prof = sim.profile()
+    sim.set_profiling(False)
+    if dist:
+        t = torch.tensor([elapsed_ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+        dist.barrier()
+    value = ws * args.steps / (elapsed_ms * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    hx = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hphi = torch.empty(N, dtype=torch.float64, pin_memory=True).numpy()
+    hpsi = torch.empty(N, dtype=torch.float64, pin_memory=True).numpy()
+    hx[:] = sim.get_vertices()
+    hphi[:] = sim.get_phi()
+    hpsi[:] = sim.get_psi()
+    e2e_steps = args.steps
+    if dist:
+        dist.barrier()
+    tw0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.set_vertices(hx)
+        sim.set_phi(hphi)
+        sim.set_psi(hpsi)
+        sim.evolve_system_RK4(DT, fixdt=True)
+        hx[:] = sim.get_vertices()
+        hphi[:] = sim.get_phi()
+        hpsi[:] = sim.get_psi()
+    e2e_s = time.perf_counter() - tw0
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = ws * e2e_steps / e2e_s
+    h2d = N * 3 * 8 + 2 * N * 8
+    d2h = N * 3 * 8 + 2 * N * 8
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel (the assembly tile kernel): algorithmic FLOPs per launch
+    evals = (N * M - 3 * M) * 7
+    flops = 32.0 * evals
+    avg_asm_ms = prof.assemble_ms / max(prof.assemble_launches, 1)
+    achieved = flops / (avg_asm_ms * 1e-3) / 1e12
+    traffic = read_traffic()
+
+    # CPU baseline: the reference's own code on the host cores, bounded sample of 2 stages
+    cpu = None
+    if ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        secs = cpu_reference_stages(2, threads)
+        if secs is not None:
+            cpu = {"value": 1.0 / (4.0 * float(np.mean(secs))), "unit": "steps/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"2 RK4 stages at N=4002 of the reference code (oracle/_ref, BiCGSTAB default), "
+                             f"{threads} OpenMP threads; steps/s = 1/(4 x mean stage time)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (assembly, residual, state) + f32 (preconditioner)",
+        "data": "synthetic",
+        "config": {"workload": "single bubble icosphere nu=20 (N=4002, M=8000), RK4 dt=5e-3, p(t)=1-0.8 sin(2 pi t/5)",
+                   "solver": args.solver, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                   "l2": "working set larger than L2 (G+H = 256 MB per stage)"},
+        "fp64_gpu": {"solver": ref_solver, "ms_per_step": fp64_ms_per_step,
+                     "steps_per_s": 1e3 / fp64_ms_per_step},
+        "speedup_vs_fp64_gpu": (1e3 / fp64_ms_per_step) and value / ws / (1e3 / fp64_ms_per_step),
+        "psi_rel_err_vs_fp64": psi_err,
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(prof.kernel_launches),
+        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble (collocation tile kernel)", "achieved": achieved,
+                     "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
+                     "peak_source": "measured live: FP64 FMA-loop kernel (bem_measure_fma_peaks)",
+                     "flops_per_launch": flops, "avg_launch_ms": avg_asm_ms,
+                     "assemble_share_of_step": prof.assemble_ms / elapsed_ms},
+        "fp32_fma_peak_tflops": fp32_peak,
+        "clocks": clk.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solver", default="mixed", choices=["mixed", "bicgstab", "lu"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -131,6 +131,26 @@ int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 
 /* Synchronise the context's stream. */
 int bem_sync(bem_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work around it. */
+int bem_get_stream(bem_ctx* ctx, void** stream);
+
+/* Device-time profile of the context's stream, recorded with CUDA events when enabled:
+ * the regular/singular assembly kernel (the dominant kernel of a stage) and the whole solve
+ * phase.  bem_get_profile synchronises the stream and returns the totals since the last reset. */
+typedef struct {
+    double assemble_ms;        /* summed duration of the assembly tile kernel */
+    int64_t assemble_launches;
+    double solve_ms;           /* summed duration of the solve phases */
+    int64_t solve_calls;
+    int64_t kernel_launches;   /* kernels of this library launched while profiling */
+} bem_profile;
+int bem_set_profiling(bem_ctx* ctx, int32_t on);
+int bem_get_profile(bem_ctx* ctx, bem_profile* out);
+int bem_reset_profile(bem_ctx* ctx);
+
+/* Roofline denominators measured on `device` with FMA-loop kernels: dense FP64 and FP32
+ * FMA throughput in TFLOP/s (2 flops per FMA).  Diagnostic; allocates and frees its own buffer. */
+int bem_measure_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops);
 
 #ifdef __cplusplus
 }

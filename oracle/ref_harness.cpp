@@ -13,6 +13,8 @@
 //     pot_t      -> pot_t_multi(mesh, position_t(mesh, phi), t)   (N)
 //     rk4        -> after each of `steps` RK4 steps: verts (N*3), phi (N), psi (N), time (1)
 //     euler      -> same record layout as rk4, using evolve_system
+//     stages     -> `steps` repetitions of one RK4 stage (position_t + pot_t_multi); writes the
+//                   seconds of each repetition (timing sample for the CPU baseline)
 //   keys: p_inf epsilon sigma gamma V0 amp omega phase dt steps fixdt lu threads timing
 //   amp/omega/phase define the far-field pressure p(x,t) = amp*sin(omega*t + phase).
 #include <cstdint>
@@ -125,6 +127,16 @@ int main(int argc, char** argv) {
             put(ps.data(), ps.size());
             double tm = sim.get_time();
             put(&tm, 1);
+        }
+    } else if (action == "stages") {
+        int steps = (int)kv["steps"];
+        PotVec p = phi;
+        for (int s = 0; s < steps; ++s) {
+            auto a0 = std::chrono::steady_clock::now();
+            CoordVec v = sim.position_t(sim.mesh, p);
+            PotVec r = sim.pot_t_multi(sim.mesh, v, kv["t"]);
+            double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - a0).count();
+            put(&sec, 1);
         }
     } else {
         die("unknown action");
