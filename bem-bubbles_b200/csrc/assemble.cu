@@ -88,50 +88,83 @@ __global__ void k_triangle_records(int M, const double* __restrict__ x, const in
         r[3 * q + 1] = (ay + u * aby) + v * bcy;
         r[3 * q + 2] = (az + u * abz) + v * bcz;
     }
-    r[21] = nx * ia_;
-    r[22] = ny * ia_;
-    r[23] = nz * ia_;
+    const double unx = nx * ia_, uny = ny * ia_, unz = nz * ia_;
+    r[21] = unx;
+    r[22] = uny;
+    r[23] = unz;
     r[24] = area;
-    r[25] = r[26] = r[27] = 0.0;
+    // plane offset a.n: every quadrature point y_q satisfies y_q.n = a.n, so (y_q - x).n is one
+    // number per (row, triangle) pair
+    r[25] = ax * unx + ay * uny + az * unz;
+    r[26] = r[27] = 0.0;
+}
+
+// 1/sqrt(r2) for r2 > 0 in FP64: the hardware's approximate reciprocal square root
+// (rsqrt.approx.ftz.f64) refined by the binomial series of (1-d)^(-1/2) = 1 + d/2 + 3d^2/8 + ...
+// with d = 1 - r2*y0^2; truncation error 5d^3/16, far below the double rounding unit for the
+// estimate's relative error.
+__device__ __forceinline__ double rsqrt_fp64(double r2) {
+    double y0;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(r2));
+    const double t = r2 * y0;
+    const double d = fma(-t, y0, 1.0);
+    const double p = fma(0.375, d, 0.5);
+    return fma(y0, d * p, y0);
 }
 
 // Regular 7-point rule of one (row, triangle) pair; returns area-scaled G and H basis integrals.
+// All quadrature points lie in the triangle's plane, so (y_q - x).n = n.a - n.x is hoisted out of
+// the quadrature loop (and likewise for the image triangle).
 template <bool MIRROR>
 __device__ __forceinline__ void regular_pair(const double* __restrict__ r, double xi0, double xi1, double xi2,
                                              double& g0, double& g1, double& g2, double& h0, double& h1,
                                              double& h2) {
-    const double nx = r[21], ny = r[22], nz = r[23], area = r[24];
+    const double nx = r[21], ny = r[22], nz = r[23], area = r[24], dt = r[25];
+    const double xn_yz = xi1 * ny + xi2 * nz;
+    const double dn = dt - fma(xi0, nx, xn_yz);  // (y - x).n
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
-        double yx = r[3 * q], zy = r[3 * q + 1] - xi1, zz = r[3 * q + 2] - xi2;
-        double zx = yx - xi0;
-        double yz2 = zy * zy + zz * zz;
-        double inv = rsqrt(zx * zx + yz2);
-        double dn = zx * nx + (zy * ny + zz * nz);
-        double gq = inv;
-        double hq = -dn * (inv * inv * inv);
+        const double yx = r[3 * q];
+        const double zy = r[3 * q + 1] - xi1, zz = r[3 * q + 2] - xi2;
+        const double zx = yx - xi0;
+        const double yz2 = fma(zy, zy, zz * zz);
+        const double inv = rsqrt_fp64(fma(zx, zx, yz2));
+        const double i3 = inv * inv * inv;
+        a0 = fma(c_qc[q][0], inv, a0);
+        a1 = fma(c_qc[q][1], inv, a1);
+        a2 = fma(c_qc[q][2], inv, a2);
+        b0 = fma(c_qc[q][0], i3, b0);
+        b1 = fma(c_qc[q][1], i3, b1);
+        b2 = fma(c_qc[q][2], i3, b2);
         if (MIRROR) {
-            // image point (-y.x, y.y, y.z) with image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
-            double mx = -yx - xi0;
-            double inv2 = rsqrt(mx * mx + yz2);
-            double dn2 = -mx * nx + (zy * ny + zz * nz);
-            gq += inv2;
-            hq += -dn2 * (inv2 * inv2 * inv2);
+            // image point (-y.x, y.y, y.z), image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
+            const double mx = -yx - xi0;
+            const double inv2 = rsqrt_fp64(fma(mx, mx, yz2));
+            const double j3 = inv2 * inv2 * inv2;
+            a0 = fma(c_qc[q][0], inv2, a0);
+            a1 = fma(c_qc[q][1], inv2, a1);
+            a2 = fma(c_qc[q][2], inv2, a2);
+            m0 = fma(c_qc[q][0], j3, m0);
+            m1 = fma(c_qc[q][1], j3, m1);
+            m2 = fma(c_qc[q][2], j3, m2);
         }
-        a0 = fma(c_qc[q][0], gq, a0);
-        a1 = fma(c_qc[q][1], gq, a1);
-        a2 = fma(c_qc[q][2], gq, a2);
-        b0 = fma(c_qc[q][0], hq, b0);
-        b1 = fma(c_qc[q][1], hq, b1);
-        b2 = fma(c_qc[q][2], hq, b2);
     }
     g0 = a0 * area;
     g1 = a1 * area;
     g2 = a2 * area;
-    h0 = b0 * area;
-    h1 = b1 * area;
-    h2 = b2 * area;
+    const double sh = -dn * area;
+    h0 = b0 * sh;
+    h1 = b1 * sh;
+    h2 = b2 * sh;
+    if (MIRROR) {
+        // (y' - x).n' = n.a - (-x.x n.x + x.y n.y + x.z n.z)
+        const double sm = -(dt - fma(-xi0, nx, xn_yz)) * area;
+        h0 = fma(m0, sm, h0);
+        h1 = fma(m1, sm, h1);
+        h2 = fma(m2, sm, h2);
+    }
 }
 
 // Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  Results in the triangle's

@@ -220,10 +220,12 @@ def run_ours(args):
     sim.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(device) as clk:
+        torch.cuda.nvtx.range_push("timed_region")
         e0.record(ext)
         sim.evolve_rk4_steps(DT, args.steps)
         e1.record(ext)
         e1.synchronize()
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize(device)
     elapsed_ms = e0.elapsed_time(e1)
     prof = sim.profile()
