@@ -42,9 +42,8 @@ static void free_all(Ctx& c) {
 
 // ---------------------------------------------------------------- topology preprocessing
 struct HostTopo {
-    std::vector<int> tri, csr_off, csr_idx, grp_off, grp_tri, grp_slot, grp_vert, part_of_vert, part_off,
-        part_tidx, tri_rot;
-    int ngroups = 0, nparts = 0;
+    std::vector<int> tri, csr_off, csr_idx, part_of_vert, part_off, part_tidx, tri_rot, ch_c0, col_off, ent;
+    int nparts = 0, nchunks = 0, ncolors = 0, asm_rows = 1;
 };
 
 static int build_topology(int64_t N, int64_t M, const int64_t* trigs, HostTopo& h, std::string& err) {
@@ -114,52 +113,86 @@ static int build_topology(int64_t N, int64_t M, const int64_t* trigs, HostTopo& 
         if (t[2] > t[r]) r = 2;
         for (int k = 0; k < 3; ++k) h.tri_rot[(size_t)(3 * j + k)] = t[(r + k) % 3];
     }
-    // assembly column groups: breadth-first patches of at most CG vertices
-    std::vector<int> grp((size_t)N, -1), slot((size_t)N, -1);
-    std::vector<std::vector<int>> members;
-    for (int64_t s = 0; s < N; ++s) {
-        if (grp[(size_t)s] >= 0) continue;
-        const int gid = (int)members.size();
-        members.emplace_back();
-        std::deque<int> q{(int)s};
-        std::vector<char> queued;
-        std::set<int> inq{(int)s};
-        while (!q.empty() && (int)members.back().size() < CG) {
-            int v = q.front();
-            q.pop_front();
-            if (grp[(size_t)v] >= 0) continue;
-            grp[(size_t)v] = gid;
-            slot[(size_t)v] = (int)members.back().size();
-            members.back().push_back(v);
-            for (int u : nbr[(size_t)v])
-                if (grp[(size_t)u] < 0 && !inq.count(u)) {
-                    inq.insert(u);
-                    q.push_back(u);
+    // assembly work list.  Rows per CTA and column chunks from the shared-memory budget: full rows
+    // when they fit (1..4 rows), else chunks of contiguous columns with 2 rows per CTA.
+    {
+        const int64_t per_row = 16 * N;  // G and H, FP64
+        int rows = (int)std::min<int64_t>(4, ASM_SMEM_BUDGET / per_row);
+        int cw = (int)N;
+        if (rows < 1) {
+            rows = 2;
+            cw = ASM_SMEM_BUDGET / (16 * rows);
+        }
+        h.asm_rows = rows;
+        h.ch_c0.clear();
+        for (int64_t c0 = 0; c0 < N; c0 += cw) h.ch_c0.push_back((int)c0);
+        h.ch_c0.push_back((int)N);
+        h.nchunks = (int)h.ch_c0.size() - 1;
+        // colour classes: greedy in triangle order, a colour may not repeat a vertex; classes capped
+        // at a multiple of the CTA width so that they are balanced across the CTA's threads
+        int cmin = 0;
+        {
+            std::vector<uint64_t> used((size_t)N, 0);
+            for (int64_t j = 0; j < M; ++j) {
+                const int* t = &h.tri[(size_t)(3 * j)];
+                uint64_t u = used[(size_t)t[0]] | used[(size_t)t[1]] | used[(size_t)t[2]];
+                int col = 0;
+                while (col < 64 && (u >> col) & 1ull) ++col;
+                if (col >= 64) {
+                    err = "mesh vertex valence too high for the assembly colouring";
+                    return BEM_ERR_ARG;
                 }
-        }
-    }
-    h.ngroups = (int)members.size();
-    h.grp_off.assign((size_t)h.ngroups + 1, 0);
-    h.grp_vert.assign((size_t)h.ngroups * CG, -1);
-    for (int g = 0; g < h.ngroups; ++g) {
-        std::vector<int> tl;
-        for (int v : members[(size_t)g]) {
-            h.grp_vert[(size_t)g * CG + slot[(size_t)v]] = v;
-            for (int e = h.csr_off[(size_t)v]; e < h.csr_off[(size_t)v + 1]; ++e) tl.push_back(h.csr_idx[(size_t)e]);
-        }
-        std::sort(tl.begin(), tl.end());
-        tl.erase(std::unique(tl.begin(), tl.end()), tl.end());
-        for (int t : tl) {
-            int code = 0;
-            for (int k = 0; k < 3; ++k) {
-                int v = h.tri[(size_t)(3 * t + k)];
-                int sl = (grp[(size_t)v] == g) ? slot[(size_t)v] : 63;
-                code |= sl << (6 * k);
+                cmin = std::max(cmin, col + 1);
+                for (int k = 0; k < 3; ++k) used[(size_t)t[k]] |= 1ull << col;
             }
-            h.grp_tri.push_back(t);
-            h.grp_slot.push_back(code);
         }
-        h.grp_off[(size_t)g + 1] = (int)h.grp_tri.size();
+        int64_t target = (M + cmin - 1) / cmin;
+        int64_t cap = std::max<int64_t>(ASM_THREADS, (target / ASM_THREADS) * ASM_THREADS);
+        std::vector<int> color((size_t)M, -1);
+        int ncol = 0;
+        {
+            std::vector<uint64_t> used((size_t)N, 0);
+            std::vector<int64_t> count(64, 0);
+            for (int64_t j = 0; j < M; ++j) {
+                const int* t = &h.tri[(size_t)(3 * j)];
+                uint64_t u = used[(size_t)t[0]] | used[(size_t)t[1]] | used[(size_t)t[2]];
+                int col = 0;
+                while (col < 64 && (((u >> col) & 1ull) || count[(size_t)col] >= cap)) ++col;
+                if (col >= 64) {
+                    col = 0;  // caps exhausted: fall back to the first free colour
+                    while (col < 64 && (u >> col) & 1ull) ++col;
+                    if (col >= 64) {
+                        err = "mesh vertex valence too high for the assembly colouring";
+                        return BEM_ERR_ARG;
+                    }
+                }
+                color[(size_t)j] = col;
+                count[(size_t)col]++;
+                ncol = std::max(ncol, col + 1);
+                for (int k = 0; k < 3; ++k) used[(size_t)t[k]] |= 1ull << col;
+            }
+        }
+        h.ncolors = ncol;
+        h.col_off.assign((size_t)h.nchunks * (ncol + 1), 0);
+        h.ent.clear();
+        for (int k = 0; k < h.nchunks; ++k) {
+            const int a = h.ch_c0[(size_t)k], bnd = h.ch_c0[(size_t)k + 1];
+            std::vector<std::vector<int>> bycol((size_t)ncol);
+            for (int64_t j = 0; j < M; ++j) {
+                const int* t = &h.tri[(size_t)(3 * j)];
+                bool touch = false;
+                for (int q = 0; q < 3; ++q) touch |= (t[q] >= a && t[q] < bnd);
+                if (touch) bycol[(size_t)color[(size_t)j]].push_back((int)j);
+            }
+            for (int col = 0; col < ncol; ++col) {
+                h.col_off[(size_t)k * (ncol + 1) + col] = (int)(h.ent.size() / 4);
+                for (int j : bycol[(size_t)col]) {
+                    h.ent.push_back(j);
+                    for (int q = 0; q < 3; ++q) h.ent.push_back(h.tri[(size_t)(3 * j + q)]);
+                }
+            }
+            h.col_off[(size_t)k * (ncol + 1) + ncol] = (int)(h.ent.size() / 4);
+        }
     }
     return BEM_OK;
 }
@@ -302,17 +335,22 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     Topology& t = c.topo;
     t.N = N;
     t.M = M;
-    t.ngroups = h.ngroups;
     t.nparts = h.nparts;
+    t.nchunks = h.nchunks;
+    t.ncolors = h.ncolors;
+    t.asm_rows = h.asm_rows;
+    t.E = (int64_t)(h.ent.size() / 4);
     t.h_part_of_vert = h.part_of_vert;
+    t.h_ch_c0 = h.ch_c0;
     int rc;
+    int* ent_raw = nullptr;
     if ((rc = upload(c, &t.tri, h.tri)) || (rc = upload(c, &t.csr_off, h.csr_off)) ||
-        (rc = upload(c, &t.csr_idx, h.csr_idx)) || (rc = upload(c, &t.grp_off, h.grp_off)) ||
-        (rc = upload(c, &t.grp_tri, h.grp_tri)) || (rc = upload(c, &t.grp_slot, h.grp_slot)) ||
-        (rc = upload(c, &t.grp_vert, h.grp_vert)) || (rc = upload(c, &t.part_of_vert, h.part_of_vert)) ||
-        (rc = upload(c, &t.part_off, h.part_off)) || (rc = upload(c, &t.part_tidx, h.part_tidx)) ||
-        (rc = upload(c, &t.tri_rot, h.tri_rot)))
+        (rc = upload(c, &t.csr_idx, h.csr_idx)) || (rc = upload(c, &t.ch_c0, h.ch_c0)) ||
+        (rc = upload(c, &t.col_off, h.col_off)) || (rc = upload(c, &ent_raw, h.ent)) ||
+        (rc = upload(c, &t.part_of_vert, h.part_of_vert)) || (rc = upload(c, &t.part_off, h.part_off)) ||
+        (rc = upload(c, &t.part_tidx, h.part_tidx)) || (rc = upload(c, &t.tri_rot, h.tri_rot)))
         return rc;
+    t.ent = reinterpret_cast<int4*>(ent_raw);
     const size_t n = (size_t)N, m = (size_t)M, nn = n * n;
     const int ncs = 64;
     double** vec3s[] = {&c.x, &c.x1, &c.xs, &c.k1, &c.k2, &c.k3, &c.k4, &c.vn};
@@ -323,9 +361,9 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     for (auto p : vecs)
         if ((rc = dalloc(c, p, n))) return rc;
     if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (rc = dalloc(c, &c.LU, nn)) ||
-        (rc = dalloc(c, &c.rec, m * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) || (rc = dalloc(c, &c.tg, 3 * m)) ||
-        (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, (size_t)h.ngroups * n)) ||
-        (rc = dalloc(c, &c.bp, (size_t)h.ngroups * n)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
+        (rc = dalloc(c, &c.rec, (size_t)t.E * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) ||
+        (rc = dalloc(c, &c.tg, 3 * m)) || (rc = dalloc(c, &c.tk, m)) ||
+        (rc = dalloc(c, &c.rowHp, (size_t)h.nchunks * n)) || (rc = dalloc(c, &c.bp, (size_t)h.nchunks * n)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)))
@@ -566,8 +604,15 @@ int bem_assemble(bem_ctx* c, const double* verts, double* G, double* H) {
     BEM_CUDA(*c, cudaMemsetAsync(c->p1, 0, sizeof(double) * N, c->stream));
     launch_assemble(*c, x, c->p1, c->G, c->H, nullptr, c->stream);
     BEM_CUDA(*c, cudaGetLastError());
-    if (G) COPY_OUT(G, c->G, N * N);
-    if (H) COPY_OUT(H, c->H, N * N);
+    // internal storage is row-major; the ABI returns Eigen's column-major layout
+    if (G) {
+        transpose(N, c->G, c->LU, c->stream);
+        COPY_OUT(G, c->LU, N * N);
+    }
+    if (H) {
+        transpose(N, c->H, c->LU, c->stream);
+        COPY_OUT(H, c->LU, N * N);
+    }
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
 }
@@ -577,7 +622,8 @@ int bem_solve_system(bem_ctx* c, const double* G, const double* b, double* x) {
     NEED_MESH(c);
     const int64_t N = c->topo.N;
     if (!G || !b || !x) return c->fail(BEM_ERR_ARG, "null pointer");
-    COPY_IN(c->G, G, N * N);
+    COPY_IN(c->LU, G, N * N);
+    transpose(N, c->LU, c->G, c->stream);  // column-major input -> row-major storage
     COPY_IN(c->b, b, N);
     int rc = solve(*c, c->G, c->b, c->psil, c->stream);
     if (rc) return rc;
