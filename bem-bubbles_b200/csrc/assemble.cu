@@ -6,22 +6,17 @@
 //     (integrate_disjoint_coloc[_mir], Integrator.hpp:471-513, kernel Integrator.hpp:116-119);
 //   * singular pairs (i on t): polar rule with the analytic radial integral and 7-point Gauss in
 //     the angle (integrate_identical_coloc[_mir], Integrator.cpp:13-89);
-//   * the "4 pi rule" diagonal H(i,i) -= 4 pi + sum_j H(i,j) (ColocSim.cpp:85-97);
-//   * the right-hand side b = H phi of position_t (LinLinSim.cpp:32), fused.
+//   * the "4 pi rule" diagonal H(i,i) -= 4 pi + sum_j H(i,j) (ColocSim.cpp:85-97).
 //
-// Tiling (B200): one CTA owns R complete rows (collocation points) of G and H in shared memory
-// (R*N*16 bytes, up to 225 KB) and walks every triangle exactly once.  Triangles are split into
-// colour classes in which no two triangles share a vertex, so the threads of a colour scatter
-// their three basis contributions into the shared rows without conflicts or atomics; one barrier
-// separates colours.  Each thread evaluates its triangle's 7 quadrature points for all R rows (7R
-// independent chains).  Triangle records are field-major so every warp load is one coalesced
-// 256-byte line.  The epilogue reduces each row in a fixed order (row sum for the 4 pi rule,
-// H.phi), fixes the diagonal and writes the rows contiguously: G and H are stored row-major.
-// Nothing is evaluated twice and the result is bit-reproducible run to run.  Meshes too large for
-// full rows in shared memory are split into column chunks (grid.y), finished by k_finish_rows.
+// Tiling (B200): a CTA owns one column group (cg vertices, i.e. cg columns of G and H) and a block
+// of collocation rows, one row per thread.  It walks the triangles incident to its
+// vertices in increasing index order (the reference's per-column summation order), with the
+// triangle records staged in shared memory and read as broadcasts, and accumulates the cg columns
+// of its rows in shared memory.  Column writes are coalesced (column-major, consecutive rows).
+// No atomics: every entry is summed by exactly one thread in a fixed order, so the result is
+// bit-reproducible run to run.  The same pass produces the per-group partial row sums of H and
+// partial H*phi, so the 4 pi diagonal and the right-hand side need no second read of H.
 #include <math.h>
-
-#include <algorithm>
 
 #include "ctx.h"
 
@@ -32,6 +27,12 @@ namespace bemb {
 __constant__ double c_qc[7][3];
 __constant__ double c_quv[7][2];
 __constant__ double c_gcos[7], c_gsin[7], c_gw[7];
+// The 7-point rule is symmetric: the centroid plus two orbits of three points whose barycentric
+// weights are rotations of (alpha, beta, beta).  With S the orbit sum of kernel values and
+// g_k the orbit point whose alpha sits on vertex k, sum_q w_q basis_k(q) K(q) =
+//   C + dA * gA_k + dB * gB_k,   C = w0 b0 K(centroid) + cA*S_A + cB*S_B.
+// c_orb = {w0*b0, cA, dA, cB, dB}.
+__constant__ double c_orb[5];
 
 // Reference tables (quadrature.hpp:30-38 gauss_7, :88-96 quadrature_7), evaluated on the host once.
 static void upload_constants() {
@@ -64,6 +65,15 @@ static void upload_constants() {
         gs[q] = sin(th);
         gw[q] = GL[q][1];
     }
+    // orbit form: point 0 is the centroid; points 3,1,2 carry alpha on vertex 0,1,2 (orbit A) and
+    // points 6,4,5 (orbit B), with barycentric coordinates (1-u, u-v, v)
+    {
+        const double w0 = Q[0][2], wA = Q[1][2], wB = Q[4][2];
+        const double aA = 1.0 - (Q[3][0] + Q[3][1]), bA = Q[3][1];  // point 3: (alpha, beta, beta)
+        const double aB = 1.0 - (Q[6][0] + Q[6][1]), bB = Q[6][1];  // point 6
+        const double orb[5] = {w0 * (1.0 / 3.0), wA * bA, wA * (aA - bA), wB * bB, wB * (aB - bB)};
+        cudaMemcpyToSymbol(c_orb, orb, sizeof(orb));
+    }
     cudaMemcpyToSymbol(c_qc, qc, sizeof(qc));
     cudaMemcpyToSymbol(c_quv, quv, sizeof(quv));
     cudaMemcpyToSymbol(c_gcos, gc, sizeof(gc));
@@ -72,39 +82,42 @@ static void upload_constants() {
     done = true;
 }
 
-// Per-entry triangle record, field-major (rec[f*E + e]): Interpolator (Interpolator.hpp:15-37)
-// quantities, the 7 quadrature points y_q = a + u_q*ab + v_q*bc and the plane offset n.a.
-__global__ void k_triangle_records(int64_t E, const double* __restrict__ x, const int4* __restrict__ ent,
+// Per-triangle record: Interpolator (Interpolator.hpp:15-37) quantities and the 7 quadrature
+// points y_q = a + u_q*ab + v_q*bc.
+__global__ void k_triangle_records(int M, const double* __restrict__ x, const int* __restrict__ tri,
                                    double* __restrict__ rec) {
-    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E) return;
-    const int4 t = ent[e];
-    const int ia = t.y, ib = t.z, ic = t.w;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
     double ax = x[3 * ia], ay = x[3 * ia + 1], az = x[3 * ia + 2];
     double abx = x[3 * ib] - ax, aby = x[3 * ib + 1] - ay, abz = x[3 * ib + 2] - az;
     double bcx = x[3 * ic] - x[3 * ib], bcy = x[3 * ic + 1] - x[3 * ib + 1], bcz = x[3 * ic + 2] - x[3 * ib + 2];
     double nx = aby * bcz - abz * bcy, ny = abz * bcx - abx * bcz, nz = abx * bcy - aby * bcx;
     double area = sqrt(nx * nx + ny * ny + nz * nz);
     double ia_ = 1.0 / area;
+    double* r = rec + (size_t)t * REC;
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
         double u = c_quv[q][0], v = c_quv[q][1];
-        rec[(3 * q + 0) * E + e] = (ax + u * abx) + v * bcx;
-        rec[(3 * q + 1) * E + e] = (ay + u * aby) + v * bcy;
-        rec[(3 * q + 2) * E + e] = (az + u * abz) + v * bcz;
+        r[3 * q + 0] = (ax + u * abx) + v * bcx;
+        r[3 * q + 1] = (ay + u * aby) + v * bcy;
+        r[3 * q + 2] = (az + u * abz) + v * bcz;
     }
     const double unx = nx * ia_, uny = ny * ia_, unz = nz * ia_;
-    rec[21 * E + e] = unx;
-    rec[22 * E + e] = uny;
-    rec[23 * E + e] = unz;
-    rec[24 * E + e] = area;
-    // every quadrature point y_q satisfies y_q.n = a.n, so (y_q - x).n is one number per pair
-    rec[25 * E + e] = ax * unx + ay * uny + az * unz;
+    r[21] = unx;
+    r[22] = uny;
+    r[23] = unz;
+    r[24] = area;
+    // plane offset a.n: every quadrature point y_q satisfies y_q.n = a.n, so (y_q - x).n is one
+    // number per (row, triangle) pair
+    r[25] = ax * unx + ay * uny + az * unz;
+    r[26] = r[27] = 0.0;
 }
 
 // 1/sqrt(r2) for r2 > 0 in FP64: the hardware's approximate reciprocal square root
 // (rsqrt.approx.ftz.f64) refined by the binomial series of (1-d)^(-1/2) = 1 + d/2 + 3d^2/8 + ...
-// with d = 1 - r2*y0^2; the truncation error 5d^3/16 is far below the double rounding unit.
+// with d = 1 - r2*y0^2; truncation error 5d^3/16, far below the double rounding unit for the
+// estimate's relative error.
 __device__ __forceinline__ double rsqrt_fp64(double r2) {
     double y0;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(r2));
@@ -114,14 +127,73 @@ __device__ __forceinline__ double rsqrt_fp64(double r2) {
     return fma(y0, d * p, y0);
 }
 
-// Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  Results in the triangle's
-// original vertex order.  Reads the vertex positions from global memory (rare path).
+// Orbit-form basis sums of the 7 kernel values k[0..6] (see c_orb): out_k = C + dA*kA_k + dB*kB_k.
+__device__ __forceinline__ void orbit_sums(const double* k, double& o0, double& o1, double& o2) {
+    const double SA = (k[1] + k[2]) + k[3], SB = (k[4] + k[5]) + k[6];
+    const double C = fma(c_orb[0], k[0], fma(c_orb[1], SA, c_orb[3] * SB));
+    o0 = fma(c_orb[2], k[3], fma(c_orb[4], k[6], C));
+    o1 = fma(c_orb[2], k[1], fma(c_orb[4], k[4], C));
+    o2 = fma(c_orb[2], k[2], fma(c_orb[4], k[5], C));
+}
+
+// Regular 7-point rule of one (row, triangle) pair; returns area-scaled G and H basis integrals.
+// All quadrature points lie in the triangle's plane, so (y_q - x).n = n.a - n.x is hoisted out of
+// the quadrature loop (and likewise for the image triangle).
 template <bool MIRROR>
-__device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta, int tb, int tc, int shift,
-                                           double& g0, double& g1, double& g2, double& h0, double& h1,
-                                           double& h2) {
-    int v[3] = {ta, tb, tc};
-    int r0 = v[shift], r1 = v[(shift + 1) % 3], r2 = v[(shift + 2) % 3];
+__device__ __forceinline__ void regular_pair(const double* __restrict__ r, double xi0, double xi1, double xi2,
+                                             double& g0, double& g1, double& g2, double& h0, double& h1,
+                                             double& h2) {
+    const double nx = r[21], ny = r[22], nz = r[23], area = r[24], dt = r[25];
+    const double xn_yz = xi1 * ny + xi2 * nz;
+    const double dn = dt - fma(xi0, nx, xn_yz);  // (y - x).n
+    double kg[7], kh[7], km[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        const double yx = r[3 * q];
+        const double zy = r[3 * q + 1] - xi1, zz = r[3 * q + 2] - xi2;
+        const double zx = yx - xi0;
+        const double yz2 = fma(zy, zy, zz * zz);
+        const double inv = rsqrt_fp64(fma(zx, zx, yz2));
+        kg[q] = inv;
+        kh[q] = inv * inv * inv;
+        if (MIRROR) {
+            // image point (-y.x, y.y, y.z), image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
+            const double mx = -yx - xi0;
+            const double inv2 = rsqrt_fp64(fma(mx, mx, yz2));
+            kg[q] += inv2;
+            km[q] = inv2 * inv2 * inv2;
+        }
+    }
+    double a0, a1, a2, b0, b1, b2;
+    orbit_sums(kg, a0, a1, a2);
+    orbit_sums(kh, b0, b1, b2);
+    g0 = a0 * area;
+    g1 = a1 * area;
+    g2 = a2 * area;
+    const double sh = -dn * area;
+    h0 = b0 * sh;
+    h1 = b1 * sh;
+    h2 = b2 * sh;
+    if (MIRROR) {
+        double m0, m1, m2;
+        orbit_sums(km, m0, m1, m2);
+        // (y' - x).n' = n.a - (-x.x n.x + x.y n.y + x.z n.z)
+        const double sm = -(dt - fma(-xi0, nx, xn_yz)) * area;
+        h0 = fma(m0, sm, h0);
+        h1 = fma(m1, sm, h1);
+        h2 = fma(m2, sm, h2);
+    }
+}
+
+// Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  Adds G and H of the pair
+// directly into the row's shared-memory accumulators of the owned slots (codes as in k_assemble),
+// so nothing of this rare path lives in the hot loop's registers or in local memory.
+template <bool MIRROR>
+__device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta, int tb, int tc, int shift, int code,
+                                           double* accG, double* accH, int stride) {
+    const int r0 = shift == 0 ? ta : (shift == 1 ? tb : tc);
+    const int r1 = shift == 0 ? tb : (shift == 1 ? tc : ta);
+    const int r2 = shift == 0 ? tc : (shift == 1 ? ta : tb);
     double ax = x[3 * r0], ay = x[3 * r0 + 1], az = x[3 * r0 + 2];
     double abx = x[3 * r1] - ax, aby = x[3 * r1 + 1] - ay, abz = x[3 * r1 + 2] - az;
     double bcx = x[3 * r2] - x[3 * r1], bcy = x[3 * r2 + 1] - x[3 * r1 + 1], bcz = x[3 * r2 + 2] - x[3 * r1 + 2];
@@ -140,7 +212,7 @@ __device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta,
         s1 += of * (cx - sx) * fac;
         s2 += of * sx * fac;
     }
-    double rg[3] = {s0, s1, s2}, rh[3] = {0.0, 0.0, 0.0};
+    double rg0 = s0, rg1 = s1, rg2 = s2, rh0 = 0.0, rh1 = 0.0, rh2 = 0.0;
     if (MIRROR) {
         // regular rule over the mirrored own triangle, plain kernel, H sign flipped (Integrator.cpp:70-86)
         double bx = ax + abx, by = ay + aby, bz = az + abz;
@@ -170,245 +242,164 @@ __device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta,
             b1 += c_qc[q][1] * hq;
             b2 += c_qc[q][2] * hq;
         }
-        rg[0] += a0 * marea;
-        rg[1] += a1 * marea;
-        rg[2] += a2 * marea;
-        rh[0] = -(b0 * marea);
-        rh[1] = -(b1 * marea);
-        rh[2] = -(b2 * marea);
+        rg0 += a0 * marea;
+        rg1 += a1 * marea;
+        rg2 += a2 * marea;
+        rh0 = -(b0 * marea);
+        rh1 = -(b1 * marea);
+        rh2 = -(b2 * marea);
     }
-    // rotated order (i first) back to the triangle's own order
-    const int k0 = (3 - shift) % 3, k1 = (4 - shift) % 3, k2 = (5 - shift) % 3;
-    g0 = rg[k0];
-    g1 = rg[k1];
-    g2 = rg[k2];
-    h0 = rh[k0];
-    h1 = rh[k1];
-    h2 = rh[k2];
+    // rotated vertex m sits at triangle position (m + shift) % 3
+    const double gg[3] = {rg0, rg1, rg2}, hh[3] = {rh0, rh1, rh2};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int k = (m + shift) % 3;
+        const int sl = (code >> (SLOT_BITS * k)) & SLOT_NONE;
+        if (sl != SLOT_NONE) {
+            accG[sl * stride] += gg[m];
+            accH[sl * stride] += hh[m];
+        }
+    }
 }
 
-__device__ __forceinline__ double block_sum_fixed(double v, double* s_w) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) s_w[wid] = v;
-    __syncthreads();
-    double r = 0.0;
-    if (wid == 0) {
-        r = (lane < (int)(blockDim.x >> 5)) ? s_w[lane] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-        if (lane == 0) s_w[0] = r;
+// Column-group tile kernel.  CGT: vertices (columns) per group, ROWS: rows per CTA (one per thread).
+template <bool MIRROR, int CGT, int ROWS, int MINB>
+__global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __restrict__ x, const int* __restrict__ tri,
+                                                         const double* __restrict__ rec, const int* __restrict__ grp_off,
+                                                         const int* __restrict__ grp_tri, const int* __restrict__ grp_slot,
+                                                         const int* __restrict__ grp_vert, const double* __restrict__ phi,
+                                                         double* __restrict__ G, double* __restrict__ H,
+                                                         double* __restrict__ rowHp, double* __restrict__ bp) {
+    extern __shared__ __align__(16) double smem[];
+    double* accG = smem;                      // [CGT][ROWS]
+    double* accH = accG + CGT * ROWS;         // [CGT][ROWS]
+    double* srec = accH + CGT * ROWS;         // [ASM_TC][REC]
+    int* sinfo = reinterpret_cast<int*>(srec + ASM_TC * REC);  // [ASM_TC][4]
+    const int g = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int i = blockIdx.y * ROWS + tid;
+#pragma unroll 4
+    for (int s = 0; s < CGT; ++s) {
+        accG[s * ROWS + tid] = 0.0;
+        accH[s * ROWS + tid] = 0.0;
     }
-    __syncthreads();
-    r = s_w[0];
-    __syncthreads();
-    return r;
-}
-
-template <bool MIRROR, int R>
-__global__ void __launch_bounds__(ASM_THREADS) k_assemble_rows(
-    int N, const int* __restrict__ ch_c0, int ncolors, const int* __restrict__ col_off, const int4* __restrict__ ent,
-    int64_t E, const double* __restrict__ rec, const double* __restrict__ x, const double* __restrict__ phi,
-    double* __restrict__ G, double* __restrict__ H, double* __restrict__ b, double* __restrict__ rowHp,
-    double* __restrict__ bp, int single) {
-    extern __shared__ __align__(16) double sm[];
-    __shared__ double s_red[32];
-    const int chunk = blockIdx.y;
-    const int c0 = ch_c0[chunk], cw = ch_c0[chunk + 1] - c0;
-    double* aG = sm;           // [R][cw]
-    double* aH = sm + R * cw;  // [R][cw]
-    const int r0 = blockIdx.x * R;
-    for (int k = threadIdx.x; k < 2 * R * cw; k += ASM_THREADS) sm[k] = 0.0;
-    double xr[R][3];
-    int row[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int i = r0 + r;
-        row[r] = (i < N) ? i : -1;
-        const int ii = (i < N) ? i : r0;  // padding rows repeat a valid position; results are discarded
-        xr[r][0] = x[3 * ii];
-        xr[r][1] = x[3 * ii + 1];
-        xr[r][2] = x[3 * ii + 2];
+    double xi0 = 0.0, xi1 = 0.0, xi2 = 0.0;
+    if (i < N) {
+        xi0 = x[3 * i];
+        xi1 = x[3 * i + 1];
+        xi2 = x[3 * i + 2];
     }
-    __syncthreads();
-    const int* coff = col_off + (size_t)chunk * (ncolors + 1);
-    for (int col = 0; col < ncolors; ++col) {
-        const int e1 = coff[col + 1];
-        for (int e = coff[col] + threadIdx.x; e < e1; e += ASM_THREADS) {
-            const int4 tv = ent[e];
-            const double nx = rec[21 * E + e], ny = rec[22 * E + e], nz = rec[23 * E + e];
-            const double area = rec[24 * E + e], dt = rec[25 * E + e];
-            double a[R][3], h[R][3], m[R][3];
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) a[r][k] = h[r][k] = m[r][k] = 0.0;
-#pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const double yx = rec[(3 * q) * E + e], yy = rec[(3 * q + 1) * E + e], yz = rec[(3 * q + 2) * E + e];
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const double zy = yy - xr[r][1], zz = yz - xr[r][2];
-                    const double zx = yx - xr[r][0];
-                    const double yz2 = fma(zy, zy, zz * zz);
-                    const double inv = rsqrt_fp64(fma(zx, zx, yz2));
-                    const double i3 = inv * inv * inv;
-                    a[r][0] = fma(c_qc[q][0], inv, a[r][0]);
-                    a[r][1] = fma(c_qc[q][1], inv, a[r][1]);
-                    a[r][2] = fma(c_qc[q][2], inv, a[r][2]);
-                    h[r][0] = fma(c_qc[q][0], i3, h[r][0]);
-                    h[r][1] = fma(c_qc[q][1], i3, h[r][1]);
-                    h[r][2] = fma(c_qc[q][2], i3, h[r][2]);
-                    if (MIRROR) {
-                        // image point (-y.x, y.y, y.z), image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
-                        const double mx = -yx - xr[r][0];
-                        const double inv2 = rsqrt_fp64(fma(mx, mx, yz2));
-                        const double j3 = inv2 * inv2 * inv2;
-                        a[r][0] = fma(c_qc[q][0], inv2, a[r][0]);
-                        a[r][1] = fma(c_qc[q][1], inv2, a[r][1]);
-                        a[r][2] = fma(c_qc[q][2], inv2, a[r][2]);
-                        m[r][0] = fma(c_qc[q][0], j3, m[r][0]);
-                        m[r][1] = fma(c_qc[q][1], j3, m[r][1]);
-                        m[r][2] = fma(c_qc[q][2], j3, m[r][2]);
-                    }
-                }
-            }
-            const int lv[3] = {tv.y - c0, tv.z - c0, tv.w - c0};
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (row[r] < 0) continue;
-                double g0, g1, g2, h0, h1, h2;
-                const int i = row[r];
-                if (i == tv.y || i == tv.z || i == tv.w) {
-                    const int shift = (i == tv.y) ? 0 : ((i == tv.z) ? 1 : 2);
-                    singular_pair<MIRROR>(x, tv.y, tv.z, tv.w, shift, g0, g1, g2, h0, h1, h2);
-                } else {
-                    const double xn_yz = xr[r][1] * ny + xr[r][2] * nz;
-                    const double sh = -(dt - fma(xr[r][0], nx, xn_yz)) * area;  // -(y - x).n * area
-                    g0 = a[r][0] * area;
-                    g1 = a[r][1] * area;
-                    g2 = a[r][2] * area;
-                    h0 = h[r][0] * sh;
-                    h1 = h[r][1] * sh;
-                    h2 = h[r][2] * sh;
-                    if (MIRROR) {
-                        // (y' - x).n' = n.a - (-x.x n.x + x.y n.y + x.z n.z)
-                        const double sm2 = -(dt - fma(-xr[r][0], nx, xn_yz)) * area;
-                        h0 = fma(m[r][0], sm2, h0);
-                        h1 = fma(m[r][1], sm2, h1);
-                        h2 = fma(m[r][2], sm2, h2);
-                    }
-                }
-                double* rG = aG + r * cw;
-                double* rH = aH + r * cw;
-                if ((unsigned)lv[0] < (unsigned)cw) {
-                    rG[lv[0]] += g0;
-                    rH[lv[0]] += h0;
-                }
-                if ((unsigned)lv[1] < (unsigned)cw) {
-                    rG[lv[1]] += g1;
-                    rH[lv[1]] += h1;
-                }
-                if ((unsigned)lv[2] < (unsigned)cw) {
-                    rG[lv[2]] += g2;
-                    rH[lv[2]] += h2;
-                }
-            }
+    const int tb = grp_off[g], te = grp_off[g + 1];
+    for (int c0 = tb; c0 < te; c0 += ASM_TC) {
+        const int cnt = min(ASM_TC, te - c0);
+        __syncthreads();
+        for (int e = tid; e < cnt * (REC / 2); e += ROWS) {
+            int tt = e / (REC / 2), w = e - tt * (REC / 2);
+            const double2* src = reinterpret_cast<const double2*>(rec + (size_t)grp_tri[c0 + tt] * REC);
+            reinterpret_cast<double2*>(srec + tt * REC)[w] = src[w];
+        }
+        for (int e = tid; e < cnt; e += ROWS) {
+            int t = grp_tri[c0 + e];
+            sinfo[4 * e] = grp_slot[c0 + e];
+            sinfo[4 * e + 1] = tri[3 * t];
+            sinfo[4 * e + 2] = tri[3 * t + 1];
+            sinfo[4 * e + 3] = tri[3 * t + 2];
         }
         __syncthreads();
-    }
-    // epilogue: fixed-order row reductions, 4 pi diagonal, H.phi, contiguous row writes
-#pragma unroll 1
-    for (int r = 0; r < R; ++r) {
-        const int i = row[r];
-        if (i < 0) break;
-        double* rG = aG + r * cw;
-        double* rH = aH + r * cw;
-        double sh = 0.0, sb = 0.0;
-        for (int j = threadIdx.x; j < cw; j += ASM_THREADS) {
-            const double hv = rH[j];
-            sh += hv;
-            sb = fma(hv, phi[c0 + j], sb);
-        }
-        sh = block_sum_fixed(sh, s_red);
-        sb = block_sum_fixed(sb, s_red);
-        if (single) {
-            // H(i,i) -= 4 pi - val, val = -sum_j H(i,j)  (ColocSim.cpp:85-97)
-            const double d = -(4.0 * 3.14159265358979323846 + sh);
-            if (threadIdx.x == 0) {
-                rH[i - c0] += d;
-                if (b) b[i] = fma(d, phi[i], sb);
+        if (i < N) {
+            for (int tt = 0; tt < cnt; ++tt) {
+                const int4 info = reinterpret_cast<const int4*>(sinfo)[tt];
+                const int code = info.x;
+                if (i == info.y || i == info.z || i == info.w) {
+                    const int shift = (i == info.y) ? 0 : ((i == info.z) ? 1 : 2);
+                    singular_pair<MIRROR>(x, info.y, info.z, info.w, shift, code, accG + tid, accH + tid, ROWS);
+                    continue;
+                }
+                double g0, g1, g2, h0, h1, h2;
+                regular_pair<MIRROR>(srec + tt * REC, xi0, xi1, xi2, g0, g1, g2, h0, h1, h2);
+                const int s0 = code & SLOT_NONE, s1 = (code >> SLOT_BITS) & SLOT_NONE,
+                          s2 = (code >> (2 * SLOT_BITS)) & SLOT_NONE;
+                if (s0 != SLOT_NONE) {
+                    accG[s0 * ROWS + tid] += g0;
+                    accH[s0 * ROWS + tid] += h0;
+                }
+                if (s1 != SLOT_NONE) {
+                    accG[s1 * ROWS + tid] += g1;
+                    accH[s1 * ROWS + tid] += h1;
+                }
+                if (s2 != SLOT_NONE) {
+                    accG[s2 * ROWS + tid] += g2;
+                    accH[s2 * ROWS + tid] += h2;
+                }
             }
-            __syncthreads();
-        } else if (threadIdx.x == 0) {
-            rowHp[(size_t)chunk * N + i] = sh;
-            bp[(size_t)chunk * N + i] = sb;
         }
-        double* gG = G + (size_t)i * N + c0;
-        double* gH = H + (size_t)i * N + c0;
-        for (int j = threadIdx.x; j < cw; j += ASM_THREADS) {
-            gG[j] = rG[j];
-            gH[j] = rH[j];
+    }
+    __syncthreads();
+    if (i < N) {
+        double rs = 0.0, bs = 0.0;
+        for (int s = 0; s < CGT; ++s) {
+            int v = grp_vert[g * CGT + s];
+            if (v < 0) continue;
+            double gv = accG[s * ROWS + tid], hv = accH[s * ROWS + tid];
+            G[(size_t)v * N + i] = gv;
+            H[(size_t)v * N + i] = hv;
+            rs += hv;
+            bs = fma(hv, phi[v], bs);
         }
+        rowHp[(size_t)g * N + i] = rs;
+        bp[(size_t)g * N + i] = bs;
     }
 }
 
-// Multi-chunk finish: 4 pi diagonal and right-hand side from the per-chunk partials.
-__global__ void k_finish_rows(int N, int nchunks, const double* __restrict__ rowHp, const double* __restrict__ bp,
-                              const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
+// 4 pi rule and right-hand side: H(i,i) -= 4 pi - val, val = -sum_j H(i,j); b = H*phi.
+__global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
+                           const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    double sh = 0.0, sb = 0.0;
-    for (int k = 0; k < nchunks; ++k) {
-        sh += rowHp[(size_t)k * N + i];
-        sb += bp[(size_t)k * N + i];
+    double val = 0.0, bs = 0.0;
+    for (int g = 0; g < ngroups; ++g) {
+        val -= rowHp[(size_t)g * N + i];
+        bs += bp[(size_t)g * N + i];
     }
-    const double d = -(4.0 * 3.14159265358979323846 + sh);
+    double d = -(4.0 * 3.14159265358979323846 - val);
     H[(size_t)i * N + i] += d;
-    if (b) b[i] = fma(d, phi[i], sb);
+    if (b) b[i] = fma(d, phi[i], bs);
 }
 
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
     upload_constants();
-    const int64_t E = c.topo.E;
-    KLAUNCH(), k_triangle_records<<<(unsigned)((E + 127) / 128), 128, 0, s>>>(E, x, c.topo.ent, c.rec);
+    int M = (int)c.topo.M;
+    KLAUNCH(), k_triangle_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, c.topo.tri, c.rec);
 }
 
-size_t assemble_smem_bytes(int rows, int cw) { return sizeof(double) * 2 * (size_t)rows * cw; }
-
-template <bool MIRROR, int R>
-static void launch_rows(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b, cudaStream_t s) {
-    const Topology& t = c.topo;
-    const int N = (int)t.N;
-    int cwmax = 0;
-    for (int k = 0; k < t.nchunks; ++k) cwmax = std::max(cwmax, t.h_ch_c0[k + 1] - t.h_ch_c0[k]);
-    const size_t sm = assemble_smem_bytes(R, cwmax);
-    static int attr_set = 0;
-    if (attr_set < (int)sm) {
-        cudaFuncSetAttribute(k_assemble_rows<MIRROR, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        attr_set = (int)sm;
+template <bool MIRROR, int CGT, int ROWS, int MINB>
+static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    const size_t sm = sizeof(double) * (2 * CGT * ROWS + ASM_TC * REC) + sizeof(int) * 4 * ASM_TC;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_assemble<MIRROR, CGT, ROWS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
     }
-    dim3 grid((N + R - 1) / R, t.nchunks);
-    KLAUNCH(), k_assemble_rows<MIRROR, R><<<grid, ASM_THREADS, sm, s>>>(N, t.ch_c0, t.ncolors, t.col_off, t.ent, t.E,
-                                                                       c.rec, x, phi, G, H, b, c.rowHp, c.bp,
-                                                                       t.nchunks == 1 ? 1 : 0);
+    dim3 grid(c.topo.ngroups, (N + ROWS - 1) / ROWS);
+    KLAUNCH(), k_assemble<MIRROR, CGT, ROWS, MINB><<<grid, ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off,
+                                                                          c.topo.grp_tri, c.topo.grp_slot,
+                                                                          c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
 }
 
+// Tile shapes: 32 columns x 128 rows (12 warps/SM), 48 x 64 and 64 x 64 (fewer boundary triangles,
+// 6 warps/SM); all at 3 CTAs per SM within the 228 KB of shared memory.
 template <bool MIRROR>
-static void launch_rows_r(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b, cudaStream_t s) {
-    switch (c.topo.asm_rows) {
-        case 4:
-            launch_rows<MIRROR, 4>(c, x, phi, G, H, b, s);
+static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
+    switch (c.topo.cg) {
+        case 64:
+            launch_tiles_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s);
             break;
-        case 3:
-            launch_rows<MIRROR, 3>(c, x, phi, G, H, b, s);
-            break;
-        case 2:
-            launch_rows<MIRROR, 2>(c, x, phi, G, H, b, s);
+        case 48:
+            launch_tiles_t<MIRROR, 48, 64, 3>(c, x, phi, G, H, s);
             break;
         default:
-            launch_rows<MIRROR, 1>(c, x, phi, G, H, b, s);
+            launch_tiles_t<MIRROR, 32, 128, 3>(c, x, phi, G, H, s);
     }
 }
 
@@ -422,15 +413,14 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
         cudaEventRecord(e0, s);
     }
     if (c.prm.mirror)
-        launch_rows_r<true>(c, x, phi, G, H, b, s);
+        launch_tiles<true>(c, x, phi, G, H, s);
     else
-        launch_rows_r<false>(c, x, phi, G, H, b, s);
+        launch_tiles<false>(c, x, phi, G, H, s);
     if (c.prof) {
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }
-    if (c.topo.nchunks > 1)
-        KLAUNCH(), k_finish_rows<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.nchunks, c.rowHp, c.bp, phi, H, b);
+    KLAUNCH(), k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
 }
 
 }  // namespace bemb

@@ -2,6 +2,7 @@
 // preprocessing, and the per-step orchestration of LinLinSim::evolve_system_RK4 / evolve_system
 // (Bem/Simulation/LinLinSim.cpp:194-284) as a sequence of device kernels on one stream.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -42,11 +43,14 @@ static void free_all(Ctx& c) {
 
 // ---------------------------------------------------------------- topology preprocessing
 struct HostTopo {
-    std::vector<int> tri, csr_off, csr_idx, part_of_vert, part_off, part_tidx, tri_rot, ch_c0, col_off, ent;
-    int nparts = 0, nchunks = 0, ncolors = 0, asm_rows = 1;
+    int cg = 32;
+    std::vector<int> tri, csr_off, csr_idx, grp_off, grp_tri, grp_slot, grp_vert, part_of_vert, part_off,
+        part_tidx, tri_rot;
+    int ngroups = 0, nparts = 0;
 };
 
-static int build_topology(int64_t N, int64_t M, const int64_t* trigs, HostTopo& h, std::string& err) {
+static int build_topology(int64_t N, int64_t M, const int64_t* trigs, const double* verts, HostTopo& h,
+                          std::string& err) {
     h.tri.resize((size_t)(3 * M));
     for (int64_t j = 0; j < 3 * M; ++j) {
         if (trigs[j] < 0 || trigs[j] >= N) {
@@ -113,86 +117,68 @@ static int build_topology(int64_t N, int64_t M, const int64_t* trigs, HostTopo& 
         if (t[2] > t[r]) r = 2;
         for (int k = 0; k < 3; ++k) h.tri_rot[(size_t)(3 * j + k)] = t[(r + k) % 3];
     }
-    // assembly work list.  Rows per CTA and column chunks from the shared-memory budget: full rows
-    // when they fit (1..4 rows), else chunks of contiguous columns with 2 rows per CTA.
+    // assembly column groups: recursive coordinate bisection of the vertex positions into full
+    // groups of cg vertices (compact patches, so few triangles straddle two groups)
+    std::vector<int> grp((size_t)N, -1), slot((size_t)N, -1);
+    std::vector<std::vector<int>> members;
     {
-        const int64_t per_row = 16 * N;  // G and H, FP64
-        int rows = (int)std::min<int64_t>(4, ASM_SMEM_BUDGET / per_row);
-        int cw = (int)N;
-        if (rows < 1) {
-            rows = 2;
-            cw = ASM_SMEM_BUDGET / (16 * rows);
-        }
-        h.asm_rows = rows;
-        h.ch_c0.clear();
-        for (int64_t c0 = 0; c0 < N; c0 += cw) h.ch_c0.push_back((int)c0);
-        h.ch_c0.push_back((int)N);
-        h.nchunks = (int)h.ch_c0.size() - 1;
-        // colour classes: greedy in triangle order, a colour may not repeat a vertex; classes capped
-        // at a multiple of the CTA width so that they are balanced across the CTA's threads
-        int cmin = 0;
-        {
-            std::vector<uint64_t> used((size_t)N, 0);
-            for (int64_t j = 0; j < M; ++j) {
-                const int* t = &h.tri[(size_t)(3 * j)];
-                uint64_t u = used[(size_t)t[0]] | used[(size_t)t[1]] | used[(size_t)t[2]];
-                int col = 0;
-                while (col < 64 && (u >> col) & 1ull) ++col;
-                if (col >= 64) {
-                    err = "mesh vertex valence too high for the assembly colouring";
-                    return BEM_ERR_ARG;
+        std::vector<int> idx((size_t)N);
+        std::iota(idx.begin(), idx.end(), 0);
+        struct Rec {
+            static void go(std::vector<int>& idx, int lo, int hi, const double* xyz, int CG,
+                           std::vector<std::vector<int>>& out) {
+                const int n = hi - lo;
+                if (n <= CG) {
+                    out.emplace_back(idx.begin() + lo, idx.begin() + hi);
+                    return;
                 }
-                cmin = std::max(cmin, col + 1);
-                for (int k = 0; k < 3; ++k) used[(size_t)t[k]] |= 1ull << col;
-            }
-        }
-        int64_t target = (M + cmin - 1) / cmin;
-        int64_t cap = std::max<int64_t>(ASM_THREADS, (target / ASM_THREADS) * ASM_THREADS);
-        std::vector<int> color((size_t)M, -1);
-        int ncol = 0;
-        {
-            std::vector<uint64_t> used((size_t)N, 0);
-            std::vector<int64_t> count(64, 0);
-            for (int64_t j = 0; j < M; ++j) {
-                const int* t = &h.tri[(size_t)(3 * j)];
-                uint64_t u = used[(size_t)t[0]] | used[(size_t)t[1]] | used[(size_t)t[2]];
-                int col = 0;
-                while (col < 64 && (((u >> col) & 1ull) || count[(size_t)col] >= cap)) ++col;
-                if (col >= 64) {
-                    col = 0;  // caps exhausted: fall back to the first free colour
-                    while (col < 64 && (u >> col) & 1ull) ++col;
-                    if (col >= 64) {
-                        err = "mesh vertex valence too high for the assembly colouring";
-                        return BEM_ERR_ARG;
+                double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+                for (int k = lo; k < hi; ++k)
+                    for (int d = 0; d < 3; ++d) {
+                        mn[d] = std::min(mn[d], xyz[3 * (size_t)idx[(size_t)k] + d]);
+                        mx[d] = std::max(mx[d], xyz[3 * (size_t)idx[(size_t)k] + d]);
                     }
-                }
-                color[(size_t)j] = col;
-                count[(size_t)col]++;
-                ncol = std::max(ncol, col + 1);
-                for (int k = 0; k < 3; ++k) used[(size_t)t[k]] |= 1ull << col;
+                int ax = 0;
+                for (int d = 1; d < 3; ++d)
+                    if (mx[d] - mn[d] > mx[ax] - mn[ax]) ax = d;
+                std::stable_sort(idx.begin() + lo, idx.begin() + hi,
+                                 [&](int a, int b) { return xyz[3 * (size_t)a + ax] < xyz[3 * (size_t)b + ax]; });
+                const int ngr = (n + CG - 1) / CG;
+                const int left = (ngr / 2) * CG;
+                go(idx, lo, lo + left, xyz, CG, out);
+                go(idx, lo + left, hi, xyz, CG, out);
             }
+        };
+        Rec::go(idx, 0, (int)N, verts, h.cg, members);
+        for (size_t g = 0; g < members.size(); ++g)
+            for (size_t k = 0; k < members[g].size(); ++k) {
+                grp[(size_t)members[g][k]] = (int)g;
+                slot[(size_t)members[g][k]] = (int)k;
+            }
+    }
+    h.ngroups = (int)members.size();
+    h.grp_off.assign((size_t)h.ngroups + 1, 0);
+    const int CG = h.cg;
+    h.grp_vert.assign((size_t)h.ngroups * CG, -1);
+    for (int g = 0; g < h.ngroups; ++g) {
+        std::vector<int> tl;
+        for (int v : members[(size_t)g]) {
+            h.grp_vert[(size_t)g * CG + slot[(size_t)v]] = v;
+            for (int e = h.csr_off[(size_t)v]; e < h.csr_off[(size_t)v + 1]; ++e) tl.push_back(h.csr_idx[(size_t)e]);
         }
-        h.ncolors = ncol;
-        h.col_off.assign((size_t)h.nchunks * (ncol + 1), 0);
-        h.ent.clear();
-        for (int k = 0; k < h.nchunks; ++k) {
-            const int a = h.ch_c0[(size_t)k], bnd = h.ch_c0[(size_t)k + 1];
-            std::vector<std::vector<int>> bycol((size_t)ncol);
-            for (int64_t j = 0; j < M; ++j) {
-                const int* t = &h.tri[(size_t)(3 * j)];
-                bool touch = false;
-                for (int q = 0; q < 3; ++q) touch |= (t[q] >= a && t[q] < bnd);
-                if (touch) bycol[(size_t)color[(size_t)j]].push_back((int)j);
+        std::sort(tl.begin(), tl.end());
+        tl.erase(std::unique(tl.begin(), tl.end()), tl.end());
+        for (int t : tl) {
+            int code = 0;
+            for (int k = 0; k < 3; ++k) {
+                int v = h.tri[(size_t)(3 * t + k)];
+                int sl = (grp[(size_t)v] == g) ? slot[(size_t)v] : SLOT_NONE;
+                code |= sl << (SLOT_BITS * k);
             }
-            for (int col = 0; col < ncol; ++col) {
-                h.col_off[(size_t)k * (ncol + 1) + col] = (int)(h.ent.size() / 4);
-                for (int j : bycol[(size_t)col]) {
-                    h.ent.push_back(j);
-                    for (int q = 0; q < 3; ++q) h.ent.push_back(h.tri[(size_t)(3 * j + q)]);
-                }
-            }
-            h.col_off[(size_t)k * (ncol + 1) + ncol] = (int)(h.ent.size() / 4);
+            h.grp_tri.push_back(t);
+            h.grp_slot.push_back(code);
         }
+        h.grp_off[(size_t)g + 1] = (int)h.grp_tri.size();
     }
     return BEM_OK;
 }
@@ -335,22 +321,18 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     Topology& t = c.topo;
     t.N = N;
     t.M = M;
+    t.ngroups = h.ngroups;
+    t.cg = h.cg;
     t.nparts = h.nparts;
-    t.nchunks = h.nchunks;
-    t.ncolors = h.ncolors;
-    t.asm_rows = h.asm_rows;
-    t.E = (int64_t)(h.ent.size() / 4);
     t.h_part_of_vert = h.part_of_vert;
-    t.h_ch_c0 = h.ch_c0;
     int rc;
-    int* ent_raw = nullptr;
     if ((rc = upload(c, &t.tri, h.tri)) || (rc = upload(c, &t.csr_off, h.csr_off)) ||
-        (rc = upload(c, &t.csr_idx, h.csr_idx)) || (rc = upload(c, &t.ch_c0, h.ch_c0)) ||
-        (rc = upload(c, &t.col_off, h.col_off)) || (rc = upload(c, &ent_raw, h.ent)) ||
-        (rc = upload(c, &t.part_of_vert, h.part_of_vert)) || (rc = upload(c, &t.part_off, h.part_off)) ||
-        (rc = upload(c, &t.part_tidx, h.part_tidx)) || (rc = upload(c, &t.tri_rot, h.tri_rot)))
+        (rc = upload(c, &t.csr_idx, h.csr_idx)) || (rc = upload(c, &t.grp_off, h.grp_off)) ||
+        (rc = upload(c, &t.grp_tri, h.grp_tri)) || (rc = upload(c, &t.grp_slot, h.grp_slot)) ||
+        (rc = upload(c, &t.grp_vert, h.grp_vert)) || (rc = upload(c, &t.part_of_vert, h.part_of_vert)) ||
+        (rc = upload(c, &t.part_off, h.part_off)) || (rc = upload(c, &t.part_tidx, h.part_tidx)) ||
+        (rc = upload(c, &t.tri_rot, h.tri_rot)))
         return rc;
-    t.ent = reinterpret_cast<int4*>(ent_raw);
     const size_t n = (size_t)N, m = (size_t)M, nn = n * n;
     const int ncs = 64;
     double** vec3s[] = {&c.x, &c.x1, &c.xs, &c.k1, &c.k2, &c.k3, &c.k4, &c.vn};
@@ -361,9 +343,9 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     for (auto p : vecs)
         if ((rc = dalloc(c, p, n))) return rc;
     if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (rc = dalloc(c, &c.LU, nn)) ||
-        (rc = dalloc(c, &c.rec, (size_t)t.E * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) ||
-        (rc = dalloc(c, &c.tg, 3 * m)) || (rc = dalloc(c, &c.tk, m)) ||
-        (rc = dalloc(c, &c.rowHp, (size_t)h.nchunks * n)) || (rc = dalloc(c, &c.bp, (size_t)h.nchunks * n)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
+        (rc = dalloc(c, &c.rec, m * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) || (rc = dalloc(c, &c.tg, 3 * m)) ||
+        (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, (size_t)h.ngroups * n)) ||
+        (rc = dalloc(c, &c.bp, (size_t)h.ngroups * n)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)))
@@ -484,7 +466,12 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     cudaStreamSynchronize(c->stream);
     free_all(*c);
     HostTopo h;
-    int rc = build_topology(N, M, trigs, h, c->err);
+    // column-group width: 32 (128 rows per CTA) unless BEM_ASM_CG selects 48 or 64 (64 rows per CTA)
+    if (const char* e = getenv("BEM_ASM_CG")) {
+        int v = atoi(e);
+        if (v == 48 || v == 64 || v == 32) h.cg = v;
+    }
+    int rc = build_topology(N, M, trigs, verts, h, c->err);
     if (rc) return rc;
     if ((rc = alloc_mesh(*c, N, M, h))) return rc;
     BEM_CUDA(*c, cudaMemcpy(c->x, verts, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
@@ -604,15 +591,8 @@ int bem_assemble(bem_ctx* c, const double* verts, double* G, double* H) {
     BEM_CUDA(*c, cudaMemsetAsync(c->p1, 0, sizeof(double) * N, c->stream));
     launch_assemble(*c, x, c->p1, c->G, c->H, nullptr, c->stream);
     BEM_CUDA(*c, cudaGetLastError());
-    // internal storage is row-major; the ABI returns Eigen's column-major layout
-    if (G) {
-        transpose(N, c->G, c->LU, c->stream);
-        COPY_OUT(G, c->LU, N * N);
-    }
-    if (H) {
-        transpose(N, c->H, c->LU, c->stream);
-        COPY_OUT(H, c->LU, N * N);
-    }
+    if (G) COPY_OUT(G, c->G, N * N);
+    if (H) COPY_OUT(H, c->H, N * N);
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
 }
@@ -622,8 +602,7 @@ int bem_solve_system(bem_ctx* c, const double* G, const double* b, double* x) {
     NEED_MESH(c);
     const int64_t N = c->topo.N;
     if (!G || !b || !x) return c->fail(BEM_ERR_ARG, "null pointer");
-    COPY_IN(c->LU, G, N * N);
-    transpose(N, c->LU, c->G, c->stream);  // column-major input -> row-major storage
+    COPY_IN(c->G, G, N * N);
     COPY_IN(c->b, b, N);
     int rc = solve(*c, c->G, c->b, c->psil, c->stream);
     if (rc) return rc;

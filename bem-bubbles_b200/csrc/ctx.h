@@ -30,15 +30,15 @@ struct Ctx {
     DevScalars* h_sc = nullptr;  // pinned mirror
 
     // ---- per-stage work
-    double* G = nullptr;       // N*N row-major: G[i*N + j] = G(i, j)
-    double* H = nullptr;       // N*N row-major
+    double* G = nullptr;       // N*N column-major
+    double* H = nullptr;       // N*N column-major
     double* b = nullptr;       // N
     double* psil = nullptr;    // N, solved dphi/dn of the current stage
-    double* rec = nullptr;     // REC*E triangle records, field-major over the assembly entries
+    double* rec = nullptr;     // M*REC triangle records (quadrature points, normal, area)
     double* tn = nullptr;      // M*3 triangle unit normals (Mesh.cpp formula)
     double* tg = nullptr;      // M*3 tangential gradients of the stage potential
-    double* rowHp = nullptr;   // nchunks*N partial row sums of H (multi-chunk assembly)
-    double* bp = nullptr;      // nchunks*N partial H*phi
+    double* rowHp = nullptr;   // ngroups*N partial row sums of H
+    double* bp = nullptr;      // ngroups*N partial H*phi
     double* vol = nullptr;     // nparts volumes
     double* kap = nullptr;     // N mean curvature (sigma != 0)
     double* tk = nullptr;      // M per-triangle mean curvature
@@ -67,6 +67,7 @@ struct Ctx {
     double* Z = nullptr;       // N*m preconditioned directions
     double* hcol = nullptr;    // (m+2) Hessenberg column / dot results
     bool xinv_valid = false;
+    int ir_steps = 3;  // refinement steps issued per round of the mixed solve (adapted)
     int gmres_m = 30;
 
     // statistics

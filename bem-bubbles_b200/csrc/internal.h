@@ -17,13 +17,17 @@ namespace bemb {
 extern std::atomic<long long> g_kernel_launches;
 #define KLAUNCH() (::bemb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed))
 
-// Assembly CTA: ASM_THREADS threads, 1..4 full rows of G and H held in shared memory.
-constexpr int ASM_THREADS = 256;
-// Shared-memory budget of one assembly CTA (B200: up to 227 KB per CTA).
-constexpr int ASM_SMEM_BUDGET = 225 * 1024;
-// Fields of a triangle record (stored field-major): 7 quadrature points (21), unit normal (3),
-// area (1), plane offset n.a (1).
-constexpr int REC = 26;
+// Largest column-group width of the assembly tiles (a CTA owns up to CG_MAX columns of G and H);
+// the width used for a mesh is Topology::cg, with the rows per CTA tied to it (see assemble.cu).
+constexpr int CG_MAX = 64;
+// Per (group, triangle): the owned slot of each of the 3 vertices in SLOT_BITS-bit fields,
+// SLOT_NONE when the vertex belongs to another group.
+constexpr int SLOT_BITS = 7;
+constexpr int SLOT_NONE = 127;
+// Triangle records staged per chunk in shared memory.
+constexpr int ASM_TC = 40;
+// Doubles per triangle record: 7 quadrature points (21), unit normal (3), area (1), pad (3).
+constexpr int REC = 28;
 // Fixed block count of the vector kernels, so reductions have a fixed, deterministic shape.
 constexpr int VBLK = 128;
 constexpr int VTHR = 256;
@@ -34,15 +38,12 @@ struct Topology {
     int* tri = nullptr;          // M*3 int32, reference vertex order
     int* csr_off = nullptr;      // N+1, vertex -> incident triangles (increasing index)
     int* csr_idx = nullptr;      // 3M
-    // assembly work list: the columns are split into nchunks ranges [ch_c0[k], ch_c0[k+1]); chunk k
-    // lists every triangle touching its columns (entries ent_off[k]..ent_off[k+1]), grouped by
-    // colour, where no two triangles of one colour share a vertex (col_off: nchunks*(ncolors+1))
-    int nchunks = 0, ncolors = 0, asm_rows = 1;
-    int64_t E = 0;               // total entries
-    int* ch_c0 = nullptr;        // nchunks+1
-    int* col_off = nullptr;      // nchunks*(ncolors+1), absolute entry offsets
-    int4* ent = nullptr;         // E: (triangle, vertex a, vertex b, vertex c)
-    std::vector<int> h_ch_c0;
+    int ngroups = 0;             // assembly column groups
+    int cg = 32;                 // vertices per column group
+    int* grp_off = nullptr;      // ngroups+1 into grp_tri
+    int* grp_tri = nullptr;      // triangles incident to the group's vertices, increasing
+    int* grp_slot = nullptr;     // per grp_tri entry: 3 x SLOT_BITS owned-slot codes (SLOT_NONE = not owned)
+    int* grp_vert = nullptr;     // ngroups*cg vertex of each slot, -1 padding
     int nparts = 0;              // loose parts (bubbles)
     int* part_of_vert = nullptr; // N
     int* part_off = nullptr;     // nparts+1 into part_tidx
@@ -89,8 +90,6 @@ void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s);
 // linalg.cu
 void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part,
           unsigned* counters);
-void transpose(int64_t n, const double* A, double* B, cudaStream_t s);
-size_t assemble_smem_bytes(int rows, int cw);
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);

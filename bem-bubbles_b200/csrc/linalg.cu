@@ -21,6 +21,7 @@
 
 namespace bemb {
 
+constexpr int GV_ROWS = 256;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -62,90 +63,84 @@ __device__ double block_sum(double v) {
     return r;
 }
 
-// y = A x with A row-major N x N (T = double or float), x and y FP64: one warp per row, lanes
-// stride the row (each warp load is one coalesced 256-byte line for FP64), 4 independent
-// accumulators per lane, fixed shuffle tree.  Optional fused dots y.u and y.w: per-CTA partials
-// (fixed warp order), reduced by the consumer.
-constexpr int GV_WARPS = 8;
-
+// y = A x; A column-major (T = double or float), x and y FP64.  grid (row blocks, column splits).
+// Optional fused dots of the result: d1 = y.u, d2 = y.w partials per row block.
 template <typename T>
-__global__ void __launch_bounds__(32 * GV_WARPS, 4) k_gemv(int n, const T* __restrict__ A, const double* __restrict__ x,
-                                                      double* __restrict__ y, const int* __restrict__ gate,
-                                                      int gate_val, const double* __restrict__ u,
-                                                      double* __restrict__ du, const double* __restrict__ w,
-                                                      double* __restrict__ dw) {
+// y, u and w are not __restrict__: callers pass u == y to get y.y.  With cvec != null the result is
+// y = cvec + sgn * (A x) (residuals b - A x, accumulations x + X r); cvec may alias y.
+__global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, const T* __restrict__ A, const double* __restrict__ x,
+                                                  double* y, double* __restrict__ part,
+                                                  unsigned* __restrict__ cnt, const int* __restrict__ gate,
+                                                  int gate_val, const double* u, double* __restrict__ du,
+                                                  const double* w, double* __restrict__ dw, const double* cvec,
+                                                  double sgn) {
     if (gate && *gate != gate_val) return;
-    __shared__ double s_u[GV_WARPS], s_w[GV_WARPS];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int nw = gridDim.x * GV_WARPS;
-    double su = 0.0, sw = 0.0;
-    for (int i = blockIdx.x * GV_WARPS + wib; i < n; i += nw) {
-        const T* row = A + (size_t)i * n;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        int j = lane;
-        for (; j + 96 < n; j += 128) {
-            a0 = fma((double)__ldcs(row + j), __ldg(x + j), a0);
-            a1 = fma((double)__ldcs(row + j + 32), __ldg(x + j + 32), a1);
-            a2 = fma((double)__ldcs(row + j + 64), __ldg(x + j + 64), a2);
-            a3 = fma((double)__ldcs(row + j + 96), __ldg(x + j + 96), a3);
+    const int rb = blockIdx.x, cs = blockIdx.y, ncs = gridDim.y;
+    const int i = rb * GV_ROWS + threadIdx.x;
+    const int chunk = (n + ncs - 1) / ncs;
+    const int c0 = cs * chunk, c1 = min(n, c0 + chunk);
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    if (i < n) {
+        const T* col = A + (size_t)c0 * n + i;
+        int j = c0;
+        for (; j + 3 < c1; j += 4) {
+            T a0 = col[0], a1 = col[(size_t)n], a2 = col[2 * (size_t)n], a3 = col[3 * (size_t)n];
+            acc0 = fma((double)a0, __ldg(x + j), acc0);
+            acc1 = fma((double)a1, __ldg(x + j + 1), acc1);
+            acc2 = fma((double)a2, __ldg(x + j + 2), acc2);
+            acc3 = fma((double)a3, __ldg(x + j + 3), acc3);
+            col += 4 * (size_t)n;
         }
-        for (; j < n; j += 32) a0 = fma((double)__ldcs(row + j), __ldg(x + j), a0);
-        double v = warp_sum((a0 + a1) + (a2 + a3));
-        if (lane == 0) {
-            y[i] = v;
-            if (u) su = fma(v, u[i], su);
-            if (w) sw = fma(v, w[i], sw);
+        for (; j < c1; ++j) {
+            acc0 = fma((double)col[0], __ldg(x + j), acc0);
+            col += n;
         }
+        part[(size_t)cs * n + i] = (acc0 + acc1) + (acc2 + acc3);
     }
-    if (!du && !dw) return;
-    if (lane == 0) {
-        s_u[wib] = su;
-        s_w[wib] = sw;
-    }
+    __threadfence();
+    __shared__ unsigned s_ticket;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0.0, c = 0.0;
-        for (int k = 0; k < GV_WARPS; ++k) {
-            a += s_u[k];
-            c += s_w[k];
-        }
-        if (du) du[blockIdx.x] = a;
-        if (dw) dw[blockIdx.x] = c;
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&cnt[rb], 1u);
+    __syncthreads();
+    if (s_ticket != (unsigned)(ncs - 1)) return;
+    // last CTA of this row block: fixed-order sum of the column-split partials
+    __threadfence();
+    double yi = 0.0;
+    if (i < n) {
+        for (int k = 0; k < ncs; ++k) yi += __ldcg(part + (size_t)k * n + i);
+        if (cvec) yi = fma(sgn, yi, cvec[i]);
+        y[i] = yi;
     }
+    if (du) {
+        double v = (i < n) ? yi * u[i] : 0.0;
+        v = block_sum(v);
+        if (threadIdx.x == 0) du[rb] = v;
+    }
+    if (dw) {
+        double v = (i < n) ? yi * w[i] : 0.0;
+        v = block_sum(v);
+        if (threadIdx.x == 0) dw[rb] = v;
+    }
+    if (threadIdx.x == 0) cnt[rb] = 0u;
 }
 
-// CTAs of the GEMV: enough warps for one row each, at most 4 CTAs per SM.
-static int gemv_blocks(int n) { return std::max(1, std::min((n + GV_WARPS - 1) / GV_WARPS, 4 * 148)); }
+static int gemv_splits(int n) {
+    int rb = (n + GV_ROWS - 1) / GV_ROWS;
+    int cs = std::max(1, std::min(64, (4 * 148 + rb - 1) / rb));
+    cs = std::min(cs, std::max(1, n / 16));
+    return cs;
+}
 
 template <typename T>
-static void gemv_t(int n, const T* A, const double* x, double* y, cudaStream_t s, double* /*part*/,
-                   unsigned* /*cnt*/, const int* gate = nullptr, int gate_val = 0, const double* u = nullptr,
-                   double* du = nullptr, const double* w = nullptr, double* dw = nullptr) {
-    KLAUNCH(), k_gemv<T><<<gemv_blocks(n), 32 * GV_WARPS, 0, s>>>(n, A, x, y, gate, gate_val, u, du, w, dw);
+static void gemv_t(int n, const T* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt,
+                   const int* gate = nullptr, int gate_val = 0, const double* u = nullptr, double* du = nullptr,
+                   const double* w = nullptr, double* dw = nullptr, const double* cvec = nullptr, double sgn = 1.0) {
+    dim3 grid((n + GV_ROWS - 1) / GV_ROWS, gemv_splits(n));
+    KLAUNCH(), k_gemv<T><<<grid, GV_ROWS, 0, s>>>(n, A, x, y, part, cnt, gate, gate_val, u, du, w, dw, cvec, sgn);
 }
 
 void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt) {
     gemv_t<double>((int)n, A, x, y, s, part, cnt);
-}
-
-// B = A^T for N x N FP64 (layout conversion between row-major and column-major storage)
-__global__ void k_transpose(int n, const double* __restrict__ A, double* __restrict__ B) {
-    __shared__ double tile[32][33];
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        int c = bx + threadIdx.x, r = by + k;
-        tile[k][threadIdx.x] = (r < n && c < n) ? A[(size_t)r * n + c] : 0.0;
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-        int c = by + threadIdx.x, r = bx + k;
-        if (r < n && c < n) B[(size_t)r * n + c] = tile[threadIdx.x][k];
-    }
-}
-
-void transpose(int64_t n, const double* A, double* B, cudaStream_t s) {
-    dim3 g((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32)), b(32, 8);
-    KLAUNCH(), k_transpose<<<g, b, 0, s>>>((int)n, A, B);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -307,7 +302,7 @@ __global__ void k_bicg_xr(int n, int nrb, DevScalars* sc, const double* __restri
 
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
-    const int nrb = gemv_blocks(n);
+    const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
     double* red = c.red;
     // GEMV dot partial slots (one per row block) after the VBLK-sized vector slots
     double* g_r0v = red + RS_N * VBLK;
@@ -543,7 +538,7 @@ int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
     const int n = (int)c.topo.N;
     if ((size_t)n * sizeof(double) > 200 * 1024)
         return c.fail(BEM_ERR_ARG, "LU solver: N too large for the single-CTA substitution (N <= 25600)");
-    transpose(n, A, c.LU, s);  // row-major G -> column-major working copy
+    BEM_CUDA(c, cudaMemcpyAsync(c.LU, A, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemsetAsync(c.flag, 0, sizeof(int), s));
     for (int k0 = 0; k0 < n; k0 += LU_NB) {
         const int nb = std::min(LU_NB, n - k0);
@@ -715,13 +710,11 @@ static void sgemm(int n, const float* A, const float* B, float* C, cudaStream_t 
 static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
-    // row-major storage is the column-major transpose, so the column-major kernel computes
-    // C^T = B^T A^T: passing (X, G32) yields T = G X and (T, X) yields P = X T, both row-major
-    sgemm(n, c.Xinv, c.G32, c.Tw, s);  // T = G X
+    sgemm(n, c.G32, c.Xinv, c.Tw, s);  // T = G X
     KLAUNCH(), k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
     KLAUNCH(), k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
     float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
-    sgemm(n, c.Tw, c.Xinv, P, s);      // P = X T
+    sgemm(n, c.Xinv, c.Tw, P, s);      // P = X T
     KLAUNCH(), k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
     double v = 0.0;
     BEM_CUDA(c, cudaMemcpyAsync(&v, c.red + VBLK, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -842,7 +835,7 @@ __global__ void k_resid_final(const double* __restrict__ part, double* out) {
     }
 }
 
-int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+static int gmres_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
     const int m = c.gmres_m;
     const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
@@ -853,7 +846,6 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     double* hp = c.red;                    // partial slots: up to (m+1)*VBLK
     double* hh = c.hcol;                   // device h column (m+2)
     std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), hcol(m + 2);
-    BEM_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, s));
     int total_it = 0;
     double relres = 1.0;
     for (int cycle = 0; cycle < 20; ++cycle) {
@@ -924,16 +916,93 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         BEM_CUDA(c, cudaMemcpyAsync(hh, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
         KLAUNCH(), k_combine<<<VBLK, VTHR, 0, s>>>(n, k, c.Z, hh, x);
     }
-    c.stats.solves++;
-    c.stats.last_iters = total_it;
+    c.stats.last_iters += total_it;
     c.stats.last_rel_residual = relres;
     if (relres > tol) return c.fail(BEM_ERR_NOT_CONVERGED, "mixed GMRES did not reach the tolerance");
-    // keep the inverse fresh: refresh when the Krylov iteration count grows
-    if (total_it > 6) {
-        int rc = refresh_inverse(c, A, s, false);
+    return BEM_OK;
+}
+
+// ||b||^2 partials with the GEMV's row-block shape (one partial per GV_ROWS rows)
+__global__ void k_rowblock_norm2(int n, const double* __restrict__ b, double* __restrict__ part) {
+    const int i = blockIdx.x * GV_ROWS + threadIdx.x;
+    double v = (i < n) ? b[i] * b[i] : 0.0;
+    v = block_sum(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// Mixed solve.  Iterative refinement x <- x + X (b - G x): the residual in FP64 against the FP64 G
+// (so the limit is the FP64 solution), the correction through the FP32 approximate inverse X.
+// Warm-started from the previous solution (the previous RK4 stage's psi); K steps are issued
+// without host synchronisation, with the residual norms of every step kept on the device and read
+// once.  A contraction too weak for refinement hands over to GMRES (same preconditioner, same
+// start vector); a contraction above 0.02 triggers a Newton-Schulz refresh of X.
+int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
+    if (!c.xinv_valid) {
+        int rc = refresh_inverse(c, A, s, true);
         if (rc) return rc;
     }
-    return BEM_OK;
+    const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
+    constexpr int KMAX = 12;
+    double* pb = c.red;        // nrb
+    double* pr = c.red + nrb;  // (KMAX+1)*nrb
+    KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb);
+    std::vector<double> host((size_t)(KMAX + 2) * nrb);
+    c.stats.last_iters = 0;
+    int K = std::max(1, std::min(KMAX, c.ir_steps));
+    double rho = 1.0, rel = 1.0, rel0 = -1.0;
+    bool converged = false;
+    for (int round = 0; round < 4; ++round) {
+        for (int k = 0; k < K; ++k) {
+            gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr, nullptr, b, -1.0);
+            gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, nullptr, 0, nullptr, nullptr, nullptr, nullptr, x, 1.0);
+        }
+        gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b, -1.0);
+        BEM_CUDA(c, cudaMemcpyAsync(host.data(), c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
+        BEM_CUDA(c, cudaStreamSynchronize(s));
+        c.stats.last_iters += K;
+        double bb = 0.0;
+        for (int q = 0; q < nrb; ++q) bb += host[(size_t)q];
+        if (bb == 0.0) {
+            BEM_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+            rel = 0.0;
+            converged = true;
+            break;
+        }
+        std::vector<double> rk((size_t)K + 1);
+        for (int k = 0; k <= K; ++k) {
+            double a = 0.0;
+            for (int q = 0; q < nrb; ++q) a += host[(size_t)(1 + k) * nrb + q];
+            rk[(size_t)k] = sqrt(a / bb);
+        }
+        if (rel0 < 0) rel0 = rk[0];
+        rel = rk[(size_t)K];
+        // contraction per step, from the steps still well above the FP64 floor of the residual
+        rho = 0.0;
+        for (int k = 0; k < K; ++k)
+            if (rk[(size_t)k] > 1e3 * tol) rho = std::max(rho, rk[(size_t)k + 1] / rk[(size_t)k]);
+        if (rel <= tol) {
+            converged = true;
+            break;
+        }
+        if (!(rho < 0.3)) break;  // refinement too slow: GMRES below
+        K = std::max(1, std::min(KMAX, (int)ceil(log(tol / rel) / log(std::max(rho, 1e-6))) + 1));
+        if (rho == 0.0) K = 1;
+    }
+    int rc = BEM_OK;
+    if (!converged) {
+        rc = gmres_solve(c, A, b, x, s);
+        rho = 1.0;
+    } else {
+        c.stats.last_rel_residual = rel;
+    }
+    c.stats.solves++;
+    // steps for the next solve from the observed contraction, and the refresh policy
+    if (converged && rho > 0.0 && rel0 > tol)
+        c.ir_steps = std::max(1, std::min(KMAX, (int)ceil(log(tol / rel0) / log(std::max(rho, 1e-6)))));
+    if (rc == BEM_OK && rho > 0.02) rc = refresh_inverse(c, A, s, false);
+    return rc;
 }
 
 }  // namespace bemb

@@ -54,6 +54,18 @@ def test_assembly_nu10_matches_oracle_and_is_reproducible():
     assert rel(G, Go) < 1e-13 and rel(H, Ho) < 1e-13
 
 
+@pytest.mark.parametrize("cg", ["32", "48", "64"])
+def test_assembly_tile_shapes_agree(cg, monkeypatch):
+    # every column-group width of the tile kernel gives the same matrices (two bubbles, nu=7)
+    monkeypatch.setenv("BEM_ASM_CG", cg)
+    a = mesh.bubble(7, 1.0, (2.5, 0, 0))
+    b = mesh.bubble(7, 0.8, (4.9, 0, 0))
+    v, f = mesh.join([a, b])
+    G, H = ColocSim(v, f, mirror=True).assemble_matrices()
+    Go, Ho = O.assemble(v, f, True)
+    assert rel(G, Go) < 1e-13 and rel(H, Ho) < 1e-13
+
+
 def test_assembly_full_size_four_pi_rule():
     # N = 4002 (icosphere nu=20): sum_j H(i,j) = -4 pi for every row (ColocSim.cpp:85-97)
     v, f = mesh.bubble(20, 1.0, (2.0, 0.0, 0.0))
