@@ -85,6 +85,7 @@ SIGNATURES = {
     "bem_reset_profile": (C.c_int, [C.c_void_p]),
     "bem_measure_fma_peaks": (C.c_int, [C.c_int, _D, _D]),
     "bem_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "bem_gemm_bf16x3": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }
 
 _lib = None

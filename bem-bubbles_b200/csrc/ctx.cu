@@ -317,6 +317,20 @@ static int euler_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
     return BEM_OK;
 }
 
+// Buffers of the mixed solver: FP32 inverse, GEMM work, bf16 planes, Krylov basis.
+static int alloc_mixed(Ctx& c) {
+    const size_t n = (size_t)c.topo.N, nn = n * n, np = (size_t)tc_pad((int)n) * tc_pad((int)n);
+    uint16_t* planes = nullptr;
+    int rc;
+    if ((rc = dalloc(c, &c.Xinv, nn)) || (rc = dalloc(c, &c.Tw, nn)) || (rc = dalloc(c, &c.G32, nn)) ||
+        (rc = dalloc(c, &planes, 4 * np)) || (rc = dalloc(c, &c.tc_err, 1)) ||
+        (rc = dalloc(c, &c.V, n * (size_t)(c.gmres_m + 1))) || (rc = dalloc(c, &c.Z, n * (size_t)c.gmres_m)))
+        return rc;
+    c.tcp = planes;
+    BEM_CUDA(c, cudaMemset(c.tc_err, 0, sizeof(int)));
+    return BEM_OK;
+}
+
 static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     Topology& t = c.topo;
     t.N = N;
@@ -351,9 +365,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)))
         return rc;
     if (c.prm.solver == BEM_SOLVER_MIXED) {
-        if ((rc = dalloc(c, &c.Xinv, nn)) || (rc = dalloc(c, &c.Tw, nn)) || (rc = dalloc(c, &c.G32, nn)) ||
-            (rc = dalloc(c, &c.V, n * (size_t)(c.gmres_m + 1))) || (rc = dalloc(c, &c.Z, n * (size_t)c.gmres_m)))
-            return rc;
+        if ((rc = alloc_mixed(c))) return rc;
     }
     BEM_CUDA(c, cudaMemset(c.cnt, 0, sizeof(unsigned) * ((n + 255) / 256 + 1)));
     BEM_CUDA(c, cudaMemset(c.phi, 0, sizeof(double) * n));
@@ -364,12 +376,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
 
 static int ensure_mixed_buffers(Ctx& c) {
     if (c.Xinv || !c.have_mesh) return BEM_OK;
-    const size_t n = (size_t)c.topo.N, nn = n * n;
-    int rc;
-    if ((rc = dalloc(c, &c.Xinv, nn)) || (rc = dalloc(c, &c.Tw, nn)) || (rc = dalloc(c, &c.G32, nn)) ||
-        (rc = dalloc(c, &c.V, n * (size_t)(c.gmres_m + 1))) || (rc = dalloc(c, &c.Z, n * (size_t)c.gmres_m)))
-        return rc;
-    return BEM_OK;
+    return alloc_mixed(c);
 }
 
 }  // namespace bemb

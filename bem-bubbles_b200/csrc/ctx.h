@@ -63,6 +63,8 @@ struct Ctx {
     float* Xinv = nullptr;     // N*N column-major
     float* Tw = nullptr;       // N*N work for the Newton-Schulz refresh
     float* G32 = nullptr;      // N*N FP32 copy of G for the refresh GEMMs
+    void* tcp = nullptr;       // 4 bf16 operand planes of the split-precision tensor-core GEMM
+    int* tc_err = nullptr;     // error word of the tensor-core GEMM (bounded waits)
     double* V = nullptr;       // N*(m+1) Krylov basis
     double* Z = nullptr;       // N*m preconditioned directions
     double* hcol = nullptr;    // (m+2) Hessenberg column / dot results

@@ -87,6 +87,10 @@ void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cud
 void launch_any_negative(Ctx& c, const double* x, int* flag, cudaStream_t s);
 void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s);
 
+// tc_gemm.cu
+int tc_pad(int n);
+int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s);
+
 // linalg.cu
 void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part,
           unsigned* counters);

@@ -627,58 +627,6 @@ __global__ void k_scaled_transpose(int n, const double* __restrict__ A, const do
     }
 }
 
-// C = A * B, N x N column-major FP32, SIMT tiles 128x128x8, 8x8 per thread.
-__global__ void __launch_bounds__(256) k_sgemm(int n, const float* __restrict__ A, const float* __restrict__ B,
-                                               float* __restrict__ C) {
-    __shared__ float As[8][128];
-    __shared__ float Bs[8][128];
-    const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * 128, j0 = blockIdx.y * 128;
-    const int tx = tid % 16, ty = tid / 16;
-    float acc[8][8];
-#pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 8; ++b) acc[a][b] = 0.f;
-    for (int k0 = 0; k0 < n; k0 += 8) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            int idx = tid + 256 * e;  // 0..1023
-            int r = idx % 128, k = idx / 128;
-            int gi = i0 + r, gk = k0 + k;
-            As[k][r] = (gi < n && gk < n) ? A[(size_t)gk * n + gi] : 0.f;
-            int kk = idx % 8, c = idx / 8;
-            int gj = j0 + c, gk2 = k0 + kk;
-            Bs[kk][c] = (gj < n && gk2 < n) ? B[(size_t)gj * n + gk2] : 0.f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            float a[8], b[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                a[q] = As[k][tx + 16 * q];
-                b[q] = Bs[k][ty + 16 * q];
-            }
-#pragma unroll
-            for (int x = 0; x < 8; ++x)
-#pragma unroll
-                for (int y = 0; y < 8; ++y) acc[x][y] = fmaf(a[x], b[y], acc[x][y]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int y = 0; y < 8; ++y) {
-        int gj = j0 + ty + 16 * y;
-        if (gj >= n) continue;
-#pragma unroll
-        for (int x = 0; x < 8; ++x) {
-            int gi = i0 + tx + 16 * x;
-            if (gi < n) C[(size_t)gj * n + gi] = acc[x][y];
-        }
-    }
-}
-
 // Xn = 2 X - P ; and partial ||I - T||_F^2 of the T = G X just used
 __global__ void k_ns_combine(int64_t nn, const float* __restrict__ X, const float* __restrict__ P,
                              float* __restrict__ Xn) {
@@ -701,24 +649,23 @@ __global__ void k_sum_partials(const double* __restrict__ p, int np, double* out
     if (threadIdx.x == 0) *out = v;
 }
 
-static void sgemm(int n, const float* A, const float* B, float* C, cudaStream_t s) {
-    dim3 g((n + 127) / 128, (n + 127) / 128);
-    KLAUNCH(), k_sgemm<<<g, 256, 0, s>>>(n, A, B, C);
-}
-
 // One Newton-Schulz step X <- X (2I - G X); returns ||I - G X_old||_F / sqrt(n) (host value).
 static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
-    sgemm(n, c.G32, c.Xinv, c.Tw, s);  // T = G X
+    float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
+    int rc = tc_gemm(c, n, c.G32, c.Xinv, c.Tw, c.tcp, c.tc_err, s);  // T = G X
+    if (rc) return rc;
     KLAUNCH(), k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
     KLAUNCH(), k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
-    float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
-    sgemm(n, c.Xinv, c.Tw, P, s);      // P = X T
+    if ((rc = tc_gemm(c, n, c.Xinv, c.Tw, P, c.tcp, c.tc_err, s))) return rc;  // P = X T
     KLAUNCH(), k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
     double v = 0.0;
+    int herr = 0;
     BEM_CUDA(c, cudaMemcpyAsync(&v, c.red + VBLK, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaMemcpyAsync(&herr, c.tc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));
+    if (herr) return c.fail(BEM_ERR_CUDA, "tensor-core GEMM: bounded wait expired (code " + std::to_string(herr) + ")");
     *eres = sqrt(v / n);
     return BEM_OK;
 }

@@ -152,6 +152,11 @@ int bem_reset_profile(bem_ctx* ctx);
  * FMA throughput in TFLOP/s (2 flops per FMA).  Diagnostic; allocates and frees its own buffer. */
 int bem_measure_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops);
 
+/* C = A * B for FP32 column-major n x n host matrices through the split-precision tensor-core GEMM
+ * (tcgen05, bf16 hi/lo operand split, three MMAs per product, FP32 accumulation) that refreshes the
+ * mixed solver's approximate inverse.  Exposed for verification; allocates its own device buffers. */
+int bem_gemm_bf16x3(int device, int n, const float* A, const float* B, float* C);
+
 #ifdef __cplusplus
 }
 #endif
