@@ -86,6 +86,7 @@ SIGNATURES = {
     "bem_measure_fma_peaks": (C.c_int, [C.c_int, _D, _D]),
     "bem_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bem_gemm_bf16x3": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "bem_gemm_bf16x3_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
