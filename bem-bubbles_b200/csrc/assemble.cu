@@ -17,6 +17,7 @@
 // bit-reproducible run to run.  The same pass produces the per-group partial row sums of H and
 // partial H*phi, so the 4 pi diagonal and the right-hand side need no second read of H.
 #include <math.h>
+#include <mutex>
 
 #include "ctx.h"
 
@@ -36,8 +37,12 @@ __constant__ double c_orb[5];
 
 // Reference tables (quadrature.hpp:30-38 gauss_7, :88-96 quadrature_7), evaluated on the host once.
 static void upload_constants() {
-    static bool done = false;
-    if (done) return;
+    static std::mutex mu;
+    static uint64_t done_mask = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (done_mask & (1ull << (dev & 63))) return;
     const double Q[7][3] = {{0.33333333333333333, 0.33333333333333333, 0.22500000000000000 * 0.5},
                             {0.79742698535308720, 0.10128650732345633, 0.12593918054482717 * 0.5},
                             {0.10128650732345633, 0.79742698535308720, 0.12593918054482717 * 0.5},
@@ -79,7 +84,7 @@ static void upload_constants() {
     cudaMemcpyToSymbol(c_gcos, gc, sizeof(gc));
     cudaMemcpyToSymbol(c_gsin, gs, sizeof(gs));
     cudaMemcpyToSymbol(c_gw, gw, sizeof(gw));
-    done = true;
+    done_mask |= 1ull << (dev & 63);
 }
 
 // Per-triangle record: Interpolator (Interpolator.hpp:15-37) quantities and the 7 quadrature
@@ -376,11 +381,9 @@ template <bool MIRROR, int CGT, int ROWS, int MINB>
 static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
     const int N = (int)c.topo.N;
     const size_t sm = sizeof(double) * (2 * CGT * ROWS + ASM_TC * REC) + sizeof(int) * 4 * ASM_TC;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (first_on_device(attr))
         cudaFuncSetAttribute(k_assemble<MIRROR, CGT, ROWS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        attr = true;
-    }
     dim3 grid(c.topo.ngroups, (N + ROWS - 1) / ROWS);
     KLAUNCH(), k_assemble<MIRROR, CGT, ROWS, MINB><<<grid, ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off,
                                                                           c.topo.grp_tri, c.topo.grp_slot,

@@ -17,6 +17,15 @@ namespace bemb {
 extern std::atomic<long long> g_kernel_launches;
 #define KLAUNCH() (::bemb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed))
 
+// True on the first call for this mask on the current device (device-scoped one-time set-up:
+// kernel attributes and __constant__ tables exist once per device, not once per process).
+inline bool first_on_device(std::atomic<uint64_t>& mask) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    return !(mask.fetch_or(bit) & bit);
+}
+
 // Largest column-group width of the assembly tiles (a CTA owns up to CG_MAX columns of G and H);
 // the width used for a mesh is Topology::cg, with the rows per CTA tied to it (see assemble.cu).
 constexpr int CG_MAX = 64;
@@ -89,7 +98,8 @@ void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s);
 
 // tc_gemm.cu
 int tc_pad(int n);
-int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s);
+int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s,
+            int terms = 3);
 
 // linalg.cu
 void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part,

@@ -15,6 +15,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "ctx.h"
@@ -552,11 +553,8 @@ int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
         }
     }
     size_t sm = sizeof(double) * (size_t)n;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_lu_substitute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr{0};
+    if (first_on_device(attr)) cudaFuncSetAttribute(k_lu_substitute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     KLAUNCH(), k_lu_substitute<<<1, 1024, sm, s>>>(n, c.LU, c.piv, b, x);
     int sing = 0;
     BEM_CUDA(c, cudaMemcpyAsync(&sing, c.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -650,15 +648,16 @@ __global__ void k_sum_partials(const double* __restrict__ p, int np, double* out
 }
 
 // One Newton-Schulz step X <- X (2I - G X); returns ||I - G X_old||_F / sqrt(n) (host value).
-static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
+// terms: precision of the two products (3 = BF16x3, 1 = bf16).
+static int ns_step(Ctx& c, cudaStream_t s, double* eres, int terms = 3) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
     float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
-    int rc = tc_gemm(c, n, c.G32, c.Xinv, c.Tw, c.tcp, c.tc_err, s);  // T = G X
+    int rc = tc_gemm(c, n, c.G32, c.Xinv, c.Tw, c.tcp, c.tc_err, s, terms);  // T = G X
     if (rc) return rc;
     KLAUNCH(), k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
     KLAUNCH(), k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
-    if ((rc = tc_gemm(c, n, c.Xinv, c.Tw, P, c.tcp, c.tc_err, s))) return rc;  // P = X T
+    if ((rc = tc_gemm(c, n, c.Xinv, c.Tw, P, c.tcp, c.tc_err, s, terms))) return rc;  // P = X T
     KLAUNCH(), k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
     double v = 0.0;
     int herr = 0;
@@ -666,8 +665,91 @@ static int ns_step(Ctx& c, cudaStream_t s, double* eres) {
     BEM_CUDA(c, cudaMemcpyAsync(&herr, c.tc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));
     if (herr) return c.fail(BEM_ERR_CUDA, "tensor-core GEMM: bounded wait expired (code " + std::to_string(herr) + ")");
+    c.stats.ns_steps++;
     *eres = sqrt(v / n);
     return BEM_OK;
+}
+
+__global__ void k_fill(int n, double v, double* __restrict__ x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
+}
+// x = y / ||y|| from the per-row-block partials of y.y (every block sums them in the same order);
+// lam = ||y||.
+__global__ void k_scale_by_norm(int n, const double* __restrict__ part, int np, const double* __restrict__ y,
+                                double* __restrict__ x, double* __restrict__ lam) {
+    const double nrm = sqrt(block_reduce_partials(part, np));
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = y[i] * inv;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *lam = nrm;
+}
+// X = theta I (FP32)
+__global__ void k_scaled_identity(int n, double theta, float* __restrict__ X) {
+    const int64_t nn = (int64_t)n * n;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = e / n, i = e - j * n;
+        X[e] = (i == j) ? (float)theta : 0.f;
+    }
+}
+
+// Largest eigenvalue magnitude of A by power iteration in FP64 (a handful of GEMVs).  The
+// collocation single-layer matrix has a dominant constant mode separated from the next by a factor
+// of about three, so a dozen iterations from the constant vector resolve it.
+static int power_lambda(Ctx& c, const double* A, cudaStream_t s, double* lam) {
+    const int n = (int)c.topo.N;
+    const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
+    double* y = c.r0;
+    double* x = c.tv;
+    double* dl = c.red + nrb;
+    KLAUNCH(), k_fill<<<VBLK, VTHR, 0, s>>>(n, 1.0 / sqrt((double)n), x);
+    for (int it = 0; it < 12; ++it) {
+        gemv_t<double>(n, A, x, y, s, c.part, c.cnt, nullptr, 0, y, c.red);
+        KLAUNCH(), k_scale_by_norm<<<VBLK, VTHR, 0, s>>>(n, c.red, nrb, y, x, dl);
+    }
+    BEM_CUDA(c, cudaMemcpyAsync(lam, dl, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    return BEM_OK;
+}
+
+// Approximate inverse X ~ G^-1 in FP32 by Newton-Schulz (Schulz 1933; E_{k+1} = E_k^2 with
+// E = I - G X).  From scratch the start is X0 = I / lambda_max(G): the eigenvalues of the
+// collocation single-layer matrix are positive (it discretises a positive operator), so E0 has
+// spectral radius 1 - lambda_min/lambda_max and about log2(cond) steps suffice -- half of what the
+// classical X0 = G^T / (||G||_1 ||G||_inf) needs (cond^2).  Steps whose residual is still above
+// 0.25 run the GEMMs in plain bf16; the rest in BF16x3.  Should the scaled-identity start fail to
+// contract (a matrix with eigenvalues off the positive axis), the classical start takes over.
+static int ns_from_scratch(Ctx& c, const double* A, cudaStream_t s, bool classical) {
+    const int n = (int)c.topo.N;
+    int terms = 3;
+    if (!classical) {
+        double lam = 0.0;
+        int rc = power_lambda(c, A, s, &lam);
+        if (rc) return rc;
+        if (!(lam > 0.0) || !std::isfinite(lam)) return ns_from_scratch(c, A, s, true);
+        KLAUNCH(), k_scaled_identity<<<4 * 148, 256, 0, s>>>(n, 1.0 / lam, c.Xinv);
+        terms = 1;
+    } else {
+        double* cs = c.red + 2 * VBLK;
+        KLAUNCH(), k_abs_colsum<<<n, 256, 0, s>>>(n, A, c.r);
+        KLAUNCH(), k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, A, c.r0);
+        KLAUNCH(), k_max_two<<<1, 1024, 0, s>>>(n, c.r, c.r0, cs);
+        dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
+        KLAUNCH(), k_scaled_transpose<<<tg, tb, 0, s>>>(n, A, cs, c.Xinv);
+    }
+    double emin = 1e300;
+    for (int it = 0; it < 80; ++it) {
+        double e = 1.0;
+        int rc = ns_step(c, s, &e, terms);
+        if (rc) return rc;
+        if (terms == 3 && e < 1e-4) {
+            c.xinv_valid = true;
+            return BEM_OK;
+        }
+        if (!std::isfinite(e) || (it >= 4 && e > 2.0 * emin)) break;  // not contracting
+        emin = std::min(emin, e);
+        if (terms == 1 && e < 0.25) terms = 3;
+    }
+    if (!classical) return ns_from_scratch(c, A, s, true);
+    return c.fail(BEM_ERR_NOT_CONVERGED, "Newton-Schulz inverse did not converge");
 }
 
 static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_scratch) {
@@ -675,20 +757,9 @@ static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_sc
     const int64_t nn = (int64_t)n * n;
     KLAUNCH(), k_to_f32<<<4 * 148, 256, 0, s>>>(nn, A, c.G32);
     if (from_scratch || !c.xinv_valid) {
-        double* cs = c.red + 2 * VBLK;  // scratch of size >= 2n is not guaranteed here: use r/r0
-        KLAUNCH(), k_abs_colsum<<<n, 256, 0, s>>>(n, A, c.r);
-        KLAUNCH(), k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, A, c.r0);
-        KLAUNCH(), k_max_two<<<1, 1024, 0, s>>>(n, c.r, c.r0, cs);
-        dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
-        KLAUNCH(), k_scaled_transpose<<<tg, tb, 0, s>>>(n, A, cs, c.Xinv);
-        double e = 1.0;
-        int it = 0;
-        for (; it < 60; ++it) {
-            int rc = ns_step(c, s, &e);
-            if (rc) return rc;
-            if (e < 1e-4) break;
-        }
-        c.xinv_valid = true;
+        c.xinv_valid = false;
+        int rc = ns_from_scratch(c, A, s, false);
+        if (rc) return rc;
     } else {
         double e = 0.0;
         int rc = ns_step(c, s, &e);
@@ -939,6 +1010,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     }
     int rc = BEM_OK;
     if (!converged) {
+        c.stats.gmres_fallbacks++;
         rc = gmres_solve(c, A, b, x, s);
         rho = 1.0;
     } else {

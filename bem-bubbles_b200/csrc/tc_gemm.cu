@@ -3,6 +3,8 @@
 // lo = bf16(x - hi)) and the product formed as hi*hi + hi*lo + lo*hi with FP32 accumulation in
 // tensor memory ("BF16x3": about 16 significant bits per operand, three bf16 MMAs per product).
 // Used by the mixed solver's Newton-Schulz refresh of the approximate inverse (X <- X(2I - G X)).
+// TERMS = 1 keeps only hi*hi (plain bf16 inputs, FP32 accumulation): the early Newton-Schulz steps
+// of a from-scratch inverse, whose residual is still near 1, need no more.
 //
 // Structure: one CTA per 128 x BN tile of C, 128 threads.  Thread 0 issues TMA tile loads of the
 // four operand planes (128B-swizzled, K-major) into a STAGES-deep shared-memory ring guarded by
@@ -79,13 +81,14 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int TERMS>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                   float* __restrict__ C, int n, int ldc, int kblocks, int* __restrict__ err) {
     constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    constexpr uint32_t STAGE_TX = TERMS == 1 ? A_BYTES + B_BYTES : STAGE_BYTES;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
@@ -124,12 +127,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             uint8_t* st = smem + (size_t)s * STAGE_BYTES;
-            mbar_expect_tx(&full[s], STAGE_BYTES);
+            mbar_expect_tx(&full[s], STAGE_TX);
             const int kx = kb * TC_BK;
             tma_load_2d(st, &mAh, kx, m0, &full[s]);
-            tma_load_2d(st + A_BYTES, &mAl, kx, m0, &full[s]);
             tma_load_2d(st + 2 * A_BYTES, &mBh, kx, n0, &full[s]);
-            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, kx, n0, &full[s]);
+            if (TERMS == 3) {
+                tma_load_2d(st + A_BYTES, &mAl, kx, m0, &full[s]);
+                tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBl, kx, n0, &full[s]);
+            }
             issued = kb + 1;
         }
         // drain: every issued stage must land before the CTA may exit
@@ -154,8 +159,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint64_t ah = sdesc(st + k * 32), al = sdesc(st + A_BYTES + k * 32);
                 const uint64_t bh = sdesc(st + 2 * A_BYTES + k * 32), bl = sdesc(st + 2 * A_BYTES + B_BYTES + k * 32);
                 umma_bf16(tmem, ah, bh, idesc, (kb > 0 || k > 0) ? 1u : 0u);
-                umma_bf16(tmem, ah, bl, idesc, 1u);
-                umma_bf16(tmem, al, bh, idesc, 1u);
+                if (TERMS == 3) {
+                    umma_bf16(tmem, ah, bl, idesc, 1u);
+                    umma_bf16(tmem, al, bh, idesc, 1u);
+                }
             }
             umma_commit(&empty[s]);
         }
@@ -270,7 +277,9 @@ size_t tc_smem_bytes() { return (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 2 + 2 *
 
 // C = A * B (all FP32, column-major n x n, leading dimension n).  Work buffers: four bf16 planes
 // of tc_pad(n)^2 elements each (ah, al, bh, bl); err: device int (non-zero after a timeout).
-int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s) {
+// terms: 3 (BF16x3) or 1 (hi*hi only).
+int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s,
+            int terms) {
     const int npad = tc_pad(n);
     const size_t np = (size_t)npad * npad;
     __nv_bfloat16* ah = static_cast<__nv_bfloat16*>(planes);
@@ -283,13 +292,16 @@ int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* plane
         !make_map(&mBl, bl, npad, TC_BN))
         return c.fail(BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     const size_t sm = tc_smem_bytes();
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        attr = true;
+    static std::atomic<uint64_t> attr{0};
+    if (first_on_device(attr)) {
+        BEM_CUDA(c, cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        BEM_CUDA(c, cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     }
     dim3 grid(npad / TC_BN, npad / TC_BM);
-    KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
+    if (terms == 1)
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 1><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
+    else
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
     return BEM_OK;
 }
 

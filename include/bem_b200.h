@@ -126,6 +126,8 @@ typedef struct {
     int32_t last_iters;       /* iterations of the last iterative solve */
     int32_t precond_refresh;  /* refreshes of the mixed path's approximate inverse */
     double last_rel_residual; /* final relative residual of the last iterative solve */
+    int64_t ns_steps;         /* Newton-Schulz steps taken by the mixed path (set-up and refreshes) */
+    int64_t gmres_fallbacks;  /* mixed solves that handed over from refinement to GMRES */
 } bem_stats;
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 
