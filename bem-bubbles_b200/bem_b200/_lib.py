@@ -87,6 +87,13 @@ SIGNATURES = {
     "bem_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bem_gemm_bf16x3": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "bem_gemm_bf16x3_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "bem_set_mesh_blocks": (C.c_int, [C.c_void_p, C.c_int64, _D, C.c_int64, _I64, C.c_int32, _I64]),
+    "bem_num_blocks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "bem_set_block_params": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D]),
+    "bem_get_block_params": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D]),
+    "bem_get_block_stats": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(C.c_int32)]),
+    "bem_evolve_rk4_graph": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
+    "bem_autotune_assembly": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), _D]),
 }
 
 _lib = None

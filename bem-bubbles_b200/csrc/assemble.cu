@@ -267,29 +267,33 @@ __device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta,
     }
 }
 
-// Column-group tile kernel.  CGT: vertices (columns) per group, ROWS: rows per CTA (one per thread).
-template <bool MIRROR, int CGT, int ROWS, int MINB>
-__global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __restrict__ x, const int* __restrict__ tri,
-                                                         const double* __restrict__ rec, const int* __restrict__ grp_off,
-                                                         const int* __restrict__ grp_tri, const int* __restrict__ grp_slot,
-                                                         const int* __restrict__ grp_vert, const double* __restrict__ phi,
-                                                         double* __restrict__ G, double* __restrict__ H,
-                                                         double* __restrict__ rowHp, double* __restrict__ bp) {
-    extern __shared__ __align__(16) double smem[];
+// Column-group tile: the columns of group g (local index gl within its block) for rows
+// [row0, row0 + ROWS) clipped at rowend, of the block whose vertices start at vbase (n of them) and
+// whose G/H block starts at element mbase.  CGT: vertices (columns) per group, ROWS: rows per CTA
+// (one per thread).  Accumulators are thread-private columns of shared memory; the triangle
+// records of the group are staged in shared memory ASM_TC at a time.
+template <bool MIRROR, int CGT, int ROWS>
+__device__ __forceinline__ void assemble_tile(double* smem, const double* __restrict__ x, const int* __restrict__ tri,
+                                              const double* __restrict__ rec, const int* __restrict__ grp_off,
+                                              const int* __restrict__ grp_tri, const int* __restrict__ grp_slot,
+                                              const int* __restrict__ grp_vert, const double* __restrict__ phi,
+                                              double* __restrict__ G, double* __restrict__ H,
+                                              double* __restrict__ rowHp, double* __restrict__ bp, int g, int gl,
+                                              int row0, int rowend, int n, int vbase, long long mbase,
+                                              long long pbase) {
     double* accG = smem;                      // [CGT][ROWS]
     double* accH = accG + CGT * ROWS;         // [CGT][ROWS]
     double* srec = accH + CGT * ROWS;         // [ASM_TC][REC]
     int* sinfo = reinterpret_cast<int*>(srec + ASM_TC * REC);  // [ASM_TC][4]
-    const int g = blockIdx.x;
     const int tid = threadIdx.x;
-    const int i = blockIdx.y * ROWS + tid;
+    const int i = row0 + tid;
 #pragma unroll 4
     for (int s = 0; s < CGT; ++s) {
         accG[s * ROWS + tid] = 0.0;
         accH[s * ROWS + tid] = 0.0;
     }
     double xi0 = 0.0, xi1 = 0.0, xi2 = 0.0;
-    if (i < N) {
+    if (i < rowend) {
         xi0 = x[3 * i];
         xi1 = x[3 * i + 1];
         xi2 = x[3 * i + 2];
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __
             sinfo[4 * e + 3] = tri[3 * t + 2];
         }
         __syncthreads();
-        if (i < N) {
+        if (i < rowend) {
             for (int tt = 0; tt < cnt; ++tt) {
                 const int4 info = reinterpret_cast<const int4*>(sinfo)[tt];
                 const int code = info.x;
@@ -339,20 +343,63 @@ __global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __
             }
         }
     }
-    __syncthreads();
-    if (i < N) {
+    if (i < rowend) {
+        const int il = i - vbase;
         double rs = 0.0, bs = 0.0;
         for (int s = 0; s < CGT; ++s) {
             int v = grp_vert[g * CGT + s];
             if (v < 0) continue;
             double gv = accG[s * ROWS + tid], hv = accH[s * ROWS + tid];
-            G[(size_t)v * N + i] = gv;
-            H[(size_t)v * N + i] = hv;
+            const size_t o = (size_t)mbase + (size_t)(v - vbase) * n + il;
+            G[o] = gv;
+            H[o] = hv;
             rs += hv;
             bs = fma(hv, phi[v], bs);
         }
-        rowHp[(size_t)g * N + i] = rs;
-        bp[(size_t)g * N + i] = bs;
+        rowHp[(size_t)pbase + (size_t)gl * n + il] = rs;
+        bp[(size_t)pbase + (size_t)gl * n + il] = bs;
+    }
+}
+
+// Single system: one CTA per (column group, row tile).
+template <bool MIRROR, int CGT, int ROWS, int MINB>
+__global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __restrict__ x, const int* __restrict__ tri,
+                                                         const double* __restrict__ rec, const int* __restrict__ grp_off,
+                                                         const int* __restrict__ grp_tri, const int* __restrict__ grp_slot,
+                                                         const int* __restrict__ grp_vert, const double* __restrict__ phi,
+                                                         double* __restrict__ G, double* __restrict__ H,
+                                                         double* __restrict__ rowHp, double* __restrict__ bp) {
+    extern __shared__ __align__(16) double smem[];
+    assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp, bp,
+                                     blockIdx.x, blockIdx.x, blockIdx.y * ROWS, N, N, 0, 0, 0);
+}
+
+// Block-diagonal batch: one persistent launch over the work list of every block's tiles
+// {group, first row, block, local group}; CTAs take tiles from an atomic counter, which the CTA
+// that draws the last ticket resets for the next launch.
+template <bool MIRROR, int CGT, int ROWS, int MINB>
+__global__ void __launch_bounds__(ROWS, MINB)
+    k_assemble_batch(const int4* __restrict__ tiles, int ntiles, unsigned* __restrict__ ctr,
+                     const BlockInfo* __restrict__ blk, const double* __restrict__ x, const int* __restrict__ tri,
+                     const double* __restrict__ rec, const int* __restrict__ grp_off, const int* __restrict__ grp_tri,
+                     const int* __restrict__ grp_slot, const int* __restrict__ grp_vert, const double* __restrict__ phi,
+                     double* __restrict__ G, double* __restrict__ H, double* __restrict__ rowHp,
+                     double* __restrict__ bp) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ unsigned s_t;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_t = atomicAdd(ctr, 1u);
+            if (s_t == (unsigned)ntiles + gridDim.x - 1) *ctr = 0u;  // last ticket of this launch
+        }
+        __syncthreads();
+        const unsigned t = s_t;
+        if (t >= (unsigned)ntiles) break;
+        const int4 td = tiles[t];
+        const BlockInfo B = blk[td.z];
+        assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp,
+                                         bp, td.x, td.w, td.y, B.vbase + B.n, B.n, B.vbase, B.mbase, B.pbase);
     }
 }
 
@@ -368,6 +415,24 @@ __global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp,
     }
     double d = -(4.0 * 3.14159265358979323846 - val);
     H[(size_t)i * N + i] += d;
+    if (b) b[i] = fma(d, phi[i], bs);
+}
+
+// The same rule per block of a batch (rows of block vblk[i], its own groups and G/H block).
+__global__ void k_diag_rhs_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
+                                 const double* __restrict__ rowHp, const double* __restrict__ bp,
+                                 const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const BlockInfo B = blk[vblk[i]];
+    const int il = i - B.vbase;
+    double val = 0.0, bs = 0.0;
+    for (int g = 0; g < B.ngroups; ++g) {
+        val -= rowHp[(size_t)B.pbase + (size_t)g * B.n + il];
+        bs += bp[(size_t)B.pbase + (size_t)g * B.n + il];
+    }
+    double d = -(4.0 * 3.14159265358979323846 - val);
+    H[(size_t)B.mbase + (size_t)il * B.n + il] += d;
     if (b) b[i] = fma(d, phi[i], bs);
 }
 
@@ -390,10 +455,67 @@ static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G
                                                                           c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
 }
 
+template <int CGT, int ROWS>
+constexpr size_t tile_smem() {
+    return sizeof(double) * (2 * CGT * ROWS + ASM_TC * REC) + sizeof(int) * 4 * ASM_TC;
+}
+
+template <bool MIRROR, int CGT, int ROWS, int MINB>
+static void prepare_batch_t(Ctx& c) {
+    const size_t sm = tile_smem<CGT, ROWS>();
+    auto kern = k_assemble_batch<MIRROR, CGT, ROWS, MINB>;
+    static std::atomic<uint64_t> attr{0};
+    if (first_on_device(attr)) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (c.asm_grid_cg != CGT) {  // persistent grid: every CTA slot the SMs can hold
+        int per_sm = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ROWS, sm);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+        c.asm_grid = std::max(1, std::min(c.ntiles, std::max(1, per_sm) * sms));
+        c.asm_grid_cg = CGT;
+    }
+}
+
+template <bool MIRROR, int CGT, int ROWS, int MINB>
+static void launch_batch_t(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
+    const size_t sm = tile_smem<CGT, ROWS>();
+    auto kern = k_assemble_batch<MIRROR, CGT, ROWS, MINB>;
+    prepare_batch_t<MIRROR, CGT, ROWS, MINB>(c);
+    KLAUNCH(), kern<<<c.asm_grid, ROWS, sm, s>>>(c.tiles, c.ntiles, c.tile_ctr, c.blk, x, c.topo.tri, c.rec,
+                                                c.topo.grp_off, c.topo.grp_tri, c.topo.grp_slot, c.topo.grp_vert, phi,
+                                                G, H, c.rowHp, c.bp);
+}
+
 // Tile shapes: 32 columns x 128 rows (12 warps/SM), 48 x 64 and 64 x 64 (fewer boundary triangles,
 // 6 warps/SM); all at 3 CTAs per SM within the 228 KB of shared memory.
+void prepare_assemble(Ctx& c) {
+    if (!c.batch) return;
+    c.asm_grid_cg = 0;
+    if (c.prm.mirror) {
+        if (c.topo.cg == 64) prepare_batch_t<true, 64, 64, 3>(c);
+        else if (c.topo.cg == 48) prepare_batch_t<true, 48, 64, 3>(c);
+        else prepare_batch_t<true, 32, 128, 3>(c);
+    } else {
+        if (c.topo.cg == 64) prepare_batch_t<false, 64, 64, 3>(c);
+        else if (c.topo.cg == 48) prepare_batch_t<false, 48, 64, 3>(c);
+        else prepare_batch_t<false, 32, 128, 3>(c);
+    }
+}
+
 template <bool MIRROR>
 static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
+    if (c.batch) {
+        switch (c.topo.cg) {
+            case 64:
+                launch_batch_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s);
+                break;
+            case 48:
+                launch_batch_t<MIRROR, 48, 64, 3>(c, x, phi, G, H, s);
+                break;
+            default:
+                launch_batch_t<MIRROR, 32, 128, 3>(c, x, phi, G, H, s);
+        }
+        return;
+    }
     switch (c.topo.cg) {
         case 64:
             launch_tiles_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s);
@@ -423,7 +545,10 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }
-    KLAUNCH(), k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
+    if (c.batch)
+        KLAUNCH(), k_diag_rhs_batch<<<(N + 255) / 256, 256, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, phi, H, b);
+    else
+        KLAUNCH(), k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
 }
 
 }  // namespace bemb

@@ -7,6 +7,8 @@
 
 #include <algorithm>
 #include <deque>
+#include <map>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <set>
@@ -19,26 +21,47 @@ namespace bemb {
 std::atomic<long long> g_kernel_launches{0};
 
 // ---------------------------------------------------------------- device memory helpers
-template <typename T>
-static int dalloc(Ctx& c, T** p, size_t count) {
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        return c.fail(BEM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    }
-    c.allocs.push_back((void*)*p);
-    c.bytes += count * sizeof(T);
-    return BEM_OK;
-}
-
 static void free_all(Ctx& c) {
+    if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
+    c.graph_exec = nullptr;
     for (void* p : c.allocs) cudaFree(p);
     c.allocs.clear();
     c.bytes = 0;
     c.topo = Topology{};
     c.have_mesh = false;
     c.xinv_valid = false;
+    // every pointer into the freed allocations
+    c.G = c.H = c.LU = nullptr;
+    c.Xinv = c.Tw = c.G32 = nullptr;
+    c.tcp = nullptr;
+    c.tc_err = nullptr;
+    c.V = c.Z = nullptr;
+    c.batch = false;
+    c.nblk = 1;
+    c.h_blk.clear();
+    c.blk = nullptr;
+    c.vblk = nullptr;
+    c.tiles = nullptr;
+    c.ntiles = 0;
+    c.tile_ctr = nullptr;
+    c.asm_grid = c.asm_grid_cg = 0;
+    c.ppar = nullptr;
+    c.blk_elems = 0;
+    c.Xb = c.bG32 = c.bT = c.bP = nullptr;
+    c.gv_items = nullptr;
+    c.gv_nitems = 0;
+    c.bpart = nullptr;
+    c.bcnt = nullptr;
+    c.brnorm = nullptr;
+    c.bconv = nullptr;
+    c.bstat = nullptr;
+    c.bvalid.clear();
+    c.part_block.clear();
+    c.h_ppar.clear();
+    c.bmax_n = 0;
+    c.time_save = nullptr;
+    if (c.bstat_h) cudaFreeHost(c.bstat_h);
+    c.bstat_h = nullptr;
 }
 
 // ---------------------------------------------------------------- topology preprocessing
@@ -47,10 +70,13 @@ struct HostTopo {
     std::vector<int> tri, csr_off, csr_idx, grp_off, grp_tri, grp_slot, grp_vert, part_of_vert, part_off,
         part_tidx, tri_rot;
     int ngroups = 0, nparts = 0;
+    std::vector<int> blk_gbase;  // first group of each block (+ end), batches only
 };
 
+// blocks: vertex offsets of independent sub-systems (size nblocks + 1); column groups never span
+// two of them.  Empty: one block [0, N).
 static int build_topology(int64_t N, int64_t M, const int64_t* trigs, const double* verts, HostTopo& h,
-                          std::string& err) {
+                          std::string& err, const std::vector<int64_t>& blocks = {}) {
     h.tri.resize((size_t)(3 * M));
     for (int64_t j = 0; j < 3 * M; ++j) {
         if (trigs[j] < 0 || trigs[j] >= N) {
@@ -149,7 +175,16 @@ static int build_topology(int64_t N, int64_t M, const int64_t* trigs, const doub
                 go(idx, lo + left, hi, xyz, CG, out);
             }
         };
-        Rec::go(idx, 0, (int)N, verts, h.cg, members);
+        if (blocks.empty()) {
+            Rec::go(idx, 0, (int)N, verts, h.cg, members);
+        } else {
+            h.blk_gbase.clear();
+            for (size_t b = 0; b + 1 < blocks.size(); ++b) {
+                h.blk_gbase.push_back((int)members.size());
+                Rec::go(idx, (int)blocks[b], (int)blocks[b + 1], verts, h.cg, members);
+            }
+            h.blk_gbase.push_back((int)members.size());
+        }
         for (size_t g = 0; g < members.size(); ++g)
             for (size_t k = 0; k < members[g].size(); ++k) {
                 grp[(size_t)members[g][k]] = (int)g;
@@ -196,6 +231,7 @@ __global__ void k_set_dt(DevScalars* sc, double dt) { sc->dt = dt; }
 __global__ void k_set_time(DevScalars* sc, double t) { sc->time = t; }
 __global__ void k_set_V0(DevScalars* sc, double v) { sc->V0 = v; }
 __global__ void k_copy_vol(DevScalars* sc, const double* vol) { sc->V0 = vol[0]; }
+__global__ void k_add_time(DevScalars* sc, double d) { sc->time += d; }
 __global__ void k_total_volume(const double* vol, int np, double* out) {
     double s = 0.0;
     for (int p = 0; p < np; ++p) s += vol[p];
@@ -204,6 +240,7 @@ __global__ void k_total_volume(const double* vol, int np, double* out) {
 
 // ---------------------------------------------------------------- stage building blocks
 static int solve_impl(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    if (c.batch) return batch_mixed_solve(c, A, b, x, s);
     switch (c.prm.solver) {
         case BEM_SOLVER_LU:
             return lu_solve(c, A, b, x, s);
@@ -347,7 +384,14 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = upload(c, &t.part_off, h.part_off)) || (rc = upload(c, &t.part_tidx, h.part_tidx)) ||
         (rc = upload(c, &t.tri_rot, h.tri_rot)))
         return rc;
-    const size_t n = (size_t)N, m = (size_t)M, nn = n * n;
+    const size_t n = (size_t)N, m = (size_t)M;
+    // dense N x N, or the packed blocks of a batch
+    const size_t nn = c.batch ? (size_t)c.blk_elems : n * n;
+    size_t nrow_part = (size_t)h.ngroups * n;
+    if (c.batch) {
+        nrow_part = 0;
+        for (auto& B : c.h_blk) nrow_part += (size_t)B.ngroups * B.n;
+    }
     const int ncs = 64;
     double** vec3s[] = {&c.x, &c.x1, &c.xs, &c.k1, &c.k2, &c.k3, &c.k4, &c.vn};
     for (auto p : vec3s)
@@ -356,15 +400,15 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
                        &c.kp3, &c.kp4, &c.r, &c.r0, &c.pv, &c.vv, &c.yv, &c.zv, &c.sv, &c.tv, &c.invd};
     for (auto p : vecs)
         if ((rc = dalloc(c, p, n))) return rc;
-    if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (rc = dalloc(c, &c.LU, nn)) ||
+    if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (!c.batch && (rc = dalloc(c, &c.LU, nn))) ||
         (rc = dalloc(c, &c.rec, m * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) || (rc = dalloc(c, &c.tg, 3 * m)) ||
-        (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, (size_t)h.ngroups * n)) ||
-        (rc = dalloc(c, &c.bp, (size_t)h.ngroups * n)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
+        (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, nrow_part)) ||
+        (rc = dalloc(c, &c.bp, nrow_part)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)))
         return rc;
-    if (c.prm.solver == BEM_SOLVER_MIXED) {
+    if (!c.batch && c.prm.solver == BEM_SOLVER_MIXED) {
         if ((rc = alloc_mixed(c))) return rc;
     }
     BEM_CUDA(c, cudaMemset(c.cnt, 0, sizeof(unsigned) * ((n + 255) / 256 + 1)));
@@ -375,7 +419,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
 }
 
 static int ensure_mixed_buffers(Ctx& c) {
-    if (c.Xinv || !c.have_mesh) return BEM_OK;
+    if (c.Xinv || !c.have_mesh || c.batch) return BEM_OK;
     return alloc_mixed(c);
 }
 
@@ -493,6 +537,297 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     return BEM_OK;
 }
 
+// ---------------------------------------------------------------- batches of independent bubbles
+static int upload_ppar(Ctx& c) {
+    BEM_CUDA(c, cudaMemcpy(c.ppar, c.h_ppar.data(), sizeof(double) * c.h_ppar.size(), cudaMemcpyHostToDevice));
+    return BEM_OK;
+}
+
+int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, const int64_t* trigs, int32_t nblocks,
+                        const int64_t* vert_off) {
+    CTX_GUARD(c);
+    if (N < 3 || M < 1 || !verts || !trigs || nblocks < 1 || !vert_off)
+        return c->fail(BEM_ERR_ARG, "bad batch arguments");
+    if (N > (int64_t)1 << 24) return c->fail(BEM_ERR_ARG, "batch too large");
+    if (vert_off[0] != 0 || vert_off[nblocks] != N) return c->fail(BEM_ERR_ARG, "block offsets must run from 0 to N");
+    std::vector<int> vb((size_t)N);
+    for (int b = 0; b < nblocks; ++b) {
+        const int64_t n = vert_off[b + 1] - vert_off[b];
+        if (n < 3 || n > 65536) return c->fail(BEM_ERR_ARG, "block " + std::to_string(b) + ": size out of range");
+        for (int64_t i = vert_off[b]; i < vert_off[b + 1]; ++i) vb[(size_t)i] = b;
+    }
+    for (int64_t j = 0; j < M; ++j) {
+        for (int k = 0; k < 3; ++k)
+            if (trigs[3 * j + k] < 0 || trigs[3 * j + k] >= N) return c->fail(BEM_ERR_ARG, "triangle index out of range");
+        if (vb[(size_t)trigs[3 * j]] != vb[(size_t)trigs[3 * j + 1]] || vb[(size_t)trigs[3 * j]] != vb[(size_t)trigs[3 * j + 2]])
+            return c->fail(BEM_ERR_ARG, "triangle " + std::to_string(j) + " spans two blocks");
+    }
+    std::vector<int64_t> tr(trigs, trigs + 3 * M), voff(vert_off, vert_off + nblocks + 1);
+    cudaStreamSynchronize(c->stream);
+    const int keep_cg = c->batch_cg;
+    free_all(*c);
+    c->batch_cg = keep_cg;
+    HostTopo h;
+    if (c->batch_cg == 32 || c->batch_cg == 48 || c->batch_cg == 64) {
+        h.cg = c->batch_cg;
+    } else if (const char* e = getenv("BEM_ASM_CG")) {
+        int v = atoi(e);
+        if (v == 48 || v == 64 || v == 32) h.cg = v;
+    }
+    int rc = build_topology(N, M, trigs, verts, h, c->err, voff);
+    if (rc) return rc;
+    Ctx& C = *c;
+    C.batch = true;
+    C.nblk = nblocks;
+    C.h_blk.assign((size_t)nblocks, BlockInfo{});
+    long long mb = 0, pb = 0;
+    std::vector<int4> tiles;
+    const int rows = h.cg == 32 ? 128 : 64;
+    for (int b = 0; b < nblocks; ++b) {
+        BlockInfo& B = C.h_blk[(size_t)b];
+        B.n = (int)(voff[(size_t)b + 1] - voff[(size_t)b]);
+        B.vbase = (int)voff[(size_t)b];
+        B.gbase = h.blk_gbase[(size_t)b];
+        B.ngroups = h.blk_gbase[(size_t)b + 1] - B.gbase;
+        B.mbase = mb;
+        B.pbase = pb;
+        mb += (long long)B.n * B.n;
+        pb += (long long)B.ngroups * B.n;
+        for (int g = B.gbase; g < B.gbase + B.ngroups; ++g)
+            for (int r0 = B.vbase; r0 < B.vbase + B.n; r0 += rows) tiles.push_back(make_int4(g, r0, b, g - B.gbase));
+    }
+    C.blk_elems = mb;
+    C.ntiles = (int)tiles.size();
+    if ((rc = alloc_mesh(C, N, M, h))) return rc;
+    if ((rc = upload_vec(C, &C.tiles, tiles)) || (rc = upload_vec(C, &C.vblk, vb)) ||
+        (rc = dalloc(C, &C.tile_ctr, 1)) || (rc = dalloc(C, &C.time_save, 1)) || (rc = batch_setup_solver(C)))
+        return rc;
+    BEM_CUDA(C, cudaMemset(C.tile_ctr, 0, sizeof(unsigned)));
+    BEM_CUDA(C, cudaMemcpy(C.x, verts, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+    C.have_mesh = true;
+    C.h_trigs.swap(tr);
+    C.h_voff.swap(voff);
+    // every bubble is its own simulation: V_0 = its initial volume (Simulation.hpp:42), time = 0
+    cudaStream_t s = C.stream;
+    KLAUNCH(), k_set_time<<<1, 1, 0, s>>>(C.sc, 0.0);
+    launch_part_volumes(C, C.x, C.vol, s);
+    std::vector<double> vol((size_t)C.topo.nparts);
+    BEM_CUDA(C, cudaMemcpyAsync(vol.data(), C.vol, sizeof(double) * vol.size(), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(C, cudaStreamSynchronize(s));
+    C.part_block.assign((size_t)C.topo.nparts, -1);
+    for (int64_t i = 0; i < N; ++i) C.part_block[(size_t)h.part_of_vert[(size_t)i]] = vb[(size_t)i];
+    std::vector<double> vblock((size_t)nblocks, 0.0);
+    for (int p = 0; p < C.topo.nparts; ++p) vblock[(size_t)C.part_block[(size_t)p]] += vol[(size_t)p];
+    C.h_ppar.assign((size_t)5 * C.topo.nparts, 0.0);
+    for (int p = 0; p < C.topo.nparts; ++p) {
+        double* q = &C.h_ppar[(size_t)5 * p];
+        q[0] = vblock[(size_t)C.part_block[(size_t)p]];
+        q[1] = C.prm.field_amp;
+        q[2] = C.prm.field_kx;
+        q[3] = C.prm.field_omega;
+        q[4] = C.prm.field_phase;
+    }
+    if ((rc = dalloc(C, &C.ppar, C.h_ppar.size())) || (rc = upload_ppar(C))) return rc;
+    prepare_assemble(C);
+    BEM_CUDA(C, cudaGetLastError());
+    return BEM_OK;
+}
+
+int bem_num_blocks(const bem_ctx* c, int32_t* n) {
+    if (!c || !n) return BEM_ERR_ARG;
+    *n = c->batch ? c->nblk : 1;
+    return BEM_OK;
+}
+
+int bem_set_block_params(bem_ctx* c, const double* V0, const double* amp, const double* kx, const double* omega,
+                         const double* phase) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!c->batch) return c->fail(BEM_ERR_STATE, "not a batch");
+    for (int p = 0; p < c->topo.nparts; ++p) {
+        const int b = c->part_block[(size_t)p];
+        double* q = &c->h_ppar[(size_t)5 * p];
+        if (V0) q[0] = V0[b];
+        if (amp) q[1] = amp[b];
+        if (kx) q[2] = kx[b];
+        if (omega) q[3] = omega[b];
+        if (phase) q[4] = phase[b];
+    }
+    return upload_ppar(*c);
+}
+
+int bem_get_block_params(bem_ctx* c, double* V0, double* amp, double* kx, double* omega, double* phase) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!c->batch) return c->fail(BEM_ERR_STATE, "not a batch");
+    for (int p = 0; p < c->topo.nparts; ++p) {
+        const int b = c->part_block[(size_t)p];
+        const double* q = &c->h_ppar[(size_t)5 * p];
+        if (V0) V0[b] = q[0];
+        if (amp) amp[b] = q[1];
+        if (kx) kx[b] = q[2];
+        if (omega) omega[b] = q[3];
+        if (phase) phase[b] = q[4];
+    }
+    return BEM_OK;
+}
+
+int bem_get_block_stats(bem_ctx* c, double* rho, double* rel_residual, int32_t* steps) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!c->batch) return c->fail(BEM_ERR_STATE, "not a batch");
+    return batch_block_stats(*c, rho, rel_residual, steps);
+}
+
+// Fixed-dt RK4 steps of a batch; with graph != 0 each step is one replay of a captured CUDA graph.
+static int batch_steps(Ctx& c, double dt, int steps, bool graph) {
+    cudaStream_t s = c.stream;
+    if (c.field_cb) return c.fail(BEM_ERR_STATE, "batches evaluate the pressure field on the device (no callback)");
+    int rc = check_negative(c, s);
+    if (rc) return rc;
+    bool need = false;
+    for (char v : c.bvalid) need |= !v;
+    if (need) {  // approximate inverses of the blocks that have none, at the current state
+        launch_assemble(c, c.x, c.phi, c.G, c.H, c.b, s);
+        if ((rc = batch_build_inverses(c, s))) return rc;
+    }
+    if (graph && (!c.graph_exec || c.graph_dt != dt)) {
+        if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
+        c.graph_exec = nullptr;
+        prepare_assemble(c);
+        const bool prof = c.prof;
+        c.prof = false;
+        const long long l0 = g_kernel_launches.load();
+        cudaGraph_t g = nullptr;
+        BEM_CUDA(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        rc = rk4_step(c, dt, true, s);
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        c.prof = prof;
+        c.graph_launches = g_kernel_launches.load() - l0;
+        g_kernel_launches.fetch_sub(c.graph_launches);  // captured, not run
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return rc ? rc : c.fail(BEM_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&c.graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            c.graph_exec = nullptr;
+            return c.fail(BEM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+        }
+        c.graph_dt = dt;
+    }
+    const int64_t N = c.topo.N;
+    for (int k = 0; k < steps; ++k) {
+        BEM_CUDA(c, cudaMemcpyAsync(c.time_save, &c.sc->time, sizeof(double), cudaMemcpyDeviceToDevice, s));
+        for (int attempt = 0;; ++attempt) {
+            if (graph) {
+                BEM_CUDA(c, cudaGraphLaunch(c.graph_exec, s));
+                g_kernel_launches.fetch_add(c.graph_launches);
+            } else if ((rc = rk4_step(c, dt, true, s))) {
+                return rc;
+            }
+            bool redo = false;
+            if ((rc = batch_after_step(c, s, &redo))) return rc;
+            if (!redo) break;
+            if (attempt >= 2)
+                return c.fail(BEM_ERR_NOT_CONVERGED, "batched solve: a block missed the tolerance after refreshing its inverse");
+            // the step starts over from its saved start state (rk4_step copies x, phi to x1, p1 first)
+            BEM_CUDA(c, cudaMemcpyAsync(c.x, c.x1, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
+            BEM_CUDA(c, cudaMemcpyAsync(c.phi, c.p1, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+            BEM_CUDA(c, cudaMemcpyAsync(&c.sc->time, c.time_save, sizeof(double), cudaMemcpyDeviceToDevice, s));
+            c.stats.gmres_fallbacks++;  // counts repeated batched steps
+        }
+    }
+    BEM_CUDA(c, cudaGetLastError());
+    return check_negative(c, s);
+}
+
+int bem_evolve_rk4_graph(bem_ctx* c, double dt, int32_t steps) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!c->batch) return c->fail(BEM_ERR_STATE, "CUDA-graph stepping needs a batch (bem_set_mesh_blocks)");
+    return batch_steps(*c, dt, steps, true);
+}
+
+// Assembly tile shape of a batch chosen by timing: the column-group widths 32 (x 128 rows), 48 and 64
+// (x 64 rows) are each planned and timed over three assemblies of the current state; the fastest
+// is kept (and remembered per device and batch shape for later contexts).  ms: the three average
+// times, or null.
+int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!c->batch) return c->fail(BEM_ERR_STATE, "not a batch");
+    static std::mutex mu;
+    static std::map<std::string, int> cache;
+    const int64_t N = c->topo.N, M = c->topo.M;
+    std::string key = std::to_string(c->device) + ":" + std::to_string(N) + ":" + std::to_string(M) + ":" +
+                      std::to_string(c->prm.mirror);
+    for (auto& B : c->h_blk) key += ":" + std::to_string(B.n);
+    // current state to the host
+    std::vector<double> x((size_t)(3 * N)), phi((size_t)N), psi((size_t)N);
+    double t = 0.0;
+    cudaStream_t s = c->stream;
+    BEM_CUDA(*c, cudaMemcpyAsync(x.data(), c->x, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(phi.data(), c->phi, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(psi.data(), c->psi, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(&t, &c->sc->time, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    const std::vector<double> ppar = c->h_ppar;
+    const std::vector<int64_t> tr = c->h_trigs, voff = c->h_voff;
+    const int nb = c->nblk;
+    int best = 0;
+    double times[3] = {-1.0, -1.0, -1.0};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) best = it->second;
+    }
+    if (!best) {
+        const int cand[3] = {32, 48, 64};
+        double bt = 1e300;
+        for (int k = 0; k < 3; ++k) {
+            c->batch_cg = cand[k];
+            int rc = bem_set_mesh_blocks(c, N, x.data(), M, tr.data(), nb, voff.data());
+            if (rc) return rc;
+            BEM_CUDA(*c, cudaMemcpyAsync(c->phi, phi.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+            launch_assemble(*c, c->x, c->phi, c->G, c->H, c->b, s);  // warm-up
+            cudaEvent_t e0, e1;
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < 3; ++r) launch_assemble(*c, c->x, c->phi, c->G, c->H, c->b, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float el = 0.f;
+            cudaEventElapsedTime(&el, e0, e1);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            BEM_CUDA(*c, cudaGetLastError());
+            times[k] = el / 3.0;
+            if (times[k] < bt) {
+                bt = times[k];
+                best = cand[k];
+            }
+        }
+        std::lock_guard<std::mutex> lock(mu);
+        cache[key] = best;
+    }
+    c->batch_cg = best;
+    int rc = bem_set_mesh_blocks(c, N, x.data(), M, tr.data(), nb, voff.data());
+    if (rc) return rc;
+    c->h_ppar = ppar;
+    if ((rc = upload_ppar(*c))) return rc;
+    BEM_CUDA(*c, cudaMemcpyAsync(c->phi, phi.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(c->psi, psi.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    KLAUNCH(), k_set_time<<<1, 1, 0, s>>>(c->sc, t);
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    if (best_cg) *best_cg = best;
+    if (ms)
+        for (int k = 0; k < 3; ++k) ms[k] = times[k];
+    return BEM_OK;
+}
+
 int bem_num_verts(const bem_ctx* c, int64_t* n) {
     if (!c || !n) return BEM_ERR_ARG;
     *n = c->topo.N;
@@ -598,8 +933,9 @@ int bem_assemble(bem_ctx* c, const double* verts, double* G, double* H) {
     BEM_CUDA(*c, cudaMemsetAsync(c->p1, 0, sizeof(double) * N, c->stream));
     launch_assemble(*c, x, c->p1, c->G, c->H, nullptr, c->stream);
     BEM_CUDA(*c, cudaGetLastError());
-    if (G) COPY_OUT(G, c->G, N * N);
-    if (H) COPY_OUT(H, c->H, N * N);
+    const int64_t nn = c->batch ? (int64_t)c->blk_elems : N * N;  // batches: the packed blocks
+    if (G) COPY_OUT(G, c->G, nn);
+    if (H) COPY_OUT(H, c->H, nn);
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
 }
@@ -609,6 +945,7 @@ int bem_solve_system(bem_ctx* c, const double* G, const double* b, double* x) {
     NEED_MESH(c);
     const int64_t N = c->topo.N;
     if (!G || !b || !x) return c->fail(BEM_ERR_ARG, "null pointer");
+    if (c->batch) return c->fail(BEM_ERR_STATE, "bem_solve_system: not available for a batch");
     COPY_IN(c->G, G, N * N);
     COPY_IN(c->b, b, N);
     int rc = solve(*c, c->G, c->b, c->psil, c->stream);
@@ -661,6 +998,11 @@ int bem_pot_t_multi(bem_ctx* c, const double* verts, const double* grads, double
 int bem_evolve_rk4(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
     CTX_GUARD(c);
     NEED_MESH(c);
+    if (c->batch) {
+        if (!fixdt) return c->fail(BEM_ERR_STATE, "batches step with a fixed dt");
+        if (dt_out) *dt_out = dp;
+        return batch_steps(*c, dp, 1, false);
+    }
     int rc = check_negative(*c, c->stream);
     if (rc) return rc;
     if ((rc = rk4_step(*c, dp, fixdt != 0, c->stream))) return rc;
@@ -672,6 +1014,7 @@ int bem_evolve_rk4(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
 int bem_evolve_rk4_n(bem_ctx* c, double dt, int32_t steps) {
     CTX_GUARD(c);
     NEED_MESH(c);
+    if (c->batch) return batch_steps(*c, dt, steps, false);
     int rc = check_negative(*c, c->stream);
     if (rc) return rc;
     for (int k = 0; k < steps; ++k)
@@ -683,6 +1026,7 @@ int bem_evolve_rk4_n(bem_ctx* c, double dt, int32_t steps) {
 int bem_evolve_euler(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
     CTX_GUARD(c);
     NEED_MESH(c);
+    if (c->batch) return c->fail(BEM_ERR_STATE, "batches step with RK4 at a fixed dt");
     int rc = euler_step(*c, dp, fixdt != 0, c->stream);
     if (rc) return rc;
     BEM_CUDA(*c, cudaGetLastError());

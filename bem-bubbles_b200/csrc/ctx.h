@@ -72,6 +72,43 @@ struct Ctx {
     int ir_steps = 3;  // refinement steps issued per round of the mixed solve (adapted)
     int gmres_m = 30;
 
+    // ---- block-diagonal batch (batch = true): independent sub-systems (bubbles) sharing the mesh
+    // arrays; G and H are stored as packed n_b x n_b blocks
+    bool batch = false;
+    int batch_cg = 0;  // column-group width forced by the autotuner (0: default)
+    int nblk = 1;
+    std::vector<BlockInfo> h_blk;
+    BlockInfo* blk = nullptr;  // device copy
+    int* vblk = nullptr;       // N: block of each vertex
+    int4* tiles = nullptr;     // assembly work list {group, first row, block, local group}
+    int ntiles = 0;
+    unsigned* tile_ctr = nullptr;
+    int asm_grid = 0, asm_grid_cg = 0;  // persistent assembly grid and the tile shape it was sized for
+    double* ppar = nullptr;    // per part {V0, field amp, kx, omega, phase}; null: the scalar parameters
+    long long blk_elems = 0;   // sum of n_b^2
+    // batched mixed solve (batch.cu)
+    float* Xb = nullptr;        // packed FP32 approximate inverses
+    int4* gv_items = nullptr;   // GEMV work list {block, row block, column split, 0}
+    int gv_nitems = 0;
+    int nrb_total = 0;          // sum of row blocks
+    double* bpart = nullptr;    // batched GEMV column-split partials
+    unsigned* bcnt = nullptr;   // batched GEMV row-block counters
+    double* brnorm = nullptr;   // per row block residual norms
+    int* bconv = nullptr;       // per block: converged in the current solve
+    double* bstat = nullptr;    // per block: BSTAT_W doubles (norms, contraction)
+    double* bstat_h = nullptr;  // pinned host mirror
+    std::vector<char> bvalid;   // per block: inverse built
+    std::vector<int> part_block;      // block of each loose part
+    std::vector<double> h_ppar;       // host mirror of ppar
+    std::vector<int64_t> h_trigs, h_voff;  // the batch's triangles and block offsets (re-planning)
+    double* time_save = nullptr;      // device copy of the time at the start of a batched step
+    float *bG32 = nullptr, *bT = nullptr, *bP = nullptr;  // Newton-Schulz work, largest block
+    int bmax_n = 0;
+    // CUDA graph of one batched RK4 step
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_dt = 0.0;
+    long long graph_launches = 0;
+
     // statistics
     bem_stats stats{};
 
@@ -100,6 +137,28 @@ struct Ctx {
         return code;
     }
 };
+
+// Device allocation recorded in the context (freed together by free_all).
+template <typename T>
+inline int dalloc(Ctx& c, T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return c.fail(BEM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    c.allocs.push_back((void*)*p);
+    c.bytes += count * sizeof(T);
+    return BEM_OK;
+}
+template <typename T>
+inline int upload_vec(Ctx& c, T** dst, const std::vector<T>& src) {
+    int rc = dalloc(c, dst, src.size());
+    if (rc) return rc;
+    if (cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        return c.fail(BEM_ERR_CUDA, "cudaMemcpy (upload)");
+    return BEM_OK;
+}
 
 // Record a CUDA error in the context and map it to a status.
 #define BEM_CUDA(c, call)                                                              \

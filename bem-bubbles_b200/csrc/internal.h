@@ -74,12 +74,24 @@ struct DevScalars {
     int32_t pad[2];
 };
 
+// One independent sub-system of a block-diagonal batch (one bubble of a parameter sweep).  Its
+// vertices are the contiguous range [vbase, vbase + n) of the shared arrays; its G and H blocks are
+// n x n column-major at element offset mbase of the packed matrices; its column groups are
+// [gbase, gbase + ngroups) with partial row sums at pbase; its GEMV row blocks start at rbase, its
+// GEMV column splits number ncs with partials at pofs.
+struct BlockInfo {
+    int n, vbase, gbase, ngroups;
+    int rbase, ncs, pad0, pad1;
+    long long mbase, pbase, pofs;
+};
+
 struct Ctx;
 
 // assemble.cu
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s);
 void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b,
                      cudaStream_t s);
+void prepare_assemble(Ctx& c);  // kernel attributes and the persistent grid, outside any capture
 
 // stage.cu
 void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s);
@@ -96,6 +108,20 @@ void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cud
 void launch_any_negative(Ctx& c, const double* x, int* flag, cudaStream_t s);
 void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s);
 
+// Newton-Schulz job: X ~ A^-1 for an n x n column-major FP64 matrix A, with its FP32 copy G32 and
+// FP32 work matrices T, P (all n x n).
+struct NSJob {
+    int n;
+    const double* A;
+    float* G32;
+    float* X;
+    float* T;
+    float* P;
+};
+int ns_step(Ctx& c, const NSJob& j, cudaStream_t s, double* eres, int terms = 3);
+int ns_from_scratch(Ctx& c, const NSJob& j, cudaStream_t s, bool classical);
+void to_f32(int64_t nn, const double* a, float* b, cudaStream_t s);
+
 // tc_gemm.cu
 int tc_pad(int n);
 int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s,
@@ -107,5 +133,12 @@ void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+
+// batch.cu
+int batch_mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+int batch_setup_solver(Ctx& c);
+int batch_build_inverses(Ctx& c, cudaStream_t s);
+int batch_after_step(Ctx& c, cudaStream_t s, bool* redo);
+int batch_block_stats(Ctx& c, double* rho, double* rel, int32_t* steps);
 
 }  // namespace bemb

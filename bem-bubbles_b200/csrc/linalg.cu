@@ -647,18 +647,17 @@ __global__ void k_sum_partials(const double* __restrict__ p, int np, double* out
     if (threadIdx.x == 0) *out = v;
 }
 
-// One Newton-Schulz step X <- X (2I - G X); returns ||I - G X_old||_F / sqrt(n) (host value).
-// terms: precision of the two products (3 = BF16x3, 1 = bf16).
-static int ns_step(Ctx& c, cudaStream_t s, double* eres, int terms = 3) {
-    const int n = (int)c.topo.N;
+// One Newton-Schulz step X <- X (2I - G X) on job j; returns ||I - G X_old||_F / sqrt(n) (host
+// value).  terms: precision of the two products (3 = BF16x3, 1 = bf16).
+int ns_step(Ctx& c, const NSJob& j, cudaStream_t s, double* eres, int terms) {
+    const int n = j.n;
     const int64_t nn = (int64_t)n * n;
-    float* P = reinterpret_cast<float*>(c.LU);  // LU buffer reused as FP32 scratch in the mixed path
-    int rc = tc_gemm(c, n, c.G32, c.Xinv, c.Tw, c.tcp, c.tc_err, s, terms);  // T = G X
+    int rc = tc_gemm(c, n, j.G32, j.X, j.T, c.tcp, c.tc_err, s, terms);  // T = G X
     if (rc) return rc;
-    KLAUNCH(), k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, c.Tw, c.red);
+    KLAUNCH(), k_eye_resid<<<VBLK, VTHR, 0, s>>>(n, j.T, c.red);
     KLAUNCH(), k_sum_partials<<<1, 32, 0, s>>>(c.red, VBLK, c.red + VBLK);
-    if ((rc = tc_gemm(c, n, c.Xinv, c.Tw, P, c.tcp, c.tc_err, s, terms))) return rc;  // P = X T
-    KLAUNCH(), k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, c.Xinv, P, c.Xinv);
+    if ((rc = tc_gemm(c, n, j.X, j.T, j.P, c.tcp, c.tc_err, s, terms))) return rc;  // P = X T
+    KLAUNCH(), k_ns_combine<<<4 * 148, 256, 0, s>>>(nn, j.X, j.P, j.X);
     double v = 0.0;
     int herr = 0;
     BEM_CUDA(c, cudaMemcpyAsync(&v, c.red + VBLK, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -691,11 +690,10 @@ __global__ void k_scaled_identity(int n, double theta, float* __restrict__ X) {
     }
 }
 
-// Largest eigenvalue magnitude of A by power iteration in FP64 (a handful of GEMVs).  The
+// Largest eigenvalue magnitude of A (n x n) by power iteration in FP64 (a handful of GEMVs).  The
 // collocation single-layer matrix has a dominant constant mode separated from the next by a factor
 // of about three, so a dozen iterations from the constant vector resolve it.
-static int power_lambda(Ctx& c, const double* A, cudaStream_t s, double* lam) {
-    const int n = (int)c.topo.N;
+static int power_lambda(Ctx& c, int n, const double* A, cudaStream_t s, double* lam) {
     const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
     double* y = c.r0;
     double* x = c.tv;
@@ -717,52 +715,57 @@ static int power_lambda(Ctx& c, const double* A, cudaStream_t s, double* lam) {
 // classical X0 = G^T / (||G||_1 ||G||_inf) needs (cond^2).  Steps whose residual is still above
 // 0.25 run the GEMMs in plain bf16; the rest in BF16x3.  Should the scaled-identity start fail to
 // contract (a matrix with eigenvalues off the positive axis), the classical start takes over.
-static int ns_from_scratch(Ctx& c, const double* A, cudaStream_t s, bool classical) {
-    const int n = (int)c.topo.N;
+// Expects j.G32 = fp32(j.A).
+int ns_from_scratch(Ctx& c, const NSJob& j, cudaStream_t s, bool classical) {
+    const int n = j.n;
     int terms = 3;
     if (!classical) {
         double lam = 0.0;
-        int rc = power_lambda(c, A, s, &lam);
+        int rc = power_lambda(c, n, j.A, s, &lam);
         if (rc) return rc;
-        if (!(lam > 0.0) || !std::isfinite(lam)) return ns_from_scratch(c, A, s, true);
-        KLAUNCH(), k_scaled_identity<<<4 * 148, 256, 0, s>>>(n, 1.0 / lam, c.Xinv);
+        if (!(lam > 0.0) || !std::isfinite(lam)) return ns_from_scratch(c, j, s, true);
+        KLAUNCH(), k_scaled_identity<<<4 * 148, 256, 0, s>>>(n, 1.0 / lam, j.X);
         terms = 1;
     } else {
         double* cs = c.red + 2 * VBLK;
-        KLAUNCH(), k_abs_colsum<<<n, 256, 0, s>>>(n, A, c.r);
-        KLAUNCH(), k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, A, c.r0);
+        KLAUNCH(), k_abs_colsum<<<n, 256, 0, s>>>(n, j.A, c.r);
+        KLAUNCH(), k_abs_rowsum<<<(n + 255) / 256, 256, 0, s>>>(n, j.A, c.r0);
         KLAUNCH(), k_max_two<<<1, 1024, 0, s>>>(n, c.r, c.r0, cs);
         dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
-        KLAUNCH(), k_scaled_transpose<<<tg, tb, 0, s>>>(n, A, cs, c.Xinv);
+        KLAUNCH(), k_scaled_transpose<<<tg, tb, 0, s>>>(n, j.A, cs, j.X);
     }
     double emin = 1e300;
     for (int it = 0; it < 80; ++it) {
         double e = 1.0;
-        int rc = ns_step(c, s, &e, terms);
+        int rc = ns_step(c, j, s, &e, terms);
         if (rc) return rc;
-        if (terms == 3 && e < 1e-4) {
-            c.xinv_valid = true;
-            return BEM_OK;
-        }
+        if (terms == 3 && e < 1e-4) return BEM_OK;
         if (!std::isfinite(e) || (it >= 4 && e > 2.0 * emin)) break;  // not contracting
         emin = std::min(emin, e);
         if (terms == 1 && e < 0.25) terms = 3;
     }
-    if (!classical) return ns_from_scratch(c, A, s, true);
+    if (!classical) return ns_from_scratch(c, j, s, true);
     return c.fail(BEM_ERR_NOT_CONVERGED, "Newton-Schulz inverse did not converge");
+}
+
+void to_f32(int64_t nn, const double* a, float* b, cudaStream_t s) {
+    KLAUNCH(), k_to_f32<<<4 * 148, 256, 0, s>>>(nn, a, b);
 }
 
 static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_scratch) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
-    KLAUNCH(), k_to_f32<<<4 * 148, 256, 0, s>>>(nn, A, c.G32);
+    // LU buffer reused as FP32 scratch in the mixed path
+    const NSJob j{n, A, c.G32, c.Xinv, c.Tw, reinterpret_cast<float*>(c.LU)};
+    to_f32(nn, A, c.G32, s);
     if (from_scratch || !c.xinv_valid) {
         c.xinv_valid = false;
-        int rc = ns_from_scratch(c, A, s, false);
+        int rc = ns_from_scratch(c, j, s, false);
         if (rc) return rc;
+        c.xinv_valid = true;
     } else {
         double e = 0.0;
-        int rc = ns_step(c, s, &e);
+        int rc = ns_step(c, j, s, &e);
         if (rc) return rc;
         if (!(e < 0.9)) {  // diverging (stale X too far off): start over
             c.xinv_valid = false;

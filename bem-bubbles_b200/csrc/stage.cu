@@ -84,24 +84,36 @@ __global__ void k_part_volume(const double* __restrict__ x, const int* __restric
 
 // potential_t (Simulation.cpp:73-75) per vertex:
 // 2 sigma kappa + |grad|^2/2 + p_inf - epsilon (V0/V_part)^gamma + p_field(x, t_stepstart)
+// ppar (optional, batches of independent bubbles): per part {V0, amp, kx, omega, phase} in place of
+// the shared V0 and field parameters.
 __global__ void k_pot_t(int N, const double* __restrict__ x, const double* __restrict__ vel,
                         const int* __restrict__ part, const double* __restrict__ vol,
                         const double* __restrict__ kap, const double* __restrict__ fieldv,
                         const DevScalars* __restrict__ sc, double p_inf, double eps_gas, double sigma,
                         double gamma, double famp, double fkx, double fomega, double fphase, double t_host,
-                        int use_dev_time, double* __restrict__ out) {
+                        int use_dev_time, const double* __restrict__ ppar, double* __restrict__ out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     d3 g = ld3(vel, i);
-    double V = vol[part[i]];
+    const int p = part[i];
+    double V = vol[p];
     double t = use_dev_time ? sc->time : t_host;
+    double V0 = sc->V0;
+    if (ppar) {
+        const double* q = ppar + 5 * p;
+        V0 = q[0];
+        famp = q[1];
+        fkx = q[2];
+        fomega = q[3];
+        fphase = q[4];
+    }
     double f;
     if (fieldv)
         f = fieldv[i];
     else
         f = famp * sin(fkx * x[3 * i] + fomega * t + fphase);
     double k = kap ? kap[i] : 0.0;
-    out[i] = 2.0 * sigma * k + 0.5 * dot(g, g) + p_inf - eps_gas * pow(sc->V0 / V, gamma) + f;
+    out[i] = 2.0 * sigma * k + 0.5 * dot(g, g) + p_inf - eps_gas * pow(V0 / V, gamma) + f;
 }
 
 // Max-1999 vertex normals (Mesh.cpp:141-163)
@@ -368,7 +380,7 @@ void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* fiel
     KLAUNCH(), k_pot_t<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, vel, c.topo.part_of_vert, c.vol, kap, field_dev,
                                                c.sc, c.prm.p_inf, c.prm.epsilon, c.prm.sigma, c.prm.gamma,
                                                c.prm.field_amp, c.prm.field_kx, c.prm.field_omega,
-                                               c.prm.field_phase, 0.0, 1, out);
+                                               c.prm.field_phase, 0.0, 1, c.ppar, out);
 }
 void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k, double* out,
                   cudaStream_t s) {

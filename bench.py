@@ -6,12 +6,18 @@ phi=0, p_inf=1, epsilon=1, gamma=1.4, sigma=0, far-field pressure -0.8*sin(2*pi*
 fixed step, no wall image.  A "step" is one RK4 step (4 stages of assembly + solve + update).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solver mixed|bicgstab|lu]
-                  [--workload headline|pair]
+                  [--workload headline|pair|sweep]
 
 --workload pair runs the large two-bubble pair instead (two icospheres nu=40, N=32004 unknowns,
 radii 1.0 and 0.7, centres (2,0,0) and (4.2,0,0), phi = +0.4 and -0.14, epsilon=0, no field,
 dt=1e-3): mixed-precision RK4 steps/s, with the error of psi against the FP64 BiCGSTAB path on the
 same GPU at the first and the last state, and the one-time set-up of the approximate inverse.
+
+--workload sweep runs the batched parameter sweep: 256 independent bubbles, icosphere nu ~ U{4..16},
+R0 log-uniform in [0.5, 2] centred at (R0 + 1, 0, 0), far field -A sin(2 pi t/T) with A ~ U[0.1, 1.5],
+T ~ U[2, 10] (seed 0), phi = 0, epsilon = 1, gamma = 1.4, dt = 2e-3, mixed precision: bubble-steps/s of
+the batch (one CUDA graph per RK4 step, tile shape from the autotuner) against the same bubbles
+stepped one after another through the single-bubble path.
 
 ours: the mixed-precision path (FP64 assembly, FP64 GMRES, FP32 approximate-inverse preconditioner)
 through libbem_b200.so.  value = device time of K steps with the state resident in HBM (CUDA events
@@ -59,6 +65,18 @@ def pair_workload():
     v, f = mesh.join([(va, fa), (vb, fb)])
     phi = np.concatenate([np.full(len(va), 0.4), np.full(len(vb), -0.14)])
     return v, f, phi
+
+
+def sweep_workload(nb=256, seed=0):
+    from bem_b200 import mesh
+
+    rng = np.random.default_rng(seed)
+    nus = rng.integers(4, 17, size=nb)
+    R0 = np.exp(rng.uniform(np.log(0.5), np.log(2.0), size=nb))
+    A = rng.uniform(0.1, 1.5, size=nb)
+    T = rng.uniform(2.0, 10.0, size=nb)
+    meshes = [mesh.bubble(int(nu), float(r), (float(r) + 1.0, 0.0, 0.0)) for nu, r in zip(nus, R0)]
+    return meshes, nus, R0, -A, 2.0 * np.pi / T
 
 
 def dist_env():
@@ -405,6 +423,144 @@ def run_pair(args):
     return 0
 
 
+def run_sweep(args):
+    """Batched radius x pressure sweep (256 bubbles): replicas only, rank 0 reports."""
+    ws, rank, local = dist_env()
+    import torch
+
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+    from bem_b200.batch import BubbleBatch
+    from bem_b200.sim import ColocSim
+
+    dt = 2e-3
+    phys = dict(p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.4)
+    meshes, nus, R0, amp, om = sweep_workload()
+    nb = len(meshes)
+    bb = BubbleBatch(meshes, device=device, **phys)
+    bb.set_block_params(amp=amp, omega=om)
+    ext = torch.cuda.ExternalStream(bb.stream_handle(), device=device)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        bb.sync()
+        a.record(ext)
+        fn()
+        b.record(ext)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    tw = time.perf_counter()
+    cg, tune_ms = bb.autotune()
+    tune_s = time.perf_counter() - tw
+    tw = time.perf_counter()
+    bb.evolve_graph(dt, 1)  # approximate inverses of every bubble + graph capture + one step
+    bb.sync()
+    setup_s = time.perf_counter() - tw
+    for _ in range(args.warmup):
+        bb.evolve_graph(dt, 1)
+    st0 = bb.stats()
+    bb.reset_profile()
+    with ClockSampler(device) as clk:
+        el = timed(lambda: bb.evolve_graph(dt, args.steps))
+    launches = int(bb.profile().kernel_launches)
+    st1 = bb.stats()
+    value = ws * nb * args.steps / (el * 1e-3)
+
+    # end to end through the public API with host buffers (pinned), copies inside the timed region
+    N = bb.N
+    hx = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hphi = torch.empty(N, dtype=torch.float64, pin_memory=True).numpy()
+    hpsi = torch.empty(N, dtype=torch.float64, pin_memory=True).numpy()
+    hx[:], hphi[:], hpsi[:] = bb.get_vertices(), bb.get_phi(), bb.get_psi()
+    tw = time.perf_counter()
+    for _ in range(args.steps):
+        bb.set_vertices(hx)
+        bb.set_phi(hphi)
+        bb.set_psi(hpsi)
+        bb.evolve_graph(dt, 1)
+        hx[:], hphi[:], hpsi[:] = bb.get_vertices(), bb.get_phi(), bb.get_psi()
+    e2e_value = ws * nb * args.steps / (time.perf_counter() - tw)
+
+    # assembly kernel alone (one plain, profiled step), for the roofline
+    bb.set_profiling(True)
+    bb.reset_profile()
+    bb.evolve_rk4_steps(dt, 1)
+    prof = bb.profile()
+    bb.set_profiling(False)
+    avg_asm_ms = prof.assemble_ms / max(prof.assemble_launches, 1)
+    flops = sum(32.0 * (len(v) * len(f) - 3 * len(f)) * 7 for v, f in meshes)
+    from bem_b200.sim import measure_fma_peaks
+
+    fp64_peak, _ = measure_fma_peaks(device)
+    achieved = flops / (avg_asm_ms * 1e-3) / 1e12
+
+    # accuracy: batched psi against the FP64 BiCGSTAB single-bubble path on the same state
+    X, P = bb.get_vertices(), bb.get_phi()
+    _, psib = bb.position_t(P, return_psi=True)
+    errs = []
+    for b in np.linspace(0, nb - 1, 8).astype(int):
+        sl = bb.block(b)
+        sim = ColocSim(X[sl], meshes[b][1], solver="bicgstab", device=device, **phys)
+        _, p64 = sim.position_t(P[sl], return_psi=True)
+        errs.append(float(np.max(np.abs(psib[sl] - p64)) / max(np.max(np.abs(p64)), 1e-300)))
+        sim.close()
+
+    # sequential baseline: every bubble on its own through the single-bubble mixed path
+    seq_steps, seq_ms, seq_setup = 3, 0.0, 0.0
+    if not args.no_seq:
+        for b, (v, f) in enumerate(meshes):
+            sim = ColocSim(v, f, pressurefield=(float(amp[b]), float(om[b]), 0.0), solver="mixed", device=device,
+                           **phys)
+            sext = torch.cuda.ExternalStream(sim.stream_handle(), device=device)
+            tw = time.perf_counter()
+            sim.evolve_rk4_steps(dt, 2)
+            sim.sync()
+            seq_setup += time.perf_counter() - tw
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(sext)
+            for _ in range(seq_steps):
+                sim.evolve_system_RK4(dt, fixdt=True)
+            e.record(sext)
+            e.synchronize()
+            seq_ms += a.elapsed_time(e)
+            sim.close()
+    seq_value = nb * seq_steps / (seq_ms * 1e-3) if seq_ms > 0 else None
+    if rank != 0:
+        return 0
+    Ns = np.array([len(v) for v, _ in meshes])
+    line = {
+        "metric": "bubble RK4 steps/s, 256-bubble radius x pressure sweep: batched (CUDA graph) vs sequential GPU",
+        "value": value, "unit": "bubble-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (assembly, residual, state) + f32 (preconditioner)", "data": "synthetic",
+        "config": {"workload": "256 bubbles, nu~U{4..16}, R0 log-U[0.5,2], A~U[0.1,1.5], T~U[2,10], seed 0, "
+                               "phi=0, epsilon=1, gamma=1.4, RK4 dt=2e-3",
+                   "total_unknowns": int(Ns.sum()), "solver": "batched mixed",
+                   "l2": f"working set larger than L2 (G+H = {16 * float((Ns ** 2).sum()) / 1e9:.1f} GB per stage)"},
+        "sequential_gpu": {"value": seq_value, "unit": "bubble-steps/s", "steps_per_bubble": seq_steps,
+                           "solver": "mixed, one bubble at a time", "setup_s": seq_setup},
+        "speedup_vs_sequential": (value / ws / seq_value) if seq_value else None,
+        "autotune": {"chosen_column_group": cg, "ms_per_assembly": {"32x128": tune_ms[0], "48x64": tune_ms[1],
+                                                                     "64x64": tune_ms[2]}, "seconds": tune_s},
+        "setup_s_first_step": setup_s,
+        "during_timed_steps": {"ns_steps": int(st1.ns_steps - st0.ns_steps),
+                               "refreshes": int(st1.precond_refresh - st0.precond_refresh),
+                               "repeated_steps": int(st1.gmres_fallbacks - st0.gmres_fallbacks)},
+        "psi_rel_err_vs_fp64": {"max_over_8_bubbles": max(errs)},
+        "e2e": {"value": e2e_value, "unit": "bubble-steps/s", "h2d_bytes_per_step": 40 * N,
+                "d2h_bytes_per_step": 40 * N},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble_batch (persistent, all bubbles)",
+                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                     "flops_per_launch": flops, "avg_launch_ms": avg_asm_ms,
+                     "peak_source": "measured live: FP64 FMA-loop kernel (bem_measure_fma_peaks)"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,7 +569,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="mixed", choices=["mixed", "bicgstab", "lu"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="headline", choices=["headline", "pair"])
+    ap.add_argument("--workload", default="headline", choices=["headline", "pair", "sweep"])
+    ap.add_argument("--no-seq", action="store_true", help="sweep: skip the sequential baseline")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -421,6 +578,8 @@ def main():
         return run_reference(args)
     if args.workload == "pair":
         return run_pair(args)
+    if args.workload == "sweep":
+        return run_sweep(args)
     return run_ours(args)
 
 

@@ -120,6 +120,38 @@ int bem_evolve_euler(bem_ctx* ctx, double dp, int32_t fixdt, double* dt_out);
 /* `steps` RK4 steps with fixed dt without host synchronisation in between. */
 int bem_evolve_rk4_n(bem_ctx* ctx, double dt, int32_t steps);
 
+/* ---- Batches of independent bubbles (a radius x pressure sweep as in the reference's
+ * oscillations-array.sh, one process per point there).  No counterpart function in the reference:
+ * each bubble follows the reference's single-bubble path (LinLinSim::evolve_system_RK4 with its own
+ * V_0 and pressure field), and the bubbles do not interact.  The mesh is the concatenation of the
+ * bubbles' meshes: bubble b owns vertices [vert_off[b], vert_off[b+1]) and only triangles among them.
+ * G and H are block-diagonal (packed n_b x n_b blocks; bem_assemble returns them packed, block b at
+ * offset sum_{b'<b} n_b'^2).  A batch always uses the mixed solver, batched over all bubbles without
+ * host synchronisation; the pressure field is the device-evaluated family with per-bubble
+ * parameters.  Replaces the mesh like bem_set_mesh; each bubble's V_0 starts as its own volume and
+ * its field parameters as the context's. */
+int bem_set_mesh_blocks(bem_ctx* ctx, int64_t N, const double* verts, int64_t M, const int64_t* trigs,
+                        int32_t nblocks, const int64_t* vert_off);
+int bem_num_blocks(const bem_ctx* ctx, int32_t* nblocks);
+/* Per-bubble V_0 and field A*sin(kx*x + omega*t + phase); each array has nblocks entries or is NULL
+ * (unchanged). */
+int bem_set_block_params(bem_ctx* ctx, const double* V0, const double* amp, const double* kx,
+                         const double* omega, const double* phase);
+int bem_get_block_params(bem_ctx* ctx, double* V0, double* amp, double* kx, double* omega, double* phase);
+/* Per-bubble statistics of the last batched solve: contraction per refinement step, final relative
+ * residual, refinement steps used (any may be NULL). */
+int bem_get_block_stats(bem_ctx* ctx, double* rho, double* rel_residual, int32_t* steps);
+/* `steps` fixed-dt RK4 steps of a batch, each step one replay of a CUDA graph captured on the first
+ * call (and again when dt changes).  After each step the host reads the per-bubble statistics:
+ * stale approximate inverses are refreshed, and a bubble that missed the tolerance makes the step
+ * run again from its start state.  bem_evolve_rk4_n on a batch takes the same steps without the graph. */
+int bem_evolve_rk4_graph(bem_ctx* ctx, double dt, int32_t steps);
+/* Assembly tile shape of a batch by measurement: column groups of 32 (x 128 rows), 48 and 64 (x 64
+ * rows) are each planned and timed over three assemblies of the current state, and the fastest is
+ * kept (remembered per device and batch shape).  *best_cg receives the width, ms[3] the average
+ * times (either may be NULL).  The state is kept; approximate inverses are rebuilt on the next step. */
+int bem_autotune_assembly(bem_ctx* ctx, int32_t* best_cg, double* ms);
+
 /* Solver statistics of the most recent solve. */
 typedef struct {
     int64_t solves;           /* solves since creation */
