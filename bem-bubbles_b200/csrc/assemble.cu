@@ -35,14 +35,10 @@ __constant__ double c_gcos[7], c_gsin[7], c_gw[7];
 // c_orb = {w0*b0, cA, dA, cB, dB}.
 __constant__ double c_orb[5];
 
-// Reference tables (quadrature.hpp:30-38 gauss_7, :88-96 quadrature_7), evaluated on the host once.
-static void upload_constants() {
-    static std::mutex mu;
-    static uint64_t done_mask = 0;
-    std::lock_guard<std::mutex> lock(mu);
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (done_mask & (1ull << (dev & 63))) return;
+// Reference tables (quadrature.hpp:30-38 gauss_7, :88-96 quadrature_7) in the forms the kernels use:
+// per point the basis weights (1-u, u-v, v) * w of the triangle rule applied as (x+y, y) on the
+// unit triangle, and cos, sin and weight of the Gauss angles on (0, pi/4).
+void quad_tables(QuadTables& t) {
     const double Q[7][3] = {{0.33333333333333333, 0.33333333333333333, 0.22500000000000000 * 0.5},
                             {0.79742698535308720, 0.10128650732345633, 0.12593918054482717 * 0.5},
                             {0.10128650732345633, 0.79742698535308720, 0.12593918054482717 * 0.5},
@@ -57,33 +53,43 @@ static void upload_constants() {
                              {0.5 * (1.0 + 0.7415311855993945), 0.5 * 0.2797053914892766},
                              {0.5 * (1.0 - 0.9491079123427585), 0.5 * 0.1294849661688697},
                              {0.5 * (1.0 + 0.9491079123427585), 0.5 * 0.1294849661688697}};
-    double qc[7][3], quv[7][2], gc[7], gs[7], gw[7];
     for (int q = 0; q < 7; ++q) {
         double u = Q[q][0] + Q[q][1], v = Q[q][1], w = Q[q][2];
-        quv[q][0] = u;
-        quv[q][1] = v;
-        qc[q][0] = (1.0 - u) * w;
-        qc[q][1] = (u - v) * w;
-        qc[q][2] = v * w;
+        t.quv[q][0] = u;
+        t.quv[q][1] = v;
+        t.w[q] = w;
+        t.qc[q][0] = (1.0 - u) * w;
+        t.qc[q][1] = (u - v) * w;
+        t.qc[q][2] = v * w;
         double th = GL[q][0] * 0.78539816339744830962;
-        gc[q] = cos(th);
-        gs[q] = sin(th);
-        gw[q] = GL[q][1];
+        t.gc[q] = cos(th);
+        t.gs[q] = sin(th);
+        t.gw[q] = GL[q][1];
     }
     // orbit form: point 0 is the centroid; points 3,1,2 carry alpha on vertex 0,1,2 (orbit A) and
     // points 6,4,5 (orbit B), with barycentric coordinates (1-u, u-v, v)
-    {
-        const double w0 = Q[0][2], wA = Q[1][2], wB = Q[4][2];
-        const double aA = 1.0 - (Q[3][0] + Q[3][1]), bA = Q[3][1];  // point 3: (alpha, beta, beta)
-        const double aB = 1.0 - (Q[6][0] + Q[6][1]), bB = Q[6][1];  // point 6
-        const double orb[5] = {w0 * (1.0 / 3.0), wA * bA, wA * (aA - bA), wB * bB, wB * (aB - bB)};
-        cudaMemcpyToSymbol(c_orb, orb, sizeof(orb));
-    }
-    cudaMemcpyToSymbol(c_qc, qc, sizeof(qc));
-    cudaMemcpyToSymbol(c_quv, quv, sizeof(quv));
-    cudaMemcpyToSymbol(c_gcos, gc, sizeof(gc));
-    cudaMemcpyToSymbol(c_gsin, gs, sizeof(gs));
-    cudaMemcpyToSymbol(c_gw, gw, sizeof(gw));
+    const double w0 = Q[0][2], wA = Q[1][2], wB = Q[4][2];
+    const double aA = 1.0 - (Q[3][0] + Q[3][1]), bA = Q[3][1];  // point 3: (alpha, beta, beta)
+    const double aB = 1.0 - (Q[6][0] + Q[6][1]), bB = Q[6][1];  // point 6
+    const double orb[5] = {w0 * (1.0 / 3.0), wA * bA, wA * (aA - bA), wB * bB, wB * (aB - bB)};
+    for (int k = 0; k < 5; ++k) t.orb[k] = orb[k];
+}
+
+static void upload_constants() {
+    static std::mutex mu;
+    static uint64_t done_mask = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (done_mask & (1ull << (dev & 63))) return;
+    QuadTables t;
+    quad_tables(t);
+    cudaMemcpyToSymbol(c_orb, t.orb, sizeof(t.orb));
+    cudaMemcpyToSymbol(c_qc, t.qc, sizeof(t.qc));
+    cudaMemcpyToSymbol(c_quv, t.quv, sizeof(t.quv));
+    cudaMemcpyToSymbol(c_gcos, t.gc, sizeof(t.gc));
+    cudaMemcpyToSymbol(c_gsin, t.gs, sizeof(t.gs));
+    cudaMemcpyToSymbol(c_gw, t.gw, sizeof(t.gw));
     done_mask |= 1ull << (dev & 63);
 }
 

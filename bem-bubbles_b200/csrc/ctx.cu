@@ -62,6 +62,7 @@ static void free_all(Ctx& c) {
     c.time_save = nullptr;
     if (c.bstat_h) cudaFreeHost(c.bstat_h);
     c.bstat_h = nullptr;
+    c.adj = AdjWork{};
 }
 
 // ---------------------------------------------------------------- topology preprocessing
@@ -422,6 +423,9 @@ static int ensure_mixed_buffers(Ctx& c) {
     if (c.Xinv || !c.have_mesh || c.batch) return BEM_OK;
     return alloc_mixed(c);
 }
+int ensure_mixed(Ctx& c) { return ensure_mixed_buffers(c); }
+int solve_dev(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) { return solve(c, A, b, x, s); }
+int rk4_step_dev(Ctx& c, double dt, cudaStream_t s) { return rk4_step(c, dt, true, s); }
 
 }  // namespace bemb
 
@@ -825,6 +829,75 @@ int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
     if (best_cg) *best_cg = best;
     if (ms)
         for (int k = 0; k < 3; ++k) ms[k] = times[k];
+    return BEM_OK;
+}
+
+// ---------------------------------------------------------------- adjoint
+int bem_adjoint_record(bem_ctx* c, double dt, int32_t steps) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    return adjoint_record(*c, dt, steps);
+}
+
+int bem_adjoint_backward(bem_ctx* c, const double* xbar_end, const double* phibar_end, double* xbar0, double* phibar0) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!xbar_end || !phibar_end || !xbar0 || !phibar0) return c->fail(BEM_ERR_ARG, "null pointer");
+    if (c->adj.steps < 1) return c->fail(BEM_ERR_STATE, "adjoint: no recorded trajectory");
+    const int64_t N = c->topo.N;
+    cudaStream_t s = c->stream;
+    BEM_CUDA(*c, cudaMemcpyAsync(c->adj.iox, xbar_end, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(c->adj.iop, phibar_end, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    int rc = adjoint_backward(*c, c->adj.iox, c->adj.iop);
+    if (rc) return rc;
+    BEM_CUDA(*c, cudaMemcpyAsync(xbar0, c->adj.iox, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(phibar0, c->adj.iop, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    return BEM_OK;
+}
+
+int bem_adjoint_backward_device(bem_ctx* c, double* xbar, double* phibar) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!xbar || !phibar) return c->fail(BEM_ERR_ARG, "null pointer");
+    int rc = adjoint_backward(*c, xbar, phibar);
+    if (rc) return rc;
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return BEM_OK;
+}
+
+int bem_volume_gradient(bem_ctx* c, double* xbar) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!xbar) return c->fail(BEM_ERR_ARG, "null pointer");
+    cudaStream_t s = c->stream;
+    launch_part_volumes(*c, c->x, c->vol, s);
+    int rc = volume_gradient(*c, nullptr);  // into the adjoint's staging buffer
+    if (rc) return rc;
+    BEM_CUDA(*c, cudaMemcpyAsync(xbar, c->adj.iox, sizeof(double) * 3 * c->topo.N, cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    return BEM_OK;
+}
+
+int bem_set_state_device(bem_ctx* c, const double* x, const double* phi) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const int64_t N = c->topo.N;
+    cudaStream_t s = c->stream;
+    if (x) BEM_CUDA(*c, cudaMemcpyAsync(c->x, x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
+    if (phi) BEM_CUDA(*c, cudaMemcpyAsync(c->phi, phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    return BEM_OK;
+}
+
+int bem_get_state_device(bem_ctx* c, double* x, double* phi) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const int64_t N = c->topo.N;
+    cudaStream_t s = c->stream;
+    if (x) BEM_CUDA(*c, cudaMemcpyAsync(x, c->x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
+    if (phi) BEM_CUDA(*c, cudaMemcpyAsync(phi, c->phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
     return BEM_OK;
 }
 

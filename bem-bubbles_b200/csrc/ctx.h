@@ -10,6 +10,21 @@
 
 namespace bemb {
 
+// Work of the adjoint (adjoint.cu): per-step checkpoints, per-stage records of the recomputed
+// step, adjoint vectors and the partial sums of the assembly derivative.
+struct AdjWork {
+    int64_t N = 0;
+    int cap = 0, steps = 0, rch = 1, tch = 1;
+    double dt = 0.0, bb = 0.0;
+    double *ckx = nullptr, *ckp = nullptr, *ckt = nullptr;                  // checkpoints
+    double *xs = nullptr, *ps = nullptr, *ks = nullptr, *kps = nullptr;     // 4 stages
+    double *psis = nullptr, *Gs = nullptr, *Hs = nullptr;                   // 4 stages
+    double *kb = nullptr, *kpb = nullptr, *xb = nullptr, *pb = nullptr;     // adjoints
+    double *xsb = nullptr, *psb = nullptr, *vb = nullptr, *wv = nullptr, *psib = nullptr, *mu = nullptr, *r = nullptr;
+    double *tb = nullptr, *tp = nullptr, *rec = nullptr, *partA = nullptr, *partB = nullptr, *S = nullptr;
+    double *red = nullptr, *tsave = nullptr, *iox = nullptr, *iop = nullptr;
+};
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -108,6 +123,8 @@ struct Ctx {
     cudaGraphExec_t graph_exec = nullptr;
     double graph_dt = 0.0;
     long long graph_launches = 0;
+
+    AdjWork adj;
 
     // statistics
     bem_stats stats{};

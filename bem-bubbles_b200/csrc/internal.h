@@ -88,6 +88,10 @@ struct BlockInfo {
 struct Ctx;
 
 // assemble.cu
+struct QuadTables {
+    double qc[7][3], quv[7][2], w[7], gc[7], gs[7], gw[7], orb[5];
+};
+void quad_tables(QuadTables& t);
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s);
 void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b,
                      cudaStream_t s);
@@ -133,6 +137,18 @@ void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+
+int mixed_refresh(Ctx& c, const double* A, cudaStream_t s, bool from_scratch);
+
+// ctx.cu (shared with the adjoint)
+int solve_dev(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+int rk4_step_dev(Ctx& c, double dt, cudaStream_t s);
+int ensure_mixed(Ctx& c);
+
+// adjoint.cu
+int adjoint_record(Ctx& c, double dt, int steps);
+int adjoint_backward(Ctx& c, double* xbar, double* pbar);
+int volume_gradient(Ctx& c, double* xbar);
 
 // batch.cu
 int batch_mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);

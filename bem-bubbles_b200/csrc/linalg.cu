@@ -776,6 +776,10 @@ static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_sc
     return BEM_OK;
 }
 
+int mixed_refresh(Ctx& c, const double* A, cudaStream_t s, bool from_scratch) {
+    return refresh_inverse(c, A, s, from_scratch);
+}
+
 // h[k] partials of V_k . w for k <= j (one partial per block per k)
 __global__ void k_multidot(int n, int nv, const double* __restrict__ V, const double* __restrict__ w,
                            double* __restrict__ part) {

@@ -6,7 +6,7 @@ phi=0, p_inf=1, epsilon=1, gamma=1.4, sigma=0, far-field pressure -0.8*sin(2*pi*
 fixed step, no wall image.  A "step" is one RK4 step (4 stages of assembly + solve + update).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--solver mixed|bicgstab|lu]
-                  [--workload headline|pair|sweep]
+                  [--workload headline|pair|sweep|adjoint]
 
 --workload pair runs the large two-bubble pair instead (two icospheres nu=40, N=32004 unknowns,
 radii 1.0 and 0.7, centres (2,0,0) and (4.2,0,0), phi = +0.4 and -0.14, epsilon=0, no field,
@@ -18,6 +18,11 @@ R0 log-uniform in [0.5, 2] centred at (R0 + 1, 0, 0), far field -A sin(2 pi t/T)
 T ~ U[2, 10] (seed 0), phi = 0, epsilon = 1, gamma = 1.4, dt = 2e-3, mixed precision: bubble-steps/s of
 the batch (one CUDA graph per RK4 step, tile shape from the autotuner) against the same bubbles
 stepped one after another through the single-bubble path.
+
+--workload adjoint: one bubble, icosphere nu=10 (N=1002) at (2,0,0), phi = -R Rdot = 0.3, epsilon=1,
+gamma=1.4, p_inf=1, no field; objective the enclosed volume after 50 RK4 steps at dt=2e-3; gradient
+with respect to the initial positions and potential through the torch.autograd.Function over the
+adjoint, against central differences (h=1e-6) of the FP64 BiCGSTAB GPU path on 32 seeded directions.
 
 ours: the mixed-precision path (FP64 assembly, FP64 GMRES, FP32 approximate-inverse preconditioner)
 through libbem_b200.so.  value = device time of K steps with the state resident in HBM (CUDA events
@@ -561,6 +566,87 @@ def run_sweep(args):
     return 0
 
 
+def run_adjoint(args):
+    """Adjoint gradient of the volume after 50 RK4 steps (N = 1002) against central differences."""
+    ws, rank, local = dist_env()
+    import torch
+
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+    from bem_b200 import mesh
+    from bem_b200.adjoint import rk4_flow, volume
+    from bem_b200.sim import ColocSim
+
+    dt, steps, ndir, h = 2e-3, 50, 32, 1e-6
+    phys = dict(p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.4)
+    v, f = mesh.bubble(10, 1.0, (2.0, 0.0, 0.0))
+    phi = np.full(len(v), 0.3)
+    N = len(v)
+    sim = ColocSim(v, f, solver="mixed", device=device, **phys)
+    dev = torch.device(f"cuda:{device}")
+    tr = torch.tensor(f, dtype=torch.int64, device=dev)
+    fw, bw = [], []
+    for rep in range(args.warmup + 1):  # warm-up repetitions, then the timed one
+        x0 = torch.tensor(v, dtype=torch.float64, device=dev, requires_grad=True)
+        p0 = torch.tensor(phi, dtype=torch.float64, device=dev, requires_grad=True)
+        sim.set_time(0.0)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        xK, pK = rk4_flow(sim, x0, p0, dt, steps)
+        J = volume(xK, tr)
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        J.backward()
+        torch.cuda.synchronize(dev)
+        t2 = time.perf_counter()
+        fw.append(t1 - t0)
+        bw.append(t2 - t1)
+    gx, gp = x0.grad.cpu().numpy(), p0.grad.cpu().numpy()
+    J0 = float(J.item())
+
+    fd_sim = ColocSim(v, f, solver="bicgstab", device=device, **phys)  # V0 = initial volume, held fixed
+
+    def Jfd(x, p):
+        fd_sim.set_vertices(x)
+        fd_sim.set_phi(p)
+        fd_sim.set_time(0.0)
+        fd_sim.evolve_rk4_steps(dt, steps)
+        xe = fd_sim.get_vertices()
+        a, b, c = xe[f[:, 0]], xe[f[:, 1]], xe[f[:, 2]]
+        return float(np.sum(np.cross(a, b) * c) / 6.0)
+
+    rng = np.random.default_rng(0)
+    errs, errs_n = [], []
+    tw = time.perf_counter()
+    for _ in range(ndir):
+        dx, dp = rng.standard_normal((N, 3)), rng.standard_normal(N)
+        fd = (Jfd(v + h * dx, phi + h * dp) - Jfd(v - h * dx, phi - h * dp)) / (2 * h)
+        ad = float(np.sum(gx * dx) + np.dot(gp, dp))
+        errs.append(abs(ad - fd) / abs(fd))
+        errs_n.append(abs(ad - fd) / (np.sqrt(np.sum(gx ** 2) + np.sum(gp ** 2)) *
+                                      np.sqrt(np.sum(dx ** 2) + np.sum(dp ** 2))))
+    fd_s = time.perf_counter() - tw
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "adjoint gradient of the volume after 50 RK4 steps (N=1002): max relative error vs central FD",
+        "value": max(errs), "unit": "relative error", "n_gpus": ws, "steps": steps, "warmup": args.warmup,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (adjoint, assembly derivative, residuals) + f32 (preconditioner)", "data": "synthetic",
+        "config": {"workload": "one bubble nu=10 (N=1002, M=2000) at (2,0,0), phi=0.3, epsilon=1, gamma=1.4, "
+                               "p_inf=1, RK4 dt=2e-3 x 50, objective V(x_50)",
+                   "directions": ndir, "fd_step": h, "fd_solver": "FP64 BiCGSTAB GPU path"},
+        "target": 1e-5,
+        "rel_err": {"max": max(errs), "median": float(np.median(errs)),
+                    "max_normalised_by_norms": max(errs_n)},
+        "objective": J0,
+        "grad_norm": {"x": float(np.sqrt(np.sum(gx ** 2))), "phi": float(np.sqrt(np.sum(gp ** 2)))},
+        "time_s": {"forward_with_checkpoints": fw[-1], "backward": bw[-1], "fd_64_forward_runs": fd_s},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -569,7 +655,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solver", default="mixed", choices=["mixed", "bicgstab", "lu"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="headline", choices=["headline", "pair", "sweep"])
+    ap.add_argument("--workload", default="headline", choices=["headline", "pair", "sweep", "adjoint"])
     ap.add_argument("--no-seq", action="store_true", help="sweep: skip the sequential baseline")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -580,6 +666,8 @@ def main():
         return run_pair(args)
     if args.workload == "sweep":
         return run_sweep(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

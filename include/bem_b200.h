@@ -152,6 +152,30 @@ int bem_evolve_rk4_graph(bem_ctx* ctx, double dt, int32_t steps);
  * times (either may be NULL).  The state is kept; approximate inverses are rebuilt on the next step. */
 int bem_autotune_assembly(bem_ctx* ctx, int32_t* best_cg, double* ms);
 
+/* ---- Adjoint of fixed-dt RK4 trajectories.  No counterpart in the reference: reverse-mode
+ * derivative of LinLinSim::evolve_system_RK4 (LinLinSim.cpp:194-257) as computed here, for
+ * free-space bubbles (no wall image), sigma = 0 and the device-evaluated field; V_0 and the other
+ * parameters are held fixed.  The transposed solves refine against the FP64 G through the mixed
+ * solver's approximate inverse, which is built when the context uses another solver.
+ * bem_adjoint_record runs `steps` RK4 steps from the current state (advancing it) and keeps one
+ * checkpoint per step; it fails with BEM_ERR_STATE if a vertex comes within the wall treatment's
+ * range (x < nopen_eps), which is not differentiated.  bem_adjoint_backward takes the adjoint of
+ * the final state (d objective / d x_K as N x 3, d objective / d phi_K as N) and returns that of
+ * the recorded initial state, recomputing each step's stages from its checkpoint. */
+int bem_adjoint_record(bem_ctx* ctx, double dt, int32_t steps);
+int bem_adjoint_backward(bem_ctx* ctx, const double* xbar_end, const double* phibar_end, double* xbar0,
+                         double* phibar0);
+/* The same with device arrays on the context's device, overwritten in place; returns after the
+ * context's stream has finished. */
+int bem_adjoint_backward_device(bem_ctx* ctx, double* xbar, double* phibar);
+/* d(total enclosed volume)/d(vertex positions) at the current state, N x 3 host array
+ * (Mesh.cpp:206-218 differentiated). */
+int bem_volume_gradient(bem_ctx* ctx, double* xbar);
+/* State from / to device arrays (N x 3 positions, N potentials) on the context's device; either
+ * pointer may be NULL. */
+int bem_set_state_device(bem_ctx* ctx, const double* x, const double* phi);
+int bem_get_state_device(bem_ctx* ctx, double* x, double* phi);
+
 /* Solver statistics of the most recent solve. */
 typedef struct {
     int64_t solves;           /* solves since creation */
