@@ -132,30 +132,37 @@ __global__ void k_triangle_records(int M, const double* __restrict__ x, const in
 __device__ __forceinline__ double rsqrt_fp64(double r2) {
     double y0;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(r2));
-    const double t = r2 * y0;
+    const double t = __dmul_rn(r2, y0);
     const double d = fma(-t, y0, 1.0);
     const double p = fma(0.375, d, 0.5);
-    return fma(y0, d * p, y0);
+    return fma(y0, __dmul_rn(d, p), y0);
 }
 
 // Orbit-form basis sums of the 7 kernel values k[0..6] (see c_orb): out_k = C + dA*kA_k + dB*kB_k.
 __device__ __forceinline__ void orbit_sums(const double* k, double& o0, double& o1, double& o2) {
     const double SA = (k[1] + k[2]) + k[3], SB = (k[4] + k[5]) + k[6];
-    const double C = fma(c_orb[0], k[0], fma(c_orb[1], SA, c_orb[3] * SB));
+    const double C = fma(c_orb[0], k[0], fma(c_orb[1], SA, __dmul_rn(c_orb[3], SB)));
     o0 = fma(c_orb[2], k[3], fma(c_orb[4], k[6], C));
     o1 = fma(c_orb[2], k[1], fma(c_orb[4], k[4], C));
     o2 = fma(c_orb[2], k[2], fma(c_orb[4], k[5], C));
 }
 
-// Regular 7-point rule of one (row, triangle) pair; returns area-scaled G and H basis integrals.
-// All quadrature points lie in the triangle's plane, so (y_q - x).n = n.a - n.x is hoisted out of
-// the quadrature loop (and likewise for the image triangle).
+// Basis sums of one regular pair.  G_k = g_k * area; H_k = h_k * sh (+ m_k * sm with the wall image).
+// The accumulation into the shared-memory sums is written with explicit fused multiply-adds, so every
+// kernel that inlines this code produces the same bits (no contraction left to the compiler).
+struct PairSums {
+    double g[3], h[3], m[3];
+    double area, sh, sm;
+};
+
+// Regular 7-point rule of one (row, triangle) pair.  All quadrature points lie in the triangle's
+// plane, so (y_q - x).n = n.a - n.x is hoisted out of the quadrature loop (and likewise for the image
+// triangle).
 template <bool MIRROR>
 __device__ __forceinline__ void regular_pair(const double* __restrict__ r, double xi0, double xi1, double xi2,
-                                             double& g0, double& g1, double& g2, double& h0, double& h1,
-                                             double& h2) {
+                                             PairSums& p) {
     const double nx = r[21], ny = r[22], nz = r[23], area = r[24], dt = r[25];
-    const double xn_yz = xi1 * ny + xi2 * nz;
+    const double xn_yz = fma(xi1, ny, __dmul_rn(xi2, nz));
     const double dn = dt - fma(xi0, nx, xn_yz);  // (y - x).n
     double kg[7], kh[7], km[7];
 #pragma unroll
@@ -163,37 +170,36 @@ __device__ __forceinline__ void regular_pair(const double* __restrict__ r, doubl
         const double yx = r[3 * q];
         const double zy = r[3 * q + 1] - xi1, zz = r[3 * q + 2] - xi2;
         const double zx = yx - xi0;
-        const double yz2 = fma(zy, zy, zz * zz);
+        const double yz2 = fma(zy, zy, __dmul_rn(zz, zz));
         const double inv = rsqrt_fp64(fma(zx, zx, yz2));
         kg[q] = inv;
-        kh[q] = inv * inv * inv;
+        kh[q] = __dmul_rn(__dmul_rn(inv, inv), inv);
         if (MIRROR) {
             // image point (-y.x, y.y, y.z), image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
             const double mx = -yx - xi0;
             const double inv2 = rsqrt_fp64(fma(mx, mx, yz2));
             kg[q] += inv2;
-            km[q] = inv2 * inv2 * inv2;
+            km[q] = __dmul_rn(__dmul_rn(inv2, inv2), inv2);
         }
     }
-    double a0, a1, a2, b0, b1, b2;
-    orbit_sums(kg, a0, a1, a2);
-    orbit_sums(kh, b0, b1, b2);
-    g0 = a0 * area;
-    g1 = a1 * area;
-    g2 = a2 * area;
-    const double sh = -dn * area;
-    h0 = b0 * sh;
-    h1 = b1 * sh;
-    h2 = b2 * sh;
+    orbit_sums(kg, p.g[0], p.g[1], p.g[2]);
+    orbit_sums(kh, p.h[0], p.h[1], p.h[2]);
+    p.area = area;
+    p.sh = -__dmul_rn(dn, area);
     if (MIRROR) {
-        double m0, m1, m2;
-        orbit_sums(km, m0, m1, m2);
+        orbit_sums(km, p.m[0], p.m[1], p.m[2]);
         // (y' - x).n' = n.a - (-x.x n.x + x.y n.y + x.z n.z)
-        const double sm = -(dt - fma(-xi0, nx, xn_yz)) * area;
-        h0 = fma(m0, sm, h0);
-        h1 = fma(m1, sm, h1);
-        h2 = fma(m2, sm, h2);
+        p.sm = -__dmul_rn(dt - fma(-xi0, nx, xn_yz), area);
+    } else {
+        p.m[0] = p.m[1] = p.m[2] = 0.0;
+        p.sm = 0.0;
     }
+}
+
+template <bool MIRROR>
+__device__ __forceinline__ double add_h(const PairSums& p, int k, double acc) {
+    if (!MIRROR) return fma(p.h[k], p.sh, acc);
+    return __dadd_rn(acc, fma(p.m[k], p.sm, __dmul_rn(p.h[k], p.sh)));
 }
 
 // Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  Adds G and H of the pair
@@ -330,21 +336,21 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
                     singular_pair<MIRROR>(x, info.y, info.z, info.w, shift, code, accG + tid, accH + tid, ROWS);
                     continue;
                 }
-                double g0, g1, g2, h0, h1, h2;
-                regular_pair<MIRROR>(srec + tt * REC, xi0, xi1, xi2, g0, g1, g2, h0, h1, h2);
+                PairSums p;
+                regular_pair<MIRROR>(srec + tt * REC, xi0, xi1, xi2, p);
                 const int s0 = code & SLOT_NONE, s1 = (code >> SLOT_BITS) & SLOT_NONE,
                           s2 = (code >> (2 * SLOT_BITS)) & SLOT_NONE;
                 if (s0 != SLOT_NONE) {
-                    accG[s0 * ROWS + tid] += g0;
-                    accH[s0 * ROWS + tid] += h0;
+                    accG[s0 * ROWS + tid] = fma(p.g[0], p.area, accG[s0 * ROWS + tid]);
+                    accH[s0 * ROWS + tid] = add_h<MIRROR>(p, 0, accH[s0 * ROWS + tid]);
                 }
                 if (s1 != SLOT_NONE) {
-                    accG[s1 * ROWS + tid] += g1;
-                    accH[s1 * ROWS + tid] += h1;
+                    accG[s1 * ROWS + tid] = fma(p.g[1], p.area, accG[s1 * ROWS + tid]);
+                    accH[s1 * ROWS + tid] = add_h<MIRROR>(p, 1, accH[s1 * ROWS + tid]);
                 }
                 if (s2 != SLOT_NONE) {
-                    accG[s2 * ROWS + tid] += g2;
-                    accH[s2 * ROWS + tid] += h2;
+                    accG[s2 * ROWS + tid] = fma(p.g[2], p.area, accG[s2 * ROWS + tid]);
+                    accH[s2 * ROWS + tid] = add_h<MIRROR>(p, 2, accH[s2 * ROWS + tid]);
                 }
             }
         }
@@ -409,37 +415,45 @@ __global__ void __launch_bounds__(ROWS, MINB)
     }
 }
 
-// 4 pi rule and right-hand side: H(i,i) -= 4 pi - val, val = -sum_j H(i,j); b = H*phi.
+// 4 pi rule and right-hand side of one row: H(i,i) -= 4 pi - val, val = -sum_j H(i,j); b = H*phi.
+// One warp per row: lane l sums the partials of groups l, l+32, ... and the warp adds the lane sums
+// in a fixed butterfly order (deterministic).  il: row within its block; partials at rowHp[g*n + il].
+__device__ __forceinline__ void diag_row(int il, int n, int ngroups, const double* __restrict__ rowHp,
+                                         const double* __restrict__ bp, double phii, double* Hii, double* bi) {
+    const int lane = threadIdx.x & 31;
+    double val = 0.0, bs = 0.0;
+    for (int g = lane; g < ngroups; g += 32) {
+        val -= rowHp[(size_t)g * n + il];
+        bs += bp[(size_t)g * n + il];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        val += __shfl_xor_sync(0xffffffffu, val, o);
+        bs += __shfl_xor_sync(0xffffffffu, bs, o);
+    }
+    if (lane) return;
+    const double d = -(4.0 * 3.14159265358979323846 - val);
+    *Hii += d;
+    if (bi) *bi = fma(d, phii, bs);
+}
+
 __global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
                            const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= N) return;
-    double val = 0.0, bs = 0.0;
-    for (int g = 0; g < ngroups; ++g) {
-        val -= rowHp[(size_t)g * N + i];
-        bs += bp[(size_t)g * N + i];
-    }
-    double d = -(4.0 * 3.14159265358979323846 - val);
-    H[(size_t)i * N + i] += d;
-    if (b) b[i] = fma(d, phi[i], bs);
+    diag_row(i, N, ngroups, rowHp, bp, phi[i], H + (size_t)i * N + i, b ? b + i : nullptr);
 }
 
 // The same rule per block of a batch (rows of block vblk[i], its own groups and G/H block).
 __global__ void k_diag_rhs_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
                                  const double* __restrict__ rowHp, const double* __restrict__ bp,
                                  const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= N) return;
     const BlockInfo B = blk[vblk[i]];
     const int il = i - B.vbase;
-    double val = 0.0, bs = 0.0;
-    for (int g = 0; g < B.ngroups; ++g) {
-        val -= rowHp[(size_t)B.pbase + (size_t)g * B.n + il];
-        bs += bp[(size_t)B.pbase + (size_t)g * B.n + il];
-    }
-    double d = -(4.0 * 3.14159265358979323846 - val);
-    H[(size_t)B.mbase + (size_t)il * B.n + il] += d;
-    if (b) b[i] = fma(d, phi[i], bs);
+    diag_row(il, B.n, B.ngroups, rowHp + B.pbase, bp + B.pbase, phi[i], H + (size_t)B.mbase + (size_t)il * B.n + il,
+             b ? b + i : nullptr);
 }
 
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
@@ -552,9 +566,9 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
         c.ev_asm.emplace_back(e0, e1);
     }
     if (c.batch)
-        KLAUNCH(), k_diag_rhs_batch<<<(N + 255) / 256, 256, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, phi, H, b);
+        KLAUNCH(), k_diag_rhs_batch<<<(N + 7) / 8, 256, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, phi, H, b);
     else
-        KLAUNCH(), k_diag_rhs<<<(N + 255) / 256, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
+        KLAUNCH(), k_diag_rhs<<<(N + 7) / 8, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
 }
 
 }  // namespace bemb

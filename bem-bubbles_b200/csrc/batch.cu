@@ -180,10 +180,17 @@ int batch_setup_solver(Ctx& c) {
     std::vector<int4> items;
     int rbase = 0;
     long long pofs = 0;
+    // column splits: at most BG_COLS columns per item, and for large blocks enough items to keep
+    // four CTAs per SM busy by themselves in proportion to their share of the matrix elements
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    double tot = 0.0;
+    for (auto& B : c.h_blk) tot += (double)B.n * B.n;
     for (auto& B : c.h_blk) {
         const int nrb = (B.n + BG_ROWS - 1) / BG_ROWS;
+        const int fill = (int)std::ceil(4.0 * sms * ((double)B.n * B.n / tot) / nrb);
         B.rbase = rbase;
-        B.ncs = std::max(1, std::min(64, (B.n + BG_COLS - 1) / BG_COLS));
+        B.ncs = std::max(1, std::min(std::min(64, std::max(1, B.n / 16)), std::max((B.n + BG_COLS - 1) / BG_COLS, fill)));
         B.pofs = pofs;
         rbase += nrb;
         pofs += (long long)B.ncs * B.n;

@@ -377,6 +377,9 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     t.cg = h.cg;
     t.nparts = h.nparts;
     t.h_part_of_vert = h.part_of_vert;
+    t.max_part_tris = 0;
+    for (int p = 0; p < h.nparts; ++p)
+        t.max_part_tris = std::max(t.max_part_tris, h.part_off[(size_t)p + 1] - h.part_off[(size_t)p]);
     int rc;
     if ((rc = upload(c, &t.tri, h.tri)) || (rc = upload(c, &t.csr_off, h.csr_off)) ||
         (rc = upload(c, &t.csr_idx, h.csr_idx)) || (rc = upload(c, &t.grp_off, h.grp_off)) ||
@@ -405,6 +408,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = dalloc(c, &c.rec, m * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) || (rc = dalloc(c, &c.tg, 3 * m)) ||
         (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, nrow_part)) ||
         (rc = dalloc(c, &c.bp, nrow_part)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
+        (rc = dalloc(c, &c.vol_part, (size_t)h.nparts * 64)) || (rc = dalloc(c, &c.vol_cnt, (size_t)h.nparts)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)))
@@ -413,6 +417,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         if ((rc = alloc_mixed(c))) return rc;
     }
     BEM_CUDA(c, cudaMemset(c.cnt, 0, sizeof(unsigned) * ((n + 255) / 256 + 1)));
+    BEM_CUDA(c, cudaMemset(c.vol_cnt, 0, sizeof(unsigned) * (size_t)h.nparts));
     BEM_CUDA(c, cudaMemset(c.phi, 0, sizeof(double) * n));
     BEM_CUDA(c, cudaMemset(c.psi, 0, sizeof(double) * n));
     BEM_CUDA(c, cudaMemset(c.psil, 0, sizeof(double) * n));

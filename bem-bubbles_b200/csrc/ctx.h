@@ -55,6 +55,8 @@ struct Ctx {
     double* rowHp = nullptr;   // ngroups*N partial row sums of H
     double* bp = nullptr;      // ngroups*N partial H*phi
     double* vol = nullptr;     // nparts volumes
+    double* vol_part = nullptr;  // nparts x 64 chunk sums of the volume reduction
+    unsigned* vol_cnt = nullptr; // nparts completion counters of the volume reduction
     double* kap = nullptr;     // N mean curvature (sigma != 0)
     double* tk = nullptr;      // M per-triangle mean curvature
     double* fieldv = nullptr;  // N per-vertex field values (callback mode)

@@ -54,6 +54,7 @@ struct Topology {
     int* grp_slot = nullptr;     // per grp_tri entry: 3 x SLOT_BITS owned-slot codes (SLOT_NONE = not owned)
     int* grp_vert = nullptr;     // ngroups*cg vertex of each slot, -1 padding
     int nparts = 0;              // loose parts (bubbles)
+    int max_part_tris = 0;       // triangles of the largest part
     int* part_of_vert = nullptr; // N
     int* part_off = nullptr;     // nparts+1 into part_tidx
     int* part_tidx = nullptr;    // triangle ids grouped by part, increasing inside a part

@@ -4,6 +4,8 @@
 // All O(N) or O(M); memory-bound and tiny next to assembly and solve.
 #include <math.h>
 
+#include <algorithm>
+
 #include "ctx.h"
 
 namespace bemb {
@@ -62,13 +64,24 @@ __global__ void k_velocity(int N, const int* __restrict__ off, const int* __rest
     st3(vel, i, {gx * s, gy * s, gz * s});
 }
 
-// Part volumes: one CTA per loose part, fixed-shape tree reduction (Mesh.cpp:206-218).
-__global__ void k_part_volume(const double* __restrict__ x, const int* __restrict__ off,
-                              const int* __restrict__ tidx, const int* __restrict__ ptri, double* __restrict__ vol) {
+// Part volumes (Mesh.cpp:206-218), sum over the part's triangles of (a x b).c / 6, in two levels
+// with a fixed shape: CTA (chunk, part) sums VOL_CHUNK consecutive triangles of the part's list by a
+// tree; the last CTA of the part (completion counter) adds the chunk sums in chunk order.
+constexpr int VOL_CHUNK = 1024, VOL_MAXCH = 64;
+__global__ void __launch_bounds__(256) k_part_volume(const double* __restrict__ x, const int* __restrict__ off,
+                                                     const int* __restrict__ tidx, const int* __restrict__ ptri,
+                                                     double* __restrict__ part_sums, unsigned* __restrict__ cnt,
+                                                     double* __restrict__ vol) {
     __shared__ double red[256];
-    const int p = blockIdx.x;
+    __shared__ unsigned s_ticket;
+    const int p = blockIdx.y, ch = blockIdx.x;
+    const int b0 = off[p], b1 = off[p + 1];
+    const int nch = min(VOL_MAXCH, max(1, (b1 - b0 + VOL_CHUNK - 1) / VOL_CHUNK));
+    const int per = (b1 - b0 + nch - 1) / nch;  // triangles per chunk of this part
+    if (ch >= nch) return;
+    const int e0 = b0 + ch * per, e1 = min(b1, e0 + per);
     double acc = 0.0;
-    for (int e = off[p] + threadIdx.x; e < off[p + 1]; e += 256) {
+    for (int e = e0 + threadIdx.x; e < e1; e += 256) {
         const int t = tidx[e];
         d3 a = ld3(x, ptri[3 * t]), b = ld3(x, ptri[3 * t + 1]), c = ld3(x, ptri[3 * t + 2]);
         acc += dot(cross(a, b), c) / 6.0;
@@ -79,7 +92,18 @@ __global__ void k_part_volume(const double* __restrict__ x, const int* __restric
         if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) vol[p] = red[0];
+    if (threadIdx.x == 0) {
+        part_sums[(size_t)p * VOL_MAXCH + ch] = red[0];
+        __threadfence();
+        s_ticket = atomicAdd(&cnt[p], 1u);
+    }
+    __syncthreads();
+    if (s_ticket != (unsigned)(nch - 1) || threadIdx.x != 0) return;
+    __threadfence();
+    double v = 0.0;
+    for (int k = 0; k < nch; ++k) v += __ldcg(part_sums + (size_t)p * VOL_MAXCH + k);
+    vol[p] = v;
+    cnt[p] = 0u;
 }
 
 // potential_t (Simulation.cpp:73-75) per vertex:
@@ -357,7 +381,11 @@ void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s) {
                                                   vel);
 }
 void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s) {
-    KLAUNCH(), k_part_volume<<<c.topo.nparts, 256, 0, s>>>(x, c.topo.part_off, c.topo.part_tidx, c.topo.tri_rot, vol);
+    // chunks per part: enough for the largest part (the kernel exits early in smaller parts)
+    const int nch = std::min(VOL_MAXCH, std::max(1, (c.topo.max_part_tris + VOL_CHUNK - 1) / VOL_CHUNK));
+    dim3 grid(nch, c.topo.nparts);
+    KLAUNCH(), k_part_volume<<<grid, 256, 0, s>>>(x, c.topo.part_off, c.topo.part_tidx, c.topo.tri_rot, c.vol_part,
+                                                 c.vol_cnt, vol);
 }
 void launch_vertex_normals(Ctx& c, const double* x, double* out, cudaStream_t s) {
     KLAUNCH(), k_vertex_normals<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, x, c.topo.tri, c.topo.csr_off,
