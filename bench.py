@@ -84,6 +84,22 @@ def sweep_workload(nb=256, seed=0):
     return meshes, nus, R0, -A, 2.0 * np.pi / T
 
 
+def max_over_ranks(x, dist, device=None):
+    """Largest value of x over all ranks (the timing rule for replicas); x itself without a group."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ws, steps, elapsed_ms):
+    """Whole-job throughput of ws replicas, each taking `steps` steps, timed as the slowest rank."""
+    return ws * steps / (elapsed_ms * 1e-3)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -248,11 +264,9 @@ def run_ours(args):
     prof = sim.profile()
     sim.set_profiling(False)
     if dist:
-        t = torch.tensor([elapsed_ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        elapsed_ms = max_over_ranks(elapsed_ms, dist, f"cuda:{device}")
         dist.barrier()
-    value = ws * args.steps / (elapsed_ms * 1e-3)
+    value = replica_value(ws, args.steps, elapsed_ms)
 
     # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region
     hx = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -275,9 +289,7 @@ def run_ours(args):
         hpsi[:] = sim.get_psi()
     e2e_s = time.perf_counter() - tw0
     if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{device}")
     e2e_value = ws * e2e_steps / e2e_s
     h2d = N * 3 * 8 + 2 * N * 8
     d2h = N * 3 * 8 + 2 * N * 8
