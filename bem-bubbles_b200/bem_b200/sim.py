@@ -190,6 +190,17 @@ class ColocSim:
         self._check(self._L.bem_pot_t_multi(self._h, _d(v) if v is not None else None, _d(g), float(t), _d(out)))
         return out
 
+    def exterior_potential(self, points, phi=None, psi=None):
+        """compute_exterior_pot (LinLinSim.cpp:440-477) at points (P x 3) off the surface; with psi None,
+        LinLinSim::exterior_pot: psi is solved first at the current positions."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        out = np.empty(len(pts))
+        ph = None if phi is None else np.ascontiguousarray(phi, dtype=np.float64)
+        ps = None if psi is None else np.ascontiguousarray(psi, dtype=np.float64)
+        self._check(self._L.bem_exterior_potential(self._h, len(pts), _d(pts), None if ph is None else _d(ph),
+                                                   None if ps is None else _d(ps), _d(out)))
+        return out
+
     def evolve_system_RK4(self, dp, fixdt=False):
         dt = np.zeros(1)
         self._check(self._L.bem_evolve_rk4(self._h, float(dp), int(bool(fixdt)), _d(dt)))

@@ -348,28 +348,38 @@ void LinLinSim::remesh(real L) {
     psi.assign(mesh.verts.size(), 0.0);
 }
 
-// compute_exterior_pot (LinLinSim.cpp:440-477): potential at points off the surface, 19-point rule
+// compute_exterior_pot (LinLinSim.cpp:440-477): potential at points off the surface, 19-point rule, on
+// the GPU (a context for the given mesh, released on return)
 PotVec compute_exterior_pot(CoordVec const& pos, Mesh M, PotVec phi, PotVec psi) {
     PotVec out(pos.size(), 0.0);
-#pragma omp parallel
-    {
-        Integrator inter;
-        inter.set_quadrature(quadrature_19);
-#pragma omp for
-        for (long i = 0; i < (long)pos.size(); ++i) {
-            real v = 0.0;
-            for (Triplet const& t : M.trigs) v += inter.get_exterior_potential(M.verts, t, phi, psi, pos[(size_t)i]);
-            out[(size_t)i] = v;
-        }
-    }
+    if (pos.empty()) return out;
+    int dev = 0;
+    if (const char* e = std::getenv("BEM_DEVICE")) dev = std::atoi(e);
+    bem_ctx* c = nullptr;
+    if (bem_create(&c, dev, nullptr) != BEM_OK) throw std::runtime_error("compute_exterior_pot: no CUDA device");
+    struct Release {
+        bem_ctx* c;
+        ~Release() { bem_destroy(c); }
+    } release{c};
+    std::vector<int64_t> t(3 * M.trigs.size());
+    for (size_t j = 0; j < M.trigs.size(); ++j)
+        for (size_t k = 0; k < 3; ++k) t[3 * j + k] = (int64_t)M.trigs[j][k];
+    std::vector<double> x = flat(M.verts), p = flat(pos);
+    int rc = bem_set_mesh(c, (int64_t)M.verts.size(), x.data(), (int64_t)M.trigs.size(), t.data());
+    if (rc == BEM_OK) rc = bem_exterior_potential(c, (int64_t)pos.size(), p.data(), phi.data(), psi.data(), out.data());
+    if (rc != BEM_OK) throw std::runtime_error(std::string("compute_exterior_pot: ") + bem_last_error(c));
     return out;
 }
 
+// LinLinSim::exterior_pot (LinLinSim.cpp:479-485): psi solved at the current state, then the exterior
+// potential, both on the GPU
 PotVec LinLinSim::exterior_pot(CoordVec const& positions) const {
-    Eigen::MatrixXd G, H;
-    assemble_matrices(G, H, mesh);
-    const Eigen::VectorXd psi_l = solve_system(G, H * make_copy(phi));
-    return compute_exterior_pot(positions, mesh, phi, make_copy(psi_l));
+    PotVec out(positions.size(), 0.0);
+    if (positions.empty()) return out;
+    push_state();
+    std::vector<double> p = flat(positions);
+    check(bem_exterior_potential(ctx_, (int64_t)positions.size(), p.data(), nullptr, nullptr, out.data()));
+    return out;
 }
 
 }  // namespace Bem

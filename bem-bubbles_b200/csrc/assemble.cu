@@ -73,6 +73,31 @@ void quad_tables(QuadTables& t) {
     const double aB = 1.0 - (Q[6][0] + Q[6][1]), bB = Q[6][1];  // point 6
     const double orb[5] = {w0 * (1.0 / 3.0), wA * bA, wA * (aA - bA), wB * bB, wB * (aB - bB)};
     for (int k = 0; k < 5; ++k) t.orb[k] = orb[k];
+    // quadrature_19 (quadrature.hpp:126-146), the rule of compute_exterior_pot (LinLinSim.cpp:455)
+    const double Q19[19][3] = {{0.33333333333333331, 0.33333333333333331, 9.71357962827961025e-2 * 0.5},
+                               {2.06349616025259287e-2, 0.48968251919873701, 3.13347002271398278e-2 * 0.5},
+                               {0.48968251919873701, 2.06349616025259287e-2, 3.13347002271398278e-2 * 0.5},
+                               {0.48968251919873701, 0.48968251919873701, 3.13347002271398278e-2 * 0.5},
+                               {0.12582081701412900, 0.43708959149293553, 7.78275410047754301e-2 * 0.5},
+                               {0.43708959149293553, 0.12582081701412900, 7.78275410047754301e-2 * 0.5},
+                               {0.43708959149293553, 0.43708959149293553, 7.78275410047754301e-2 * 0.5},
+                               {0.62359292876193562, 0.18820353561903219, 7.96477389272090969e-2 * 0.5},
+                               {0.18820353561903219, 0.62359292876193562, 7.96477389272090969e-2 * 0.5},
+                               {0.18820353561903219, 0.18820353561903219, 7.96477389272090969e-2 * 0.5},
+                               {0.91054097321109406, 4.47295133944529688e-2, 2.55776756586981006e-2 * 0.5},
+                               {4.47295133944529688e-2, 0.91054097321109406, 2.55776756586981006e-2 * 0.5},
+                               {4.47295133944529688e-2, 4.47295133944529688e-2, 2.55776756586981006e-2 * 0.5},
+                               {0.74119859878449801, 3.68384120547362581e-2, 4.32835393772893970e-2 * 0.5},
+                               {0.74119859878449801, 0.22196298916076573, 4.32835393772893970e-2 * 0.5},
+                               {3.68384120547362581e-2, 0.74119859878449801, 4.32835393772893970e-2 * 0.5},
+                               {3.68384120547362581e-2, 0.22196298916076573, 4.32835393772893970e-2 * 0.5},
+                               {0.22196298916076573, 0.74119859878449801, 4.32835393772893970e-2 * 0.5},
+                               {0.22196298916076573, 3.68384120547362581e-2, 4.32835393772893970e-2 * 0.5}};
+    for (int q = 0; q < 19; ++q) {
+        t.q19[q][0] = Q19[q][0] + Q19[q][1];
+        t.q19[q][1] = Q19[q][1];
+        t.q19[q][2] = Q19[q][2];
+    }
 }
 
 static void upload_constants() {

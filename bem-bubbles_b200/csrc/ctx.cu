@@ -837,6 +837,48 @@ int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
     return BEM_OK;
 }
 
+// ---------------------------------------------------------------- exterior potential
+int bem_exterior_potential(bem_ctx* c, int64_t P, const double* points, const double* phi, const double* psi,
+                           double* out) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (P < 1 || !points || !out) return c->fail(BEM_ERR_ARG, "bad exterior-potential arguments");
+    if (c->batch) return c->fail(BEM_ERR_STATE, "exterior potential: single systems only");
+    cudaStream_t s = c->stream;
+    const int64_t N = c->topo.N;
+    double *pts = nullptr, *res = nullptr;
+    if (cudaMalloc(&pts, sizeof(double) * 3 * (size_t)P) != cudaSuccess ||
+        cudaMalloc(&res, sizeof(double) * (size_t)P) != cudaSuccess) {
+        cudaFree(pts);
+        return c->fail(BEM_ERR_NOMEM, "exterior potential: point buffers");
+    }
+    int rc = BEM_OK;
+    const double* phid = c->phi;
+    const double* psid = c->ps;
+    cudaError_t e = cudaMemcpyAsync(pts, points, sizeof(double) * 3 * (size_t)P, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && phi) {
+        e = cudaMemcpyAsync(c->p1, phi, sizeof(double) * N, cudaMemcpyHostToDevice, s);
+        phid = c->p1;
+    }
+    if (e == cudaSuccess && psi) e = cudaMemcpyAsync(c->ps, psi, sizeof(double) * N, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) rc = c->fail(BEM_ERR_CUDA, std::string("exterior potential: ") + cudaGetErrorString(e));
+    if (rc == BEM_OK && !psi) {
+        // LinLinSim::exterior_pot (LinLinSim.cpp:479-485): psi_l = solve_system(G, H*phi) first
+        launch_assemble(*c, c->x, phid, c->G, c->H, c->b, s);
+        rc = solve(*c, c->G, c->b, c->psil, s);
+        psid = c->psil;
+    }
+    if (rc == BEM_OK) rc = exterior_potential(*c, P, pts, phid, psid, res, s);
+    if (rc == BEM_OK) {
+        e = cudaMemcpyAsync(out, res, sizeof(double) * (size_t)P, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = c->fail(BEM_ERR_CUDA, std::string("exterior potential: ") + cudaGetErrorString(e));
+    }
+    cudaFree(pts);
+    cudaFree(res);
+    return rc;
+}
+
 // ---------------------------------------------------------------- adjoint
 int bem_adjoint_record(bem_ctx* c, double dt, int32_t steps) {
     CTX_GUARD(c);

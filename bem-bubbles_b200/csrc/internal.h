@@ -91,6 +91,7 @@ struct Ctx;
 // assemble.cu
 struct QuadTables {
     double qc[7][3], quv[7][2], w[7], gc[7], gs[7], gw[7], orb[5];
+    double q19[19][3];  // 19-point rule as (u, v, w): y = a + u (b - a) + v (c - b)
 };
 void quad_tables(QuadTables& t);
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s);
@@ -145,6 +146,10 @@ int mixed_refresh(Ctx& c, const double* A, cudaStream_t s, bool from_scratch);
 int solve_dev(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int rk4_step_dev(Ctx& c, double dt, cudaStream_t s);
 int ensure_mixed(Ctx& c);
+
+// exterior.cu
+int exterior_potential(Ctx& c, int64_t P, const double* pts_dev, const double* phi, const double* psi,
+                       double* out_dev, cudaStream_t s);
 
 // adjoint.cu
 int adjoint_record(Ctx& c, double dt, int steps);

@@ -152,6 +152,14 @@ int bem_evolve_rk4_graph(bem_ctx* ctx, double dt, int32_t steps);
  * times (either may be NULL).  The state is kept; approximate inverses are rebuilt on the next step. */
 int bem_autotune_assembly(bem_ctx* ctx, int32_t* best_cg, double* ms);
 
+/* Potential at P points off the surface (points: P x 3), compute_exterior_pot (LinLinSim.cpp:440-477):
+ * sum over triangles of (-G psi + H phi)/(4 pi) with the 19-point rule, no wall image.  phi (N) NULL:
+ * the context's phi.  psi (N) NULL: LinLinSim::exterior_pot (LinLinSim.cpp:479-485), i.e. psi solved
+ * first from G psi = H phi with the context's solver at the current positions.  Points must lie off
+ * the surface, as in the reference. */
+int bem_exterior_potential(bem_ctx* ctx, int64_t P, const double* points, const double* phi, const double* psi,
+                           double* out);
+
 /* ---- Adjoint of fixed-dt RK4 trajectories.  No counterpart in the reference: reverse-mode
  * derivative of LinLinSim::evolve_system_RK4 (LinLinSim.cpp:194-257) as computed here, for
  * free-space bubbles (no wall image), sigma = 0 and the device-evaluated field; V_0 and the other

@@ -30,6 +30,28 @@ static const double QTRI[7][3] = {
     {0.47014206410511505, 0.05971587178976981, 0.13239415278850616 * 0.5},
     {0.47014206410511505, 0.47014206410511505, 0.13239415278850616 * 0.5}};
 /* 7-point Gauss-Legendre on (0,1) (quadrature.hpp:30-38, selected at Simulation.hpp:45) */
+/* quadrature_19 (quadrature.hpp:126-146), used by compute_exterior_pot (LinLinSim.cpp:455) */
+static const double QTRI19[19][3] = {
+    {0.33333333333333331, 0.33333333333333331, 9.71357962827961025e-2 * 0.5},
+    {2.06349616025259287e-2, 0.48968251919873701, 3.13347002271398278e-2 * 0.5},
+    {0.48968251919873701, 2.06349616025259287e-2, 3.13347002271398278e-2 * 0.5},
+    {0.48968251919873701, 0.48968251919873701, 3.13347002271398278e-2 * 0.5},
+    {0.12582081701412900, 0.43708959149293553, 7.78275410047754301e-2 * 0.5},
+    {0.43708959149293553, 0.12582081701412900, 7.78275410047754301e-2 * 0.5},
+    {0.43708959149293553, 0.43708959149293553, 7.78275410047754301e-2 * 0.5},
+    {0.62359292876193562, 0.18820353561903219, 7.96477389272090969e-2 * 0.5},
+    {0.18820353561903219, 0.62359292876193562, 7.96477389272090969e-2 * 0.5},
+    {0.18820353561903219, 0.18820353561903219, 7.96477389272090969e-2 * 0.5},
+    {0.91054097321109406, 4.47295133944529688e-2, 2.55776756586981006e-2 * 0.5},
+    {4.47295133944529688e-2, 0.91054097321109406, 2.55776756586981006e-2 * 0.5},
+    {4.47295133944529688e-2, 4.47295133944529688e-2, 2.55776756586981006e-2 * 0.5},
+    {0.74119859878449801, 3.68384120547362581e-2, 4.32835393772893970e-2 * 0.5},
+    {0.74119859878449801, 0.22196298916076573, 4.32835393772893970e-2 * 0.5},
+    {3.68384120547362581e-2, 0.74119859878449801, 4.32835393772893970e-2 * 0.5},
+    {3.68384120547362581e-2, 0.22196298916076573, 4.32835393772893970e-2 * 0.5},
+    {0.22196298916076573, 0.74119859878449801, 4.32835393772893970e-2 * 0.5},
+    {0.22196298916076573, 3.68384120547362581e-2, 4.32835393772893970e-2 * 0.5}};
+
 static const double GL7[7][2] = {
     {0.5 * (1.0 + 0.0000000000000000), 0.5 * 0.4179591836734694},
     {0.5 * (1.0 + 0.4058451513773972), 0.5 * 0.3818300505051189},
@@ -79,11 +101,11 @@ static inline void kern(v3 z, v3 n, double* g, double* h) {
 
 /* integrate_disjoint_coloc[_mir] (Integrator.hpp:471-513) with integrand_coloc[_mir]
  * (Integrator.hpp:197-229): 7-point rule on the 45-degree unit triangle, x (u,v) = (qx+qy, qy). */
-static void disjoint(v3 x, const interp_t* t, int mirror, double G[3], double H[3]) {
+static void disjoint_q(v3 x, const interp_t* t, int mirror, const double (*qt)[3], int nq, double G[3], double H[3]) {
     G[0] = G[1] = G[2] = 0.0;
     H[0] = H[1] = H[2] = 0.0;
-    for (int q = 0; q < 7; ++q) {
-        double y0 = QTRI[q][0] + QTRI[q][1], y1 = QTRI[q][1], w = QTRI[q][2];
+    for (int q = 0; q < nq; ++q) {
+        double y0 = qt[q][0] + qt[q][1], y1 = qt[q][1], w = qt[q][2];
         v3 y = interp_at(t, y0, y1);
         v3 n = t->n;
         double g, h;
@@ -105,6 +127,33 @@ static void disjoint(v3 x, const interp_t* t, int mirror, double G[3], double H[
     for (int k = 0; k < 3; ++k) {
         G[k] *= t->area;
         H[k] *= t->area;
+    }
+}
+
+static void disjoint(v3 x, const interp_t* t, int mirror, double G[3], double H[3]) {
+    disjoint_q(x, t, mirror, QTRI, 7, G, H);
+}
+
+/* compute_exterior_pot (LinLinSim.cpp:440-477) with Integrator::get_exterior_potential
+ * (Integrator.cpp:287-305): per evaluation point, the sum over triangles (in order) of
+ * (-G.psi + H.phi)/(4 pi) over the 19-point rule, no wall image. */
+void orc_exterior_pot(int64_t N, int64_t M, const double* x, const int64_t* tri, const double* phi,
+                      const double* psi, int64_t P, const double* pts, double* out) {
+    (void)N;
+    for (int64_t i = 0; i < P; ++i) {
+        v3 y = ld(pts, i);
+        double val = 0.0;
+        for (int64_t j = 0; j < M; ++j) {
+            const int64_t* t = tri + 3 * j;
+            interp_t it = mk_interp(ld(x, t[0]), ld(x, t[1]), ld(x, t[2]));
+            double G[3], H[3];
+            disjoint_q(y, &it, 0, QTRI19, 19, G, H);
+            double integral = -G[0] * psi[t[0]] - G[1] * psi[t[1]] - G[2] * psi[t[2]] + H[0] * phi[t[0]] +
+                              H[1] * phi[t[1]] + H[2] * phi[t[2]];
+            integral *= (1.0 / (4.0 * M_PI));
+            val += integral;
+        }
+        out[i] = val;
     }
 }
 

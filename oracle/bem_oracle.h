@@ -43,6 +43,11 @@ int orc_solve_bicgstab(int64_t N, const double* G, const double* b, double* x,
                        int64_t* iters, double* rel_err);
 /* generate_vertex_normals (Bem/Mesh/Mesh.cpp:141-163) */
 void orc_vertex_normals(int64_t N, int64_t M, const double* x, const int64_t* tri, double* out);
+
+/* compute_exterior_pot (LinLinSim.cpp:440-477): potential at P points off the surface from the surface
+ * phi and psi (N each); 19-point rule, no wall image. */
+void orc_exterior_pot(int64_t N, int64_t M, const double* x, const int64_t* tri, const double* phi,
+                      const double* psi, int64_t P, const double* pts, double* out);
 /* volume (Bem/Mesh/Mesh.cpp:206-218) */
 double orc_volume(int64_t N, int64_t M, const double* x, const int64_t* tri);
 /* LinLinSim::position_t (Bem/Simulation/LinLinSim.cpp:26-83); psi_l may be NULL */

@@ -6,6 +6,7 @@
 // between steps, RK4 and Euler steps, the LU solver (set_bcgstab(false)) so that both builds solve to
 // rounding.  Usage: dropin_check <in.ply> <out_prefix>; writes <out_prefix>-<k>.ply after each block.
 #include <cmath>
+#include <cstdio>
 #include <iostream>
 #include <string>
 
@@ -43,5 +44,9 @@ int main(int argc, char* argv[]) {
                   << sim.mesh.verts.size() << std::endl;
         sim.export_mesh(out + "-" + std::to_string(k) + ".ply");
     }
+    // the potential off the surface (LinLinSim::exterior_pot) at a few points around the bubble
+    const CoordVec probe = {vec3(3.0, 0.0, 0.0), vec3(5.0, 0.5, -0.2), vec3(3.2, 2.5, 0.4), vec3(1.0, -0.3, 1.0)};
+    const PotVec ext = sim.exterior_pot(probe);
+    for (size_t i = 0; i < ext.size(); ++i) std::printf("exterior %zu %.17g\n", i, ext[i]);
     return 0;
 }

@@ -57,6 +57,8 @@ def lib():
                                    C.POINTER(Params), _P]
         L.orc_euler_step.argtypes = [C.c_int64, C.c_int64, _P, _PI, _P, _P, C.c_double, C.c_int32,
                                      C.POINTER(Params), _P]
+        L.orc_exterior_pot.argtypes = [C.c_int64, C.c_int64, _P, _PI, _P, _P, C.c_int64, _P, _P]
+        L.orc_exterior_pot.restype = None
         _lib = L
     return _lib
 
@@ -109,6 +111,16 @@ def vertex_normals(verts, tris):
     v, t = _prep(verts, tris)
     out = np.empty_like(v)
     lib().orc_vertex_normals(len(v), len(t), _d(v), _i(t), _d(out))
+    return out
+
+
+def exterior_pot(verts, tris, phi, psi, points):
+    """compute_exterior_pot (LinLinSim.cpp:440-477) restated in C."""
+    v, t = _prep(verts, tris)
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    out = np.empty(len(pts))
+    lib().orc_exterior_pot(len(v), len(t), _d(v), _i(t), _d(np.ascontiguousarray(phi, dtype=np.float64)),
+                           _d(np.ascontiguousarray(psi, dtype=np.float64)), len(pts), _d(pts), _d(out))
     return out
 
 
@@ -170,8 +182,9 @@ def ref_available(mirror=False) -> bool:
     return os.path.exists(os.path.join(REF_DIR, "ref_harness_" + ("mirror" if mirror else "free")))
 
 
-def ref_run(action, verts, tris, phi, mirror=False, timing=False, **kw):
-    """Run the reference's own code (oracle/_ref/ref_harness_*) and return its float64 output."""
+def ref_run(action, verts, tris, phi, mirror=False, timing=False, points=None, psi=None, **kw):
+    """Run the reference's own code (oracle/_ref/ref_harness_*) and return its float64 output.
+    points (P x 3) and psi (N) are the extra inputs of the exterior actions."""
     v, t = _prep(verts, tris)
     exe = os.path.join(REF_DIR, "ref_harness_" + ("mirror" if mirror else "free"))
     with tempfile.TemporaryDirectory() as d:
@@ -181,6 +194,12 @@ def ref_run(action, verts, tris, phi, mirror=False, timing=False, **kw):
             v.tofile(fh)
             t.tofile(fh)
             np.ascontiguousarray(phi, dtype=np.float64).tofile(fh)
+            if points is not None:
+                pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+                np.array([len(pts)], dtype=np.int64).tofile(fh)
+                pts.tofile(fh)
+                if psi is not None:
+                    np.ascontiguousarray(psi, dtype=np.float64).tofile(fh)
         args = [exe, action, fin, fout] + [f"{k}={float(val)!r}" for k, val in kw.items()]
         if timing:
             args.append("timing=1")

@@ -15,6 +15,9 @@
 //     euler      -> same record layout as rk4, using evolve_system
 //     stages     -> `steps` repetitions of one RK4 stage (position_t + pot_t_multi); writes the
 //                   seconds of each repetition (timing sample for the CPU baseline)
+//     exterior   -> exterior_pot(points) (LinLinSim.cpp:479-485: assemble, solve, compute_exterior_pot)
+//     exterior_direct -> compute_exterior_pot(points, mesh, phi, psi) with the given psi
+//   in.bin for exterior*: then int64 P, P*3 float64 points, and for exterior_direct N float64 psi
 //   keys: p_inf epsilon sigma gamma V0 amp omega phase dt steps fixdt lu threads timing
 //   amp/omega/phase define the far-field pressure p(x,t) = amp*sin(omega*t + phase).
 #include <cstdint>
@@ -62,6 +65,17 @@ int main(int argc, char** argv) {
     if (std::fread(xyz.data(), 8, xyz.size(), f) != xyz.size()) die("short verts");
     if (std::fread(tri.data(), 8, tri.size(), f) != tri.size()) die("short trigs");
     if (std::fread(phi.data(), 8, phi.size(), f) != phi.size()) die("short phi");
+    std::vector<double> pts, psi_in;
+    if (action == "exterior" || action == "exterior_direct") {
+        int64_t P = 0;
+        if (std::fread(&P, 8, 1, f) != 1) die("no points");
+        pts.resize((size_t)P * 3);
+        if (std::fread(pts.data(), 8, pts.size(), f) != pts.size()) die("short points");
+        if (action == "exterior_direct") {
+            psi_in.resize((size_t)N);
+            if (std::fread(psi_in.data(), 8, psi_in.size(), f) != psi_in.size()) die("short psi");
+        }
+    }
     std::fclose(f);
 
     Mesh mesh;
@@ -138,6 +152,11 @@ int main(int argc, char** argv) {
             double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - a0).count();
             put(&sec, 1);
         }
+    } else if (action == "exterior" || action == "exterior_direct") {
+        CoordVec pos;
+        for (size_t i = 0; i < pts.size() / 3; ++i) pos.push_back(vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]));
+        PotVec r = action == "exterior" ? sim.exterior_pot(pos) : compute_exterior_pot(pos, sim.mesh, phi, psi_in);
+        put(r.data(), r.size());
     } else {
         die("unknown action");
     }

@@ -6,7 +6,8 @@ for the comparison with the same drivers linked against the drop-in library (tes
   ../python_utils/icosphere/ico-10.ply (the path the driver opens); arguments radius 3e-6 m, acoustic
   pressure 5e4 Pa.  The driver's first three exports (mesh-0..mesh-2) are copied.
 * dropin_check/: oracle/dropin_check.cpp (oracle/_ref/refdrv/dropin_check) on the icosphere nu = 7:
-  its three exports ref-0..ref-2.  This driver is reproducible bit for bit across thread counts.
+  its three exports ref-0..ref-2 and its exterior-potential probe (ref_exterior.txt).  This driver is
+  reproducible bit for bit across thread counts.
 
 Run from the repository root after `make -C oracle refdrivers`; takes a few minutes.
 """
@@ -54,8 +55,10 @@ def main():
         v, f = mesh.icosphere(7)
         write_ply(os.path.join(tmp, "ico-7.ply"), v, f)
         exe = os.path.join(ROOT, "oracle", "_ref", "refdrv", "dropin_check")
-        subprocess.run([exe, os.path.join(tmp, "ico-7.ply"), os.path.join(check_dir, "ref")], check=True,
-                       stdout=subprocess.DEVNULL)
+        r = subprocess.run([exe, os.path.join(tmp, "ico-7.ply"), os.path.join(check_dir, "ref")], check=True,
+                           capture_output=True, text=True)
+        with open(os.path.join(check_dir, "ref_exterior.txt"), "w") as fh:
+            fh.writelines(ln + "\n" for ln in r.stdout.splitlines() if ln.startswith("exterior "))
     print("wrote", check_dir)
 
 

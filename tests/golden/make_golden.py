@@ -74,6 +74,15 @@ def main(ref_root="/root/reference"):
                                      **field).reshape(2, -1)
     out["two_euler"] = O.ref_run("euler", v, f, phi, steps=2, dt=1e-2, V0=V0, lu=1, **field).reshape(2, -1)
 
+    # exterior potential at points off the surface (outside both bubbles, between them, inside one):
+    # compute_exterior_pot with a given psi, and exterior_pot (assemble, LU solve, then the same)
+    pts = np.array([[0.5, 0.3, 0.1], [2.5, 1.8, 0.0], [3.5, 0.0, 0.2], [6.0, -1.0, 2.0], [2.5, 0.0, 0.0],
+                    [4.5, 0.2, -0.1], [3.6, 0.5, 0.4]])
+    psi_x = 0.2 * np.cos(v[:, 2]) - 0.1 * v[:, 1]
+    out["ext_points"], out["ext_psi"] = pts, psi_x
+    out["ext_direct"] = O.ref_run("exterior_direct", v, f, phi, points=pts, psi=psi_x)
+    out["ext_solve"] = O.ref_run("exterior", v, f, phi, points=pts, lu=1)
+
     # 3) wall: bubble touching the x=eps line, image kernel on, collapsing -> nopenetration
     vw, fw = mesh.bubble(2, 1.0, (1.004, 0.0, 0.0))
     out["wall_verts"], out["wall_trigs"] = vw, fw

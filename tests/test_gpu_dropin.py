@@ -12,7 +12,8 @@
 * oracle/dropin_check.cpp, a well-posed driver of the same interface (bubble away from the wall
   image, host field callback, remeshing, RK4 and Euler, LU), built against both the reference classes
   and the drop-in: every export agrees in topology, and in positions, phi and psi to the float32
-  precision of the export (tests/golden/dropin_check, reproducible bit for bit by the reference).
+  precision of the export, and the exterior potential at probe points to 1e-8 (after three blocks of
+  steps; tests/golden/dropin_check, reproducible bit for bit by the reference).
 """
 import os
 import subprocess
@@ -95,3 +96,8 @@ def test_dropin_classes_match_reference_classes(tmp_path):
         assert np.max(np.abs(x - xr)) <= 1e-6, k
         for q in ("phi", "psi"):
             assert np.max(np.abs(e[q] - er[q])) <= 1e-6 * max(np.max(np.abs(er[q])), 1e-30), (k, q)
+    # LinLinSim::exterior_pot at the probe points after the last block (full double precision)
+    got = [float(ln.split()[2]) for ln in p.stdout.splitlines() if ln.startswith("exterior ")]
+    ref = [float(ln.split()[2]) for ln in open(os.path.join(gold, "ref_exterior.txt"))]
+    assert len(got) == len(ref) == 4
+    assert np.max(np.abs(np.array(got) - ref)) <= 1e-8 * np.max(np.abs(ref))

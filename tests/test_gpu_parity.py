@@ -214,3 +214,28 @@ def test_mixed_precision_error_headline_size():
     mix = ColocSim(v, f, solver="mixed")
     _, psi_mix = mix.position_t(phi, return_psi=True)
     assert rel(psi_mix, psi_ref) <= 1e-8
+
+
+def test_exterior_potential_matches_reference():
+    # compute_exterior_pot with a given psi, and exterior_pot (LU solve first) against the reference
+    v, f, phi = GOLD["two_verts"], GOLD["two_trigs"], GOLD["two_phi"]
+    sim = ColocSim(v, f, solver="lu")
+    sim.set_phi(phi)
+    pts, psi = GOLD["ext_points"], GOLD["ext_psi"]
+    assert rel(sim.exterior_potential(pts, phi=phi, psi=psi), GOLD["ext_direct"]) <= 1e-12
+    assert rel(sim.exterior_potential(pts), GOLD["ext_solve"]) <= TOL
+
+
+def test_exterior_potential_grid_matches_oracle():
+    # nu = 10 bubble, 300 seeded points on shells around it (outside and inside)
+    v, f = mesh.bubble(10, 1.0, (2.0, 0.0, 0.0))
+    rng = np.random.default_rng(11)
+    phi = 0.1 * np.sin(2 * v[:, 1]) + 0.02 * v[:, 0]
+    psi = 0.05 * np.cos(v[:, 2])
+    d = rng.standard_normal((300, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    r = np.where(np.arange(300) % 3 == 0, 0.5, rng.uniform(1.2, 4.0, 300))
+    pts = np.array([2.0, 0.0, 0.0]) + d * r[:, None]
+    sim = ColocSim(v, f)
+    got = sim.exterior_potential(pts, phi=phi, psi=psi)
+    assert rel(got, O.exterior_pot(v, f, phi, psi, pts)) <= 1e-12

@@ -137,3 +137,15 @@ def test_negative_x_raises_like_reference():
     S = O.State(v, f, np.zeros(len(v)))
     with pytest.raises(IndexError):
         S.rk4(1e-3, O.make_params(V0=1.0))
+
+
+def test_exterior_potential_bit_exact():
+    # compute_exterior_pot (LinLinSim.cpp:440-477) with a given psi, and exterior_pot (assemble,
+    # LU solve, compute_exterior_pot) restated with the oracle's own assembly and LU
+    v, f = GOLD["two_verts"], GOLD["two_trigs"]
+    phi = GOLD["two_phi"]
+    pts, psi = GOLD["ext_points"], GOLD["ext_psi"]
+    assert np.array_equal(O.exterior_pot(v, f, phi, psi, pts), GOLD["ext_direct"])
+    G, H = O.assemble(v, f)
+    psi_l, _ = O.solve(G, O.gemv(H, phi), use_lu=True)
+    assert np.array_equal(O.exterior_pot(v, f, phi, psi_l, pts), GOLD["ext_solve"])
