@@ -94,6 +94,8 @@ SIGNATURES = {
     "bem_get_block_stats": (C.c_int, [C.c_void_p, _D, _D, C.POINTER(C.c_int32)]),
     "bem_evolve_rk4_graph": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "bem_autotune_assembly": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), _D]),
+    "bem_export_ply_async": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "bem_export_wait": (C.c_int, [C.c_void_p]),
     "bem_exterior_potential": (C.c_int, [C.c_void_p, C.c_int64, _D, _D, _D, _D]),
     "bem_adjoint_record": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "bem_adjoint_backward": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),

@@ -190,6 +190,13 @@ class ColocSim:
         self._check(self._L.bem_pot_t_multi(self._h, _d(v) if v is not None else None, _d(g), float(t), _d(out)))
         return out
 
+    def export_ply_async(self, path):
+        """Simulation::export_mesh of the current state, written in the background (see export_wait)."""
+        self._check(self._L.bem_export_ply_async(self._h, str(path).encode()))
+
+    def export_wait(self):
+        self._check(self._L.bem_export_wait(self._h))
+
     def exterior_potential(self, points, phi=None, psi=None):
         """compute_exterior_pot (LinLinSim.cpp:440-477) at points (P x 3) off the surface; with psi None,
         LinLinSim::exterior_pot: psi is solved first at the current positions."""

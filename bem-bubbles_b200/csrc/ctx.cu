@@ -22,6 +22,7 @@ std::atomic<long long> g_kernel_launches{0};
 
 // ---------------------------------------------------------------- device memory helpers
 static void free_all(Ctx& c) {
+    exporter_release(c);  // writes every queued file first
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     c.graph_exec = nullptr;
     for (void* p : c.allocs) cudaFree(p);
@@ -377,6 +378,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     t.cg = h.cg;
     t.nparts = h.nparts;
     t.h_part_of_vert = h.part_of_vert;
+    c.h_tri = h.tri;
     t.max_part_tris = 0;
     for (int p = 0; p < h.nparts; ++p)
         t.max_part_tris = std::max(t.max_part_tris, h.part_off[(size_t)p + 1] - h.part_off[(size_t)p]);
@@ -835,6 +837,19 @@ int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
     if (ms)
         for (int k = 0; k < 3; ++k) ms[k] = times[k];
     return BEM_OK;
+}
+
+// ---------------------------------------------------------------- asynchronous PLY export
+int bem_export_ply_async(bem_ctx* c, const char* path) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!path) return c->fail(BEM_ERR_ARG, "null path");
+    return export_ply_async(*c, path);
+}
+
+int bem_export_wait(bem_ctx* c) {
+    CTX_GUARD(c);
+    return export_wait(*c);
 }
 
 // ---------------------------------------------------------------- exterior potential

@@ -25,6 +25,8 @@ struct AdjWork {
     double *red = nullptr, *tsave = nullptr, *iox = nullptr, *iop = nullptr;
 };
 
+struct PlyExporter;  // export.cu
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -127,6 +129,8 @@ struct Ctx {
     long long graph_launches = 0;
 
     AdjWork adj;
+    PlyExporter* exporter = nullptr;  // asynchronous PLY writer (export.cu)
+    std::vector<int> h_tri;           // host copy of the triangles (M*3)
 
     // statistics
     bem_stats stats{};

@@ -147,6 +147,11 @@ int solve_dev(Ctx& c, const double* A, const double* b, double* x, cudaStream_t 
 int rk4_step_dev(Ctx& c, double dt, cudaStream_t s);
 int ensure_mixed(Ctx& c);
 
+// export.cu
+int export_ply_async(Ctx& c, const char* path);
+int export_wait(Ctx& c);
+void exporter_release(Ctx& c);
+
 // exterior.cu
 int exterior_potential(Ctx& c, int64_t P, const double* pts_dev, const double* phi, const double* psi,
                        double* out_dev, cudaStream_t s);

@@ -152,6 +152,14 @@ int bem_evolve_rk4_graph(bem_ctx* ctx, double dt, int32_t steps);
  * times (either may be NULL).  The state is kept; approximate inverses are rebuilt on the next step. */
 int bem_autotune_assembly(bem_ctx* ctx, int32_t* best_cg, double* ms);
 
+/* Simulation::export_mesh (Simulation.cpp:94-96, export_ply_float MeshIO.cpp:263-298) of the current
+ * state without waiting for the file: the state is packed to float32 on the device in stream order
+ * (later steps may follow at once), copied to pinned memory on a separate stream and written by a
+ * background thread.  Up to four files are in flight; a fifth call waits for the oldest.
+ * bem_export_wait returns when every queued file is written, with the first write error if any. */
+int bem_export_ply_async(bem_ctx* ctx, const char* path);
+int bem_export_wait(bem_ctx* ctx);
+
 /* Potential at P points off the surface (points: P x 3), compute_exterior_pot (LinLinSim.cpp:440-477):
  * sum over triangles of (-G psi + H phi)/(4 pi) with the 19-point rule, no wall image.  phi (N) NULL:
  * the context's phi.  psi (N) NULL: LinLinSim::exterior_pot (LinLinSim.cpp:479-485), i.e. psi solved
