@@ -79,9 +79,10 @@ class BubbleBatch(ColocSim):
         self._check(self._L.bem_evolve_rk4_graph(self._h, float(dt), int(steps)))
 
     def autotune(self):
-        """Time the assembly tile shapes on this batch and keep the fastest; returns (width, ms[3])."""
+        """Time the assembly tile shapes on this batch and keep the fastest; returns (width, ms) with ms the
+        times of the widths 32, 48, 64 and 16."""
         cg = C.c_int32(0)
-        ms = np.empty(3)
+        ms = np.empty(4)
         self._check(self._L.bem_autotune_assembly(self._h, C.byref(cg), _d(ms)))
         return int(cg.value), ms
 

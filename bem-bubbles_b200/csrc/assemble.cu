@@ -530,17 +530,20 @@ static void launch_batch_t(Ctx& c, const double* x, const double* phi, double* G
                                                 G, H, c.rowHp, c.bp);
 }
 
-// Tile shapes: 32 columns x 128 rows (12 warps/SM), 48 x 64 and 64 x 64 (fewer boundary triangles,
-// 6 warps/SM); all at 3 CTAs per SM within the 228 KB of shared memory.
+// Tile shapes: 16 columns x 256 rows (24 warps/SM, more boundary triangles), 32 x 128 (12 warps/SM),
+// 48 x 64 and 64 x 64 (fewer boundary triangles, 6 warps/SM); all at 3 CTAs per SM within the 228 KB
+// of shared memory.
 void prepare_assemble(Ctx& c) {
     if (!c.batch) return;
     c.asm_grid_cg = 0;
     if (c.prm.mirror) {
-        if (c.topo.cg == 64) prepare_batch_t<true, 64, 64, 3>(c);
+        if (c.topo.cg == 16) prepare_batch_t<true, 16, 256, 3>(c);
+        else if (c.topo.cg == 64) prepare_batch_t<true, 64, 64, 3>(c);
         else if (c.topo.cg == 48) prepare_batch_t<true, 48, 64, 3>(c);
         else prepare_batch_t<true, 32, 128, 3>(c);
     } else {
-        if (c.topo.cg == 64) prepare_batch_t<false, 64, 64, 3>(c);
+        if (c.topo.cg == 16) prepare_batch_t<false, 16, 256, 3>(c);
+        else if (c.topo.cg == 64) prepare_batch_t<false, 64, 64, 3>(c);
         else if (c.topo.cg == 48) prepare_batch_t<false, 48, 64, 3>(c);
         else prepare_batch_t<false, 32, 128, 3>(c);
     }
@@ -550,6 +553,9 @@ template <bool MIRROR>
 static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
     if (c.batch) {
         switch (c.topo.cg) {
+            case 16:
+                launch_batch_t<MIRROR, 16, 256, 3>(c, x, phi, G, H, s);
+                break;
             case 64:
                 launch_batch_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s);
                 break;
@@ -562,6 +568,9 @@ static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, 
         return;
     }
     switch (c.topo.cg) {
+        case 16:
+            launch_tiles_t<MIRROR, 16, 256, 3>(c, x, phi, G, H, s);
+            break;
         case 64:
             launch_tiles_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s);
             break;

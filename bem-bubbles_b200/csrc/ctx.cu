@@ -68,7 +68,7 @@ static void free_all(Ctx& c) {
 
 // ---------------------------------------------------------------- topology preprocessing
 struct HostTopo {
-    int cg = 32;
+    int cg = 16;  // column-group width of the assembly tiles (16 x 256 rows, measured fastest)
     std::vector<int> tri, csr_off, csr_idx, grp_off, grp_tri, grp_slot, grp_vert, part_of_vert, part_off,
         part_tidx, tri_rot;
     int ngroups = 0, nparts = 0;
@@ -528,10 +528,10 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     cudaStreamSynchronize(c->stream);
     free_all(*c);
     HostTopo h;
-    // column-group width: 32 (128 rows per CTA) unless BEM_ASM_CG selects 48 or 64 (64 rows per CTA)
+    // column-group width: 16 (256 rows per CTA) unless BEM_ASM_CG selects 32 (128 rows) or 48 / 64 (64 rows)
     if (const char* e = getenv("BEM_ASM_CG")) {
         int v = atoi(e);
-        if (v == 48 || v == 64 || v == 32) h.cg = v;
+        if (v == 16 || v == 48 || v == 64 || v == 32) h.cg = v;
     }
     int rc = build_topology(N, M, trigs, verts, h, c->err);
     if (rc) return rc;
@@ -579,11 +579,11 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
     free_all(*c);
     c->batch_cg = keep_cg;
     HostTopo h;
-    if (c->batch_cg == 32 || c->batch_cg == 48 || c->batch_cg == 64) {
+    if (c->batch_cg == 16 || c->batch_cg == 32 || c->batch_cg == 48 || c->batch_cg == 64) {
         h.cg = c->batch_cg;
     } else if (const char* e = getenv("BEM_ASM_CG")) {
         int v = atoi(e);
-        if (v == 48 || v == 64 || v == 32) h.cg = v;
+        if (v == 16 || v == 48 || v == 64 || v == 32) h.cg = v;
     }
     int rc = build_topology(N, M, trigs, verts, h, c->err, voff);
     if (rc) return rc;
@@ -593,7 +593,7 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
     C.h_blk.assign((size_t)nblocks, BlockInfo{});
     long long mb = 0, pb = 0;
     std::vector<int4> tiles;
-    const int rows = h.cg == 32 ? 128 : 64;
+    const int rows = h.cg == 16 ? 256 : (h.cg == 32 ? 128 : 64);  // tile rows of each shape
     for (int b = 0; b < nblocks; ++b) {
         BlockInfo& B = C.h_blk[(size_t)b];
         B.n = (int)(voff[(size_t)b + 1] - voff[(size_t)b]);
@@ -762,9 +762,9 @@ int bem_evolve_rk4_graph(bem_ctx* c, double dt, int32_t steps) {
 }
 
 // Assembly tile shape of a batch chosen by timing: the column-group widths 32 (x 128 rows), 48 and 64
-// (x 64 rows) are each planned and timed over three assemblies of the current state; the fastest
-// is kept (and remembered per device and batch shape for later contexts).  ms: the three average
-// times, or null.
+// (x 64 rows) and 16 (x 256 rows) are each planned and timed over three assemblies of the current
+// state; the fastest is kept (and remembered per device and batch shape for later contexts).  ms: the
+// four average times, or null.
 int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
     CTX_GUARD(c);
     NEED_MESH(c);
@@ -788,16 +788,16 @@ int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
     const std::vector<int64_t> tr = c->h_trigs, voff = c->h_voff;
     const int nb = c->nblk;
     int best = 0;
-    double times[3] = {-1.0, -1.0, -1.0};
+    double times[4] = {-1.0, -1.0, -1.0, -1.0};
     {
         std::lock_guard<std::mutex> lock(mu);
         auto it = cache.find(key);
         if (it != cache.end()) best = it->second;
     }
     if (!best) {
-        const int cand[3] = {32, 48, 64};
+        const int cand[4] = {32, 48, 64, 16};
         double bt = 1e300;
-        for (int k = 0; k < 3; ++k) {
+        for (int k = 0; k < 4; ++k) {
             c->batch_cg = cand[k];
             int rc = bem_set_mesh_blocks(c, N, x.data(), M, tr.data(), nb, voff.data());
             if (rc) return rc;
@@ -835,7 +835,7 @@ int bem_autotune_assembly(bem_ctx* c, int32_t* best_cg, double* ms) {
     BEM_CUDA(*c, cudaStreamSynchronize(s));
     if (best_cg) *best_cg = best;
     if (ms)
-        for (int k = 0; k < 3; ++k) ms[k] = times[k];
+        for (int k = 0; k < 4; ++k) ms[k] = times[k];
     return BEM_OK;
 }
 

@@ -48,7 +48,7 @@ struct Topology {
     int* csr_off = nullptr;      // N+1, vertex -> incident triangles (increasing index)
     int* csr_idx = nullptr;      // 3M
     int ngroups = 0;             // assembly column groups
-    int cg = 32;                 // vertices per column group
+    int cg = 16;                 // vertices per column group
     int* grp_off = nullptr;      // ngroups+1 into grp_tri
     int* grp_tri = nullptr;      // triangles incident to the group's vertices, increasing
     int* grp_slot = nullptr;     // per grp_tri entry: 3 x SLOT_BITS owned-slot codes (SLOT_NONE = not owned)

@@ -559,7 +559,8 @@ def run_sweep(args):
                            "solver": "mixed, one bubble at a time", "setup_s": seq_setup},
         "speedup_vs_sequential": (value / ws / seq_value) if seq_value else None,
         "autotune": {"chosen_column_group": cg, "ms_per_assembly": {"32x128": tune_ms[0], "48x64": tune_ms[1],
-                                                                     "64x64": tune_ms[2]}, "seconds": tune_s},
+                                                                     "64x64": tune_ms[2], "16x256": tune_ms[3]},
+                     "seconds": tune_s},
         "setup_s_first_step": setup_s,
         "during_timed_steps": {"ns_steps": int(st1.ns_steps - st0.ns_steps),
                                "refreshes": int(st1.precond_refresh - st0.precond_refresh),

@@ -147,9 +147,10 @@ int bem_get_block_stats(bem_ctx* ctx, double* rho, double* rel_residual, int32_t
  * run again from its start state.  bem_evolve_rk4_n on a batch takes the same steps without the graph. */
 int bem_evolve_rk4_graph(bem_ctx* ctx, double dt, int32_t steps);
 /* Assembly tile shape of a batch by measurement: column groups of 32 (x 128 rows), 48 and 64 (x 64
- * rows) are each planned and timed over three assemblies of the current state, and the fastest is
- * kept (remembered per device and batch shape).  *best_cg receives the width, ms[3] the average
- * times (either may be NULL).  The state is kept; approximate inverses are rebuilt on the next step. */
+ * rows) and 16 (x 256 rows) are each planned and timed over three assemblies of the current state, and
+ * the fastest is kept (remembered per device and batch shape).  *best_cg receives the width, ms[4] the
+ * average times in that order (either may be NULL).  The state is kept; approximate inverses are
+ * rebuilt on the next step. */
 int bem_autotune_assembly(bem_ctx* ctx, int32_t* best_cg, double* ms);
 
 /* Simulation::export_mesh (Simulation.cpp:94-96, export_ply_float MeshIO.cpp:263-298) of the current

@@ -54,7 +54,7 @@ def test_assembly_nu10_matches_oracle_and_is_reproducible():
     assert rel(G, Go) < 1e-13 and rel(H, Ho) < 1e-13
 
 
-@pytest.mark.parametrize("cg", ["32", "48", "64"])
+@pytest.mark.parametrize("cg", ["16", "32", "48", "64"])
 def test_assembly_tile_shapes_agree(cg, monkeypatch):
     # every column-group width of the tile kernel gives the same matrices (two bubbles, nu=7)
     monkeypatch.setenv("BEM_ASM_CG", cg)
