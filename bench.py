@@ -452,7 +452,7 @@ def run_sweep(args):
 
     dt = 2e-3
     phys = dict(p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.4)
-    meshes, nus, R0, amp, om = sweep_workload()
+    meshes, nus, R0, amp, om = sweep_workload(args.bubbles)
     nb = len(meshes)
     bb = BubbleBatch(meshes, device=device, **phys)
     bb.set_block_params(amp=amp, omega=om)
@@ -547,11 +547,11 @@ def run_sweep(args):
         return 0
     Ns = np.array([len(v) for v, _ in meshes])
     line = {
-        "metric": "bubble RK4 steps/s, 256-bubble radius x pressure sweep: batched (CUDA graph) vs sequential GPU",
+        "metric": f"bubble RK4 steps/s, {nb}-bubble radius x pressure sweep: batched (CUDA graph) vs sequential GPU",
         "value": value, "unit": "bubble-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (assembly, residual, state) + f32 (preconditioner)", "data": "synthetic",
-        "config": {"workload": "256 bubbles, nu~U{4..16}, R0 log-U[0.5,2], A~U[0.1,1.5], T~U[2,10], seed 0, "
+        "config": {"workload": f"{nb} bubbles, nu~U{{4..16}}, R0 log-U[0.5,2], A~U[0.1,1.5], T~U[2,10], seed 0, "
                                "phi=0, epsilon=1, gamma=1.4, RK4 dt=2e-3",
                    "total_unknowns": int(Ns.sum()), "solver": "batched mixed",
                    "l2": f"working set larger than L2 (G+H = {16 * float((Ns ** 2).sum()) / 1e9:.1f} GB per stage)"},
@@ -590,7 +590,7 @@ def run_adjoint(args):
     from bem_b200.adjoint import rk4_flow, volume
     from bem_b200.sim import ColocSim
 
-    dt, steps, ndir, h = 2e-3, 50, 32, 1e-6
+    dt, steps, ndir, h = 2e-3, 50, args.dirs, 1e-6
     phys = dict(p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.4)
     v, f = mesh.bubble(10, 1.0, (2.0, 0.0, 0.0))
     phi = np.full(len(v), 0.3)
@@ -670,6 +670,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--workload", default="headline", choices=["headline", "pair", "sweep", "adjoint"])
     ap.add_argument("--no-seq", action="store_true", help="sweep: skip the sequential baseline")
+    ap.add_argument("--bubbles", type=int, default=256, help="sweep: number of bubbles")
+    ap.add_argument("--dirs", type=int, default=32, help="adjoint: finite-difference directions")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
