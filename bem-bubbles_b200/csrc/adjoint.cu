@@ -490,7 +490,12 @@ static int adj_alloc(Ctx& c, int steps) {
         (rc = dalloc(c, &w.ckt, (size_t)cap)))
         return rc;
     if (w.N != (int64_t)N) {
-        const int rch = std::max(1, nbk((int64_t)N, 256)), tch = std::max(1, nbk((int64_t)M, 256));
+        // row chunks of the triangle pass and triangle chunks of the row pass: about four CTAs per SM
+        // in each pass, at least 16 rows / triangles per chunk
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+        const int rch = std::max(1, std::min(nbk(4 * sms, nbk((int64_t)M, 128)), std::max(1, (int)N / 16)));
+        const int tch = std::max(1, std::min(nbk(4 * sms, nbk((int64_t)N, 128)), std::max(1, (int)M / 16)));
         w.rch = rch;
         w.tch = tch;
         if ((rc = dalloc(c, &w.xs, 4 * 3 * N)) || (rc = dalloc(c, &w.ps, 4 * N)) || (rc = dalloc(c, &w.ks, 4 * 3 * N)) ||

@@ -120,7 +120,9 @@ def read_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region (every 20 ms;
+    the sampler is running before the region starts, and only samples taken inside it count -- or,
+    for a region shorter than one interval, the sample taken right before it)."""
 
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -129,23 +131,29 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.first = threading.Event()
+        self.begin = self.end = 0
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.first.wait(3.0)
         except OSError:
             self.proc = None
+        self.begin = len(self.lines)
         return self
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
 
     def __exit__(self, *a):
+        self.end = len(self.lines)
         if self.proc:
             self.proc.terminate()
             try:
@@ -153,10 +161,16 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
+    def window(self):
+        w = self.lines[self.begin:self.end]
+        if not w and self.begin > 0:
+            w = self.lines[self.begin - 1:self.begin]
+        return w
+
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.window():
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 6:
                 continue
