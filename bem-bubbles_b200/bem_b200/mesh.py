@@ -138,3 +138,35 @@ def signed_volume(verts, faces) -> float:
     """Sum of (a x b).c / 6 over triangles (Bem/Mesh/Mesh.cpp:206-218)."""
     a, b, c = verts[faces[:, 0]], verts[faces[:, 1]], verts[faces[:, 2]]
     return float(np.sum(np.einsum("ij,ij->i", np.cross(a, b), c)) / 6.0)
+
+
+def wall_cap(nu: int, radius: float = 1.0):
+    """Hemisphere of ``radius`` sitting on the wall x = 0 (centre at the origin, x >= 0): the four
+    octants of a geodesic octahedron sphere with x > 0, each face cut into nu^2 triangles, the
+    vertices normalised to the sphere.  The boundary loop (4*nu vertices) lies exactly on x = 0, the
+    contact line of a pinned bubble (the reference's ColocSimPin meshes).  Outward orientation."""
+    if nu < 1:
+        raise ValueError("nu >= 1")
+    X, Y, Z = np.eye(3)
+    corners = {"x": X, "y": Y, "z": Z, "-y": -Y, "-z": -Z}
+    faces = [("x", "y", "z"), ("x", "z", "-y"), ("x", "-y", "-z"), ("x", "-z", "y")]
+    index, pts, tris = {}, [], []
+
+    def vid(key_weights):
+        key = tuple(sorted((c, w) for c, w in key_weights if w))
+        if key not in index:
+            p = sum(w * corners[c] for c, w in key) / nu
+            index[key] = len(pts)
+            pts.append(p)
+        return index[key]
+
+    for a, b, c in faces:
+        lat = {(i, j): vid(((a, nu - i), (b, i - j), (c, j))) for i in range(nu + 1) for j in range(i + 1)}
+        for i in range(nu):
+            for j in range(i + 1):
+                tris.append((lat[(i, j)], lat[(i + 1, j)], lat[(i + 1, j + 1)]))
+                if j < i:
+                    tris.append((lat[(i, j)], lat[(i + 1, j + 1)], lat[(i, j + 1)]))
+    v = np.array(pts, dtype=np.float64)
+    v = v / np.sqrt((v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1]) + v[:, 2] * v[:, 2])[:, None] * float(radius)
+    return v, np.array(tris, dtype=np.int64)

@@ -9,6 +9,7 @@ every call crosses the C ABI with host arrays.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -240,6 +241,85 @@ class ColocSim:
         p = L.Profile()
         self._check(self._L.bem_get_profile(self._h, C.byref(p)))
         return p
+
+
+WALL_THRESHOLD = 1e-5  # |x| below which a vertex is on the wall (ColocSimPin.cpp:230, 264)
+# the reference's contact-angle drift law (ColocSimPin.cpp:126-136): beta, cos(theta_eq), c_nonlinear
+DRIFT_LAW = (0.2, math.cos(130.0 / 180.0 * math.pi), 0.01)
+
+
+def move_flagged_to_end(verts, trigs, flagged, *per_vertex):
+    """The reference's scan that moves flagged vertices to the end of the vertex list
+    (ColocSimPin::set_x_boundary / rearrange_boundary, ColocSimPin.cpp:196-287): over the unsettled
+    range [0, k) a flagged vertex trades places with vertex k-1, the range shrinks and the vertex
+    that came in is examined next.  ``flagged(verts, i)`` may edit verts[i] (set_x_boundary puts the
+    wall vertices exactly on x = 0).  ``per_vertex`` arrays are permuted along.
+    Returns (verts, trigs, origin, count, *per_vertex): origin[p] = old index of the vertex now at p."""
+    v = np.array(verts, dtype=np.float64, copy=True)
+    t = np.array(trigs, dtype=np.int64, copy=True)
+    extra = [np.array(a, copy=True) for a in per_vertex]
+    n = len(v)
+    origin = np.arange(n)
+    k, i, moved = n, 0, 0
+    while i < k:
+        if not flagged(v, i):
+            i += 1
+            continue
+        j = k - 1
+        for arr in (v, origin, *extra):
+            arr[[i, j]] = arr[[j, i]]
+        k -= 1
+        moved += 1
+    where = np.empty(n, dtype=np.int64)
+    where[origin] = np.arange(n)
+    return (v, where[t], origin, moved, *extra)
+
+
+def _on_wall(v, i):
+    if abs(v[i, 0]) >= WALL_THRESHOLD:
+        return False
+    v[i, 0] = 0.0
+    return True
+
+
+class ColocSimPin(ColocSim):
+    """A bubble on the wall x = 0 with its contact line pinned to the wall: Bem::ColocSimPin
+    (Bem/Simulation/ColocSimPin.hpp:13-66, ColocSimPin.cpp:25-194).
+
+    The constructor moves the vertices with |x| < 1e-5 to the end of the vertex list and puts them on
+    x = 0 (set_x_boundary); ``perm`` holds the old index of each vertex, ``N_pin`` their number.
+    ``phi_init`` / ``psi_init`` (old order) become the initial state, as in the reference's second
+    constructor.  Every assembly exchanges the pinned columns of G and H after the 4 pi rule, the
+    stages use the stored psi in place of the potential at the pinned vertices, and the pinned
+    vertices slide along the wall with the drift velocity ``drift`` = (beta, cos theta_eq, c_nl).
+    The wall image is on by default (the reference's MIRROR_MESH build, the setting of its
+    pinned-bubble drivers).
+    """
+
+    def __init__(self, verts, trigs, p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.0, pressurefield=None,
+                 device=0, solver="bicgstab", mirror=True, phi_init=None, psi_init=None, drift=DRIFT_LAW):
+        n = len(verts)
+        phi0 = np.zeros(n) if phi_init is None else np.asarray(phi_init, dtype=np.float64)
+        psi0 = np.zeros(n) if psi_init is None else np.asarray(psi_init, dtype=np.float64)
+        v, t, self.perm, self.N_pin, phi0, psi0 = move_flagged_to_end(verts, trigs, _on_wall, phi0, psi0)
+        super().__init__(v, t, p_inf, epsilon, sigma, gamma, pressurefield, device, solver, mirror)
+        self.drift = tuple(float(d) for d in drift)
+        self._check(self._L.bem_set_pinned(self._h, int(self.N_pin), *self.drift))
+        self.set_phi(phi0)
+        self.set_psi(psi0)
+
+    def position_t(self, pot, verts=None, return_psi=False):
+        """ColocSimPin::position_t: vertex velocities; ``pot`` (float64, C-contiguous ndarray) receives
+        the solved potential at the pinned vertices, as the reference's PotVec& argument does."""
+        if not (isinstance(pot, np.ndarray) and pot.dtype == np.float64 and pot.flags.c_contiguous
+                and pot.flags.writeable and pot.shape == (self.N,)):
+            raise TypeError("pot must be a writable C-contiguous float64 array of N entries")
+        vel = np.empty((self.N, 3))
+        psi = np.empty(self.N)
+        v = None if verts is None else np.ascontiguousarray(verts, dtype=np.float64)
+        self._check(self._L.bem_position_t_inout(self._h, _d(v) if v is not None else None, _d(pot), _d(vel),
+                                                 _d(psi)))
+        return (vel, psi) if return_psi else vel
 
 
 def measure_fma_peaks(device=0):

@@ -33,8 +33,8 @@ public:
           damping_factor(0.0),
           min_elm_size(0.0),
           max_elm_size(std::numeric_limits<real>::max()) {
-        phi.assign(phi_dim(), 0.0);
-        psi.assign(psi_dim(), 0.0);
+        phi = Eigen::VectorXd::Zero((Eigen::Index)phi_dim());
+        psi = Eigen::VectorXd::Zero((Eigen::Index)psi_dim());
         image_wall_ = MIRROR_MESH;
         curvature_params = curvature_param();
     }
@@ -67,9 +67,15 @@ protected:
 
     void test_negative() const;
 
+    // RK4 and Euler through the virtual position_t / pot_t_multi, for subclasses that override them
+    // (the reference's own step sequence, LinLinSim.cpp:194-284); ColocSim itself steps on the GPU
+    void evolve_rk4_virtual(real dp, bool fixdt);
+    void evolve_euler_virtual(real dp, bool fixdt);
+
     std::vector<vec3> generate_tangent_gradients(Mesh const& m, std::vector<real> const& pot) const;
 
     std::vector<real> curvature_param() const;
+    void update_curvature_params();  // damped, clamped curvature_params before a remesh
 
     real damping_factor;
     real min_elm_size, max_elm_size;

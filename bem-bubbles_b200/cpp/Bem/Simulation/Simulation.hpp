@@ -53,6 +53,7 @@ public:
     // solving the system G*psi = H_phi for psi (Simulation.cpp:40-71), on the GPU
     Eigen::VectorXd solve_system(Eigen::MatrixXd const& G, Eigen::VectorXd const& H_phi) const;
 
+    // psi from the current state (Simulation.hpp:73-77)
     void compute_psi();
 
     virtual void evolve_system(real dp, bool fixdt = false) = 0;
@@ -62,30 +63,28 @@ public:
 
     void set_phi(std::vector<real> const& value) {
         assert(value.size() == phi_dim());
-        phi = value;
+        phi = make_copy(value);
     }
     void set_psi(std::vector<real> const& value) {
         assert(value.size() == psi_dim());
-        psi = value;
+        psi = make_copy(value);
     }
-    void set_phi(real value) {
-        for (real& v : phi) v = value;
-    }
+    void set_phi(real value) { phi.fill(value); }
     void set_V_0(real value) { V_0 = value; }
     real get_phi(size_t index) const {
         assert(index < phi_dim());
-        return phi[index];
+        return phi((Eigen::Index)index);
     }
     real get_psi(size_t index) const {
         assert(index < psi_dim());
-        return psi[index];
+        return psi((Eigen::Index)index);
     }
     void set_time(real const& value) { time = value; }
     real get_time() const { return time; }
     real get_volume() const { return volume(mesh); }
     const std::vector<vec3>& get_vertices() { return mesh.verts; }
-    std::vector<real> get_psi() { return psi; }
-    std::vector<real> get_phi() { return phi; }
+    std::vector<real> get_psi() { return make_copy(psi); }
+    std::vector<real> get_phi() { return make_copy(phi); }
     void set_min_dt(real value) { min_dt = value; }
     void set_dp_balance(real value) { dp_balance = value; }
     void set_bcgstab(bool value) { bicgstab = value; }
@@ -119,14 +118,17 @@ public:
 
 protected:
     Integrator inter;
-    std::vector<real> psi;
-    std::vector<real> phi;
+    // potential and its normal derivative on the surface, the reference's types (Simulation.hpp:204-208),
+    // so that subclasses written against the reference (ColocSimPin) compile unchanged
+    Eigen::VectorXd psi;
+    Eigen::VectorXd phi;
 
     // ---- GPU context (one per simulation object) and its synchronisation with the host state
     mutable bem_ctx* ctx_ = nullptr;
     mutable std::vector<Triplet> ctx_trigs_;  // topology the context was built for
     bool image_wall_ = false;                 // wall image at x = 0 (the reference's MIRROR_MESH)
     bem_ctx* context(Mesh const& m) const;    // context whose topology is m's (rebuilt on change)
+    virtual void configure_context(bem_ctx* c) const { (void)c; }  // subclass settings (pinned vertices)
     void push_state() const;                  // host mesh.verts, phi, psi, time, V_0, params -> device
     void pull_state();                        // device -> host
     void check(int status) const;             // status -> exception (std::out_of_range for x < 0)

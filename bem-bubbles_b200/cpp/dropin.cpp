@@ -7,13 +7,16 @@
 #include <cstdlib>
 #include <set>
 #include <stdexcept>
+#include <typeinfo>
 
 #include "Bem/Simulation/ColocSim.hpp"
+#include "Bem/Simulation/ColocSimPin.hpp"
 #include "Bem/Integration/Integrator.hpp"
 #include "Bem/Mesh/HalfedgeMesh.hpp"
 #include "Bem/Mesh/MeshIO.hpp"
 #include "Bem/Mesh/MeshManip.hpp"
 #include "../../include/bem_b200.h"
+#include "dropin_util.hpp"
 
 namespace Bem {
 
@@ -73,21 +76,8 @@ static double field_trampoline(const double x[3], double t, void* user) {
     return fn(vec3(x[0], x[1], x[2]), t);
 }
 
-static std::vector<double> flat(std::vector<vec3> const& v) {
-    std::vector<double> out(3 * v.size());
-    for (size_t i = 0; i < v.size(); ++i) {
-        out[3 * i] = v[i].x;
-        out[3 * i + 1] = v[i].y;
-        out[3 * i + 2] = v[i].z;
-    }
-    return out;
-}
-
-static std::vector<vec3> unflat(std::vector<double> const& f) {
-    std::vector<vec3> out(f.size() / 3);
-    for (size_t i = 0; i < out.size(); ++i) out[i] = vec3(f[3 * i], f[3 * i + 1], f[3 * i + 2]);
-    return out;
-}
+using dropin::flat;
+using dropin::unflat;
 
 bem_ctx* Simulation::context(Mesh const& m) const {
     if (!ctx_) {
@@ -121,6 +111,7 @@ bem_ctx* Simulation::context(Mesh const& m) const {
         check(bem_set_field_callback(ctx_, nullptr, nullptr));
     else
         check(bem_set_field_callback(ctx_, &field_trampoline, reinterpret_cast<void*>(pressurefield)));
+    configure_context(ctx_);
     return ctx_;
 }
 
@@ -155,10 +146,12 @@ Eigen::VectorXd Simulation::solve_system(Eigen::MatrixXd const& G, Eigen::Vector
 void Simulation::compute_psi() {
     Eigen::MatrixXd G, H;
     assemble_matrices_prop(G, H);
-    psi = make_copy(solve_system(G, H * make_copy(phi)));
+    psi = solve_system(G, H * phi);
 }
 
-void Simulation::export_mesh(std::string fname) const { export_ply_float(fname, mesh, phi, psi); }
+void Simulation::export_mesh(std::string fname) const {
+    export_ply_float(fname, mesh, make_copy(phi), make_copy(psi));
+}
 
 void Simulation::export_mesh_values(std::string fname, std::vector<real> values) const {
     export_ply_float(fname, mesh, values);
@@ -201,7 +194,17 @@ void LinLinSim::test_negative() const {
         }
 }
 
+// ColocSim and ColocSimPin step on the GPU in one call; another subclass (a user's class overriding
+// position_t or assemble_matrices) steps through its virtual functions.
+static bool steps_on_gpu(LinLinSim const* s) {
+    return typeid(*s) == typeid(ColocSim) || typeid(*s) == typeid(ColocSimPin);
+}
+
 void LinLinSim::evolve_system_RK4(real dp, bool fixdt) {
+    if (!steps_on_gpu(this)) {
+        evolve_rk4_virtual(dp, fixdt);
+        return;
+    }
     std::cout << "begin_RK4" << std::endl;
     test_negative();
     push_state();
@@ -214,10 +217,64 @@ void LinLinSim::evolve_system_RK4(real dp, bool fixdt) {
 }
 
 void LinLinSim::evolve_system(real dp, bool fixdt) {
+    if (!steps_on_gpu(this)) {
+        evolve_euler_virtual(dp, fixdt);
+        return;
+    }
     push_state();
     double dt = 0.0;
     check(bem_evolve_euler(ctx_, dp, fixdt ? 1 : 0, &dt));
     pull_state();
+}
+
+// The reference's RK4 step (LinLinSim.cpp:194-257) through the virtual position_t: four stages, each
+// pot_t_multi, the state-dependent potential passed by reference (a subclass may update entries of it,
+// as ColocSimPin does for its pinned vertices), the wall treatment, psi from the averaged velocity.
+// The call sequence and the vector expressions are the reference's, so that a subclass sees the same
+// calls in the same order.
+void LinLinSim::evolve_rk4_virtual(real dp, bool fixdt) {
+    std::cout << "begin_RK4" << std::endl;
+    test_negative();
+    Mesh m2 = mesh, m3 = mesh, m4 = mesh;
+    const CoordVec x1 = mesh.verts;
+    PotVec p1 = get_phi();
+    const CoordVec k1_x = position_t(mesh, p1);
+    const PotVec k1_p = pot_t_multi(mesh, k1_x, time);
+    const real dt = fixdt ? dp : get_dt(dp, k1_x, k1_p);
+    m2.verts = x1 + (0.5 * dt) * k1_x;
+    PotVec p2 = p1 + (0.5 * dt) * k1_p;
+    const CoordVec k2_x = position_t(m2, p2);
+    m3.verts = x1 + (0.5 * dt) * k2_x;
+    const PotVec k2_p = pot_t_multi(m2, k2_x, time);
+    PotVec p3 = p1 + (0.5 * dt) * k2_p;
+    const CoordVec k3_x = position_t(m3, p3);
+    m4.verts = x1 + dt * k3_x;
+    const PotVec k3_p = pot_t_multi(m3, k3_x, time);
+    PotVec p4 = p1 + dt * k3_p;
+    CoordVec k4_x = position_t(m4, p4);
+    CoordVec average = (k1_x + 2.0 * k2_x + 2.0 * k3_x + k4_x) * (1.0 / 6.0);
+    const PotVec pf = p1 + (dt / 6.0) * (pot_t_multi(mesh, k1_x, time) + 2.0 * pot_t_multi(m2, k2_x, time) +
+                                         2.0 * pot_t_multi(m3, k3_x, time) + pot_t_multi(m4, k4_x, time));
+    mesh.verts = nopenetration(eps, dt, x1, average);
+    const std::vector<vec3> normals = generate_vertex_normals(mesh);
+    PotVec new_psi(average.size());
+    for (size_t i = 0; i < average.size(); ++i) new_psi[i] = average[i].dot(normals[i]);
+    set_psi(new_psi);
+    set_phi(pf);
+    time += dt;
+    std::cout << "end_RK4" << std::endl;
+    test_negative();
+}
+
+// The reference's Euler step (LinLinSim.cpp:260-284) through the virtual position_t.
+void LinLinSim::evolve_euler_virtual(real dp, bool fixdt) {
+    PotVec p = make_copy(phi);
+    const CoordVec grads = position_t(mesh, p);
+    const PotVec pot_derivative = pot_t_multi(mesh, grads, time);
+    const real dt = fixdt ? dp : get_dt(dp, grads, pot_derivative);
+    mesh.verts = mesh.verts + grads * dt;
+    set_phi(p + dt * pot_derivative);
+    time += dt;
 }
 
 CoordVec LinLinSim::position_t(Mesh const& m, PotVec& pot) const {
@@ -258,6 +315,7 @@ std::vector<real> LinLinSim::kappa(Mesh const& m) const {
 CoordVec LinLinSim::nopenetration(real eps_, real dt, CoordVec const& x0, CoordVec& c) const {
     CoordVec xf(x0.size());
     for (size_t i = 0; i < x0.size(); ++i) xf[i] = x0[i] + dt * c[i];
+    size_t applied = 0;
     for (size_t i = 0; i < x0.size(); ++i) {
         const real cx = c[i].x;
         if (cx * dt >= 0.0) continue;
@@ -273,8 +331,12 @@ CoordVec LinLinSim::nopenetration(real eps_, real dt, CoordVec const& x0, CoordV
                 moved = true;
             }
         }
-        if (moved) c[i].x = (xf[i].x - xpos) / dt;
+        if (moved) {
+            c[i].x = (xf[i].x - xpos) / dt;
+            ++applied;
+        }
     }
+    if (applied > 0) std::cout << "applied exponential " << applied << " times.      ##" << std::endl;
     return xf;
 }
 
@@ -295,7 +357,7 @@ std::vector<vec3> LinLinSim::generate_tangent_gradients(Mesh const& m, std::vect
 // curvature and the potential's tangential gradient, smoothed over the two-ring
 std::vector<real> LinLinSim::curvature_param() const {
     std::vector<real> param = max_curvature(mesh);
-    const std::vector<vec3> grad = generate_tangent_gradients(mesh, phi);
+    const std::vector<vec3> grad = generate_tangent_gradients(mesh, make_copy(phi));
     std::vector<real> gsum(mesh.verts.size(), 0.0), cnt(mesh.verts.size(), 0.0);
     for (size_t j = 0; j < mesh.trigs.size(); ++j)
         for (size_t k = 0; k < 3; ++k) {
@@ -316,9 +378,11 @@ std::vector<real> LinLinSim::curvature_param() const {
 // LinLinSim::remesh (LinLinSim.cpp:385-438): one split pass, then alternating flips, relaxation and
 // collapses with the damped curvature parameter, then projection of the new vertices onto the old
 // surface with interpolation of phi.  Host-side topology editing with the user's mesh library.
-void LinLinSim::remesh(real L) {
-    // damped update d*old + (1-d)*new; after an earlier remesh changed the vertex count only the
-    // common prefix carries the old values, as the reference's element-wise vector sum does
+// The remeshing density: damped update d*old + (1-d)*new of curvature_params, clamped to the element
+// size bounds (LinLinSim.cpp:387-394, ColocSimPin.cpp:297-304).  After an earlier remesh changed the
+// vertex count only the common prefix carries the old values, as the reference's element-wise vector
+// sum does.
+void LinLinSim::update_curvature_params() {
     const std::vector<real> fresh = curvature_param();
     std::vector<real> mixed_params(fresh.size());
     for (size_t i = 0; i < fresh.size(); ++i)
@@ -327,6 +391,10 @@ void LinLinSim::remesh(real L) {
     curvature_params = mixed_params;
     if (min_elm_size > 0.0)
         for (real& c : curvature_params) c = std::max(std::min(c, 1.0 / min_elm_size), 1.0 / max_elm_size);
+}
+
+void LinLinSim::remesh(real L) {
+    update_curvature_params();
     HalfedgeMesh he(generate_halfedges(mesh));
     split_edges(he, curvature_params, L * 0.75);
     flip_edges(he, 1);
@@ -342,10 +410,10 @@ void LinLinSim::remesh(real L) {
     relax_vertices(he);
     std::vector<real> new_phi;
     Mesh next = generate_mesh(he);
-    project_and_interpolate(next, new_phi, mesh, phi);
+    project_and_interpolate(next, new_phi, mesh, make_copy(phi));
     mesh = next;
-    phi = new_phi;
-    psi.assign(mesh.verts.size(), 0.0);
+    phi = make_copy(new_phi);
+    psi = Eigen::VectorXd::Zero((Eigen::Index)mesh.verts.size());
 }
 
 // compute_exterior_pot (LinLinSim.cpp:440-477): potential at points off the surface, 19-point rule, on

@@ -620,6 +620,7 @@ static int adj_check_scope(Ctx& c) {
     if (c.prm.mirror) return c.fail(BEM_ERR_STATE, "adjoint: free-space bubbles only (no wall image)");
     if (c.prm.sigma != 0.0) return c.fail(BEM_ERR_STATE, "adjoint: sigma = 0 only");
     if (c.field_cb) return c.fail(BEM_ERR_STATE, "adjoint: device-evaluated field only");
+    if (c.n_pin) return c.fail(BEM_ERR_STATE, "adjoint: no pinned vertices");
     return BEM_OK;
 }
 

@@ -64,6 +64,8 @@ static void free_all(Ctx& c) {
     if (c.bstat_h) cudaFreeHost(c.bstat_h);
     c.bstat_h = nullptr;
     c.adj = AdjWork{};
+    c.n_pin = 0;
+    c.potz = nullptr;
 }
 
 // ---------------------------------------------------------------- topology preprocessing
@@ -268,13 +270,30 @@ static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream
     return rc;
 }
 
-// LinLinSim::position_t (LinLinSim.cpp:26-83)
-static int position_t(Ctx& c, const double* x, const double* pot, double* vel, cudaStream_t s) {
-    launch_assemble(c, x, pot, c.G, c.H, c.b, s);
+// G, H and b = H*pot for positions x.  With pinned vertices (ColocSimPin::assemble_matrices,
+// ColocSimPin.cpp:25-118) the pinned columns are exchanged after the 4 pi rule and the right-hand
+// side takes pin_vals at the pinned vertices.
+static void assemble_system(Ctx& c, const double* x, const double* pot, const double* pin_vals, cudaStream_t s) {
+    if (c.n_pin == 0) {
+        launch_assemble(c, x, pot, c.G, c.H, c.b, s);
+        return;
+    }
+    launch_pin_zero(c, pot, c.potz, s);
+    launch_assemble(c, x, c.potz, c.G, c.H, c.b, s);
+    launch_pin_exchange(c, pin_vals, c.b, s);
+}
+
+// LinLinSim::position_t (LinLinSim.cpp:26-83).  With pinned vertices ColocSimPin::position_t
+// (ColocSimPin.cpp:139-194): the stored psi stands in for pot at the pinned vertices, the pinned
+// vertices take the drift velocity, and pot receives the solved potential there (pot is in/out, as
+// the reference's PotVec& argument).
+static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStream_t s) {
+    assemble_system(c, x, pot, c.psi, s);
     int rc = solve(c, c.G, c.b, c.psil, s);
     if (rc) return rc;
     launch_velocity_prep(c, x, pot, s);
     launch_velocity(c, c.psil, vel, s);
+    if (c.n_pin) launch_pin_finish(c, x, vel, pot, s);
     return BEM_OK;
 }
 
@@ -403,7 +422,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     for (auto p : vec3s)
         if ((rc = dalloc(c, p, 3 * n))) return rc;
     double** vecs[] = {&c.phi, &c.psi, &c.b, &c.psil, &c.kap, &c.fieldv, &c.p1, &c.ps, &c.kp1, &c.kp2,
-                       &c.kp3, &c.kp4, &c.r, &c.r0, &c.pv, &c.vv, &c.yv, &c.zv, &c.sv, &c.tv, &c.invd};
+                       &c.kp3, &c.kp4, &c.r, &c.r0, &c.pv, &c.vv, &c.yv, &c.zv, &c.sv, &c.tv, &c.invd, &c.potz};
     for (auto p : vecs)
         if ((rc = dalloc(c, p, n))) return rc;
     if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (!c.batch && (rc = dalloc(c, &c.LU, nn))) ||
@@ -879,7 +898,7 @@ int bem_exterior_potential(bem_ctx* c, int64_t P, const double* points, const do
     if (e != cudaSuccess) rc = c->fail(BEM_ERR_CUDA, std::string("exterior potential: ") + cudaGetErrorString(e));
     if (rc == BEM_OK && !psi) {
         // LinLinSim::exterior_pot (LinLinSim.cpp:479-485): psi_l = solve_system(G, H*phi) first
-        launch_assemble(*c, c->x, phid, c->G, c->H, c->b, s);
+        assemble_system(*c, c->x, phid, phid, s);
         rc = solve(*c, c->G, c->b, c->psil, s);
         psid = c->psil;
     }
@@ -1067,6 +1086,7 @@ int bem_assemble(bem_ctx* c, const double* verts, double* G, double* H) {
     }
     BEM_CUDA(*c, cudaMemsetAsync(c->p1, 0, sizeof(double) * N, c->stream));
     launch_assemble(*c, x, c->p1, c->G, c->H, nullptr, c->stream);
+    if (c->n_pin) launch_pin_exchange(*c, c->p1, nullptr, c->stream);
     BEM_CUDA(*c, cudaGetLastError());
     const int64_t nn = c->batch ? (int64_t)c->blk_elems : N * N;  // batches: the packed blocks
     if (G) COPY_OUT(G, c->G, nn);
@@ -1089,7 +1109,8 @@ int bem_solve_system(bem_ctx* c, const double* G, const double* b, double* x) {
     return BEM_OK;
 }
 
-int bem_position_t(bem_ctx* c, const double* verts, const double* pot, double* vel, double* psi_l) {
+static int position_t_host(bem_ctx* c, const double* verts, const double* pot, double* pot_out, double* vel,
+                           double* psi_l) {
     CTX_GUARD(c);
     NEED_MESH(c);
     const int64_t N = c->topo.N;
@@ -1105,6 +1126,34 @@ int bem_position_t(bem_ctx* c, const double* verts, const double* pot, double* v
     BEM_CUDA(*c, cudaGetLastError());
     COPY_OUT(vel, c->k1, 3 * N);
     if (psi_l) COPY_OUT(psi_l, c->psil, N);
+    if (pot_out) COPY_OUT(pot_out, c->ps, N);
+    return BEM_OK;
+}
+
+int bem_position_t(bem_ctx* c, const double* verts, const double* pot, double* vel, double* psi_l) {
+    return position_t_host(c, verts, pot, nullptr, vel, psi_l);
+}
+
+int bem_position_t_inout(bem_ctx* c, const double* verts, double* pot, double* vel, double* psi_l) {
+    return position_t_host(c, verts, pot, pot, vel, psi_l);
+}
+
+int bem_set_pinned(bem_ctx* c, int64_t n_pin, double beta, double costheta_eq, double c_nonlinear) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (n_pin < 0 || n_pin >= c->topo.N) return c->fail(BEM_ERR_ARG, "pinned count out of range");
+    if (n_pin > 0 && c->batch) return c->fail(BEM_ERR_STATE, "pinned vertices: single systems only");
+    if (n_pin != c->n_pin) c->xinv_valid = false;  // the exchanged system is another matrix
+    c->n_pin = n_pin;
+    c->pin_beta = beta;
+    c->pin_cos_eq = costheta_eq;
+    c->pin_cnl = c_nonlinear;
+    return BEM_OK;
+}
+
+int bem_get_pinned(const bem_ctx* c, int64_t* n_pin) {
+    if (!c || !n_pin) return BEM_ERR_ARG;
+    *n_pin = c->n_pin;
     return BEM_OK;
 }
 

@@ -128,6 +128,12 @@ struct Ctx {
     double graph_dt = 0.0;
     long long graph_launches = 0;
 
+    // ---- pinned contact line (pin.cu): the last n_pin vertices lie on the wall x = 0; drift-velocity
+    // law beta (cos_eq - c) + c_nl c^3 / (c^2 - 1)
+    int64_t n_pin = 0;
+    double pin_beta = 0.0, pin_cos_eq = 0.0, pin_cnl = 0.0;
+    double* potz = nullptr;  // N: stage potential with the pinned entries zeroed
+
     AdjWork adj;
     PlyExporter* exporter = nullptr;  // asynchronous PLY writer (export.cu)
     std::vector<int> h_tri;           // host copy of the triangles (M*3)

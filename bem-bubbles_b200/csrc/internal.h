@@ -114,6 +114,11 @@ void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cud
 void launch_any_negative(Ctx& c, const double* x, int* flag, cudaStream_t s);
 void launch_curvature(Ctx& c, const double* x, double* kap, cudaStream_t s);
 
+// pin.cu
+void launch_pin_zero(Ctx& c, const double* pot, double* potz, cudaStream_t s);
+void launch_pin_exchange(Ctx& c, const double* v, double* b, cudaStream_t s);
+void launch_pin_finish(Ctx& c, const double* x, double* vel, double* pot, cudaStream_t s);
+
 // Newton-Schulz job: X ~ A^-1 for an n x n column-major FP64 matrix A, with its FP32 copy G32 and
 // FP32 work matrices T, P (all n x n).
 struct NSJob {

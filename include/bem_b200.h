@@ -109,6 +109,25 @@ int bem_solve_system(bem_ctx* ctx, const double* G, const double* b, double* x);
 /* LinLinSim::position_t (LinLinSim.cpp:26-83): vertex velocities for positions `verts` (NULL = mesh)
  * and potential `pot`.  psi_l (the solved dphi/dn) may be NULL. */
 int bem_position_t(bem_ctx* ctx, const double* verts, const double* pot, double* vel, double* psi_l);
+/* bem_position_t with pot in/out, as the reference's PotVec& argument: with pinned vertices
+ * (bem_set_pinned) pot receives the solved potential at the pinned vertices (ColocSimPin.cpp:188). */
+int bem_position_t_inout(bem_ctx* ctx, const double* verts, double* pot, double* vel, double* psi_l);
+
+/* ---- Pinned contact line: the reference's ColocSimPin (Bem/Simulation/ColocSimPin.cpp:25-194),
+ * replacing ColocSimPin::assemble_matrices and ColocSimPin::position_t.  The last n_pin vertices of the
+ * mesh lie on the wall x = 0 (ColocSimPin::set_x_boundary moves them to the end).  With n_pin > 0:
+ *  - every assembly (bem_assemble, the steps, the exterior potential's solve) exchanges the pinned
+ *    columns after the 4 pi rule: G(:,j) = -H(:,j), H(:,j) = -G(:,j) (ColocSimPin.cpp:113-117);
+ *  - position_t and the RK4/Euler stages use the stored psi (bem_set_psi) in place of the stage
+ *    potential at the pinned vertices in H*pot (:146-148), move the pinned vertices with the drift
+ *    velocity n_w * (beta (costheta_eq - c) + c_nonlinear c^3 / (c^2 - 1)), c = vertex normal . e_x,
+ *    n_w the vertex normal with its x component removed, normalised (:126-136, :175-186), and set the
+ *    stage potential at the pinned vertices to the solved unknowns (:188).
+ * The reference's law: beta = 0.2, costheta_eq = cos(130 deg), c_nonlinear = 0.01 (:122-126).
+ * n_pin = 0 switches pinning off; bem_set_mesh and bem_set_mesh_blocks reset it.  Single systems only;
+ * the adjoint refuses pinned vertices. */
+int bem_set_pinned(bem_ctx* ctx, int64_t n_pin, double beta, double costheta_eq, double c_nonlinear);
+int bem_get_pinned(const bem_ctx* ctx, int64_t* n_pin);
 /* LinLinSim::pot_t_multi (LinLinSim.cpp:98-120): Dphi/Dt per vertex for positions `verts`
  * (NULL = mesh), vertex velocities `grads` and time t. */
 int bem_pot_t_multi(bem_ctx* ctx, const double* verts, const double* grads, double t, double* out);

@@ -8,9 +8,16 @@ for the comparison with the same drivers linked against the drop-in library (tes
 * dropin_check/: oracle/dropin_check.cpp (oracle/_ref/refdrv/dropin_check) on the icosphere nu = 7:
   its three exports ref-0..ref-2 and its exterior-potential probe (ref_exterior.txt).  This driver is
   reproducible bit for bit across thread counts.
+* pinned_check/: oracle/pinned_check.cpp (oracle/_ref/refdrv/pinned_check, the reference's ColocSimPin)
+  on the wall cap nu = 6 (bem_b200.mesh.wall_cap): its three exports ref-0..ref-2 and its printed
+  block and pinned-vertex lines (ref_stdout.txt).  The reference's ColocSimPin assembly adds the
+  triangles' columns in thread order (omp_set_num_threads(num_threads), 100 by default), so two runs
+  differ by rounding (6e-16 relative in these lines).
 
-Run from the repository root after `make -C oracle refdrivers`; takes a few minutes.
+Run from the repository root after `make -C oracle refdrivers`; takes a few minutes
+(`--only pinned` for the last part alone).
 """
+import argparse
 import os
 import shutil
 import subprocess
@@ -29,7 +36,27 @@ ARGS = ["3e-6", "50000", "out"]
 EXPORTS = 3
 
 
+def pinned_check():
+    out_dir = os.path.join(HERE, "pinned_check")
+    os.makedirs(out_dir, exist_ok=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        v, f = mesh.wall_cap(6)
+        write_ply(os.path.join(tmp, "cap-6.ply"), v, f)
+        os.makedirs(os.path.join(tmp, "borderprojects"))
+        exe = os.path.join(ROOT, "oracle", "_ref", "refdrv", "pinned_check")
+        r = subprocess.run([exe, os.path.join(tmp, "cap-6.ply"), os.path.join(out_dir, "ref")], check=True,
+                           capture_output=True, text=True, cwd=tmp)
+        with open(os.path.join(out_dir, "ref_stdout.txt"), "w") as fh:
+            fh.writelines(ln + "\n" for ln in r.stdout.splitlines() if ln.startswith(("block ", "pinned ")))
+    print("wrote", out_dir)
+
+
 def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", choices=["pinned"], default=None)
+    if ap.parse_args().only == "pinned":
+        pinned_check()
+        return
     exe = os.path.join(ROOT, "oracle", "_ref", "refdrv", "oscillations")
     out_dir = os.path.join(HERE, "dropin_oscillations")
     os.makedirs(out_dir, exist_ok=True)
@@ -60,6 +87,7 @@ def main():
         with open(os.path.join(check_dir, "ref_exterior.txt"), "w") as fh:
             fh.writelines(ln + "\n" for ln in r.stdout.splitlines() if ln.startswith("exterior "))
     print("wrote", check_dir)
+    pinned_check()
 
 
 if __name__ == "__main__":

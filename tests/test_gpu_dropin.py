@@ -101,3 +101,38 @@ def test_dropin_classes_match_reference_classes(tmp_path):
     ref = [float(ln.split()[2]) for ln in open(os.path.join(gold, "ref_exterior.txt"))]
     assert len(got) == len(ref) == 4
     assert np.max(np.abs(np.array(got) - ref)) <= 1e-8 * np.max(np.abs(ref))
+
+
+PINNED = os.path.join(DROP, "pinned_check")
+
+
+@pytest.mark.skipif(not os.path.exists(PINNED), reason="drop-in pinned driver not built (make -C oracle dropin)")
+def test_dropin_colocsimpin_matches_reference_class(tmp_path):
+    # oracle/pinned_check.cpp: the drop-in ColocSimPin (GPU steps, host remesh) against the reference's
+    # ColocSimPin.cpp built on the CPU (tests/golden/pinned_check): three blocks, the last two starting
+    # with the contact-line-preserving remesh
+    v, f = mesh.wall_cap(6)
+    write_ply(str(tmp_path / "cap-6.ply"), v, f)
+    (tmp_path / "borderprojects").mkdir()
+    p = subprocess.run([PINNED, str(tmp_path / "cap-6.ply"), str(tmp_path / "gpu")], capture_output=True, text=True,
+                       timeout=600, cwd=tmp_path)
+    assert p.returncode == 0, p.stderr[-2000:]
+    gold = os.path.join(ROOT, "tests", "golden", "pinned_check")
+    got = [ln.split() for ln in p.stdout.splitlines() if ln.startswith(("block ", "pinned "))]
+    ref = [ln.split() for ln in open(os.path.join(gold, "ref_stdout.txt"))]
+    assert len(got) == len(ref)
+    for a, b in zip(got, ref):
+        # "block k time T volume V verts N npin P" / "pinned k i x y z phi": floats at 3, 5 / 3..6
+        fl = [3, 5] if a[0] == "block" else [3, 4, 5, 6]
+        assert [w for i, w in enumerate(a) if i not in fl] == [w for i, w in enumerate(b) if i not in fl], (a, b)
+        va, vb = np.array([float(a[i]) for i in fl]), np.array([float(b[i]) for i in fl])
+        assert np.all(np.abs(va - vb) <= 1e-8 * np.maximum(np.abs(vb), 1.0)), (a, b)
+    for k in range(3):
+        x, e, t = read_ply(str(tmp_path / f"gpu-{k}.ply"))
+        xr, er, tr = read_ply(os.path.join(gold, f"ref-{k}.ply"))
+        assert x.shape == xr.shape and np.array_equal(t, tr), k
+        assert np.max(np.abs(x - xr)) <= 1e-6, k
+        for q in ("phi", "psi"):
+            assert np.max(np.abs(e[q] - er[q])) <= 1e-6 * max(np.max(np.abs(er[q])), 1e-30), (k, q)
+    # the boundary projections of the two remeshes (ColocSimPin.cpp:573-578)
+    assert sorted(os.listdir(tmp_path / "borderprojects")) == ["mesh-0.ply", "mesh-1.ply"]
