@@ -127,6 +127,7 @@ protected:
     mutable bem_ctx* ctx_ = nullptr;
     mutable std::vector<Triplet> ctx_trigs_;  // topology the context was built for
     bool image_wall_ = false;                 // wall image at x = 0 (the reference's MIRROR_MESH)
+    bem_ctx* device_ctx() const;              // the context, created on first use (no mesh needed)
     bem_ctx* context(Mesh const& m) const;    // context whose topology is m's (rebuilt on change)
     virtual void configure_context(bem_ctx* c) const { (void)c; }  // subclass settings (pinned vertices)
     void push_state() const;                  // host mesh.verts, phi, psi, time, V_0, params -> device

@@ -79,12 +79,17 @@ static double field_trampoline(const double x[3], double t, void* user) {
 using dropin::flat;
 using dropin::unflat;
 
-bem_ctx* Simulation::context(Mesh const& m) const {
+bem_ctx* Simulation::device_ctx() const {
     if (!ctx_) {
         int dev = 0;
         if (const char* e = std::getenv("BEM_DEVICE")) dev = std::atoi(e);
         check(bem_create(&ctx_, dev, nullptr));
     }
+    return ctx_;
+}
+
+bem_ctx* Simulation::context(Mesh const& m) const {
+    device_ctx();
     bem_params p;
     bem_default_params(&p);
     p.p_inf = p_inf;
@@ -377,7 +382,8 @@ std::vector<real> LinLinSim::curvature_param() const {
 
 // LinLinSim::remesh (LinLinSim.cpp:385-438): one split pass, then alternating flips, relaxation and
 // collapses with the damped curvature parameter, then projection of the new vertices onto the old
-// surface with interpolation of phi.  Host-side topology editing with the user's mesh library.
+// surface with interpolation of phi.  Host-side topology editing with the user's mesh library; the
+// projection's ray casting on the GPU.
 // The remeshing density: damped update d*old + (1-d)*new of curvature_params, clamped to the element
 // size bounds (LinLinSim.cpp:387-394, ColocSimPin.cpp:297-304).  After an earlier remesh changed the
 // vertex count only the common prefix carries the old values, as the reference's element-wise vector
@@ -410,7 +416,8 @@ void LinLinSim::remesh(real L) {
     relax_vertices(he);
     std::vector<real> new_phi;
     Mesh next = generate_mesh(he);
-    project_and_interpolate(next, new_phi, mesh, make_copy(phi));
+    dropin::project_interpolate(device_ctx(), next, generate_vertex_normals(next), mesh, make_copy(phi), new_phi,
+                                nullptr, nullptr, true);
     mesh = next;
     phi = make_copy(new_phi);
     psi = Eigen::VectorXd::Zero((Eigen::Index)mesh.verts.size());

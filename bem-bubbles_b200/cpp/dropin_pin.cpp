@@ -252,7 +252,8 @@ void ColocSimPin::remesh(real L) {
     normals.resize(normals.size() - N_pin);
     std::vector<real> new_phi, new_psi;
     const CoordVec x0 = next.verts;
-    project_and_interpolate(next, normals, new_phi, new_psi, mesh, make_copy(phi), make_copy(psi));
+    const std::vector<real> old_phi = make_copy(phi), old_psi = make_copy(psi);
+    dropin::project_interpolate(device_ctx(), next, normals, mesh, old_phi, new_phi, &old_psi, &new_psi, false);
     CoordVec shift = next.verts + (-1.0) * x0;
     next.verts = nopenetration(eps, 1.0, x0, shift);
 

@@ -514,6 +514,7 @@ int bem_destroy(bem_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_all(*c);
+    cudaFree(c->trace_buf);
     cudaFree(c->sc);
     cudaFree(c->flag);
     cudaFreeHost(c->h_sc);
@@ -1149,6 +1150,17 @@ int bem_set_pinned(bem_ctx* c, int64_t n_pin, double beta, double costheta_eq, d
     c->pin_cos_eq = costheta_eq;
     c->pin_cnl = c_nonlinear;
     return BEM_OK;
+}
+
+int bem_trace_mesh(bem_ctx* c, int64_t nverts, const double* verts, int64_t M, const int64_t* trigs, int64_t P,
+                   const double* pos, const double* dir, double* hit, int64_t* tri, int32_t* ok) {
+    CTX_GUARD(c);
+    if (P < 0 || nverts < 3 || M < 1 || !verts || !trigs) return c->fail(BEM_ERR_ARG, "bad trace arguments");
+    if (P == 0) return BEM_OK;
+    if (!pos || !dir || !hit || !tri || !ok) return c->fail(BEM_ERR_ARG, "null pointer");
+    for (int64_t k = 0; k < 3 * M; ++k)
+        if (trigs[k] < 0 || trigs[k] >= nverts) return c->fail(BEM_ERR_ARG, "triangle index out of range");
+    return trace_mesh(*c, nverts, verts, M, trigs, P, pos, dir, hit, tri, ok);
 }
 
 int bem_get_pinned(const bem_ctx* c, int64_t* n_pin) {

@@ -134,6 +134,10 @@ struct Ctx {
     double pin_beta = 0.0, pin_cos_eq = 0.0, pin_cnl = 0.0;
     double* potz = nullptr;  // N: stage potential with the pinned entries zeroed
 
+    // remesh ray casting (remesh.cu): one device buffer, grown on demand, kept across meshes
+    void* trace_buf = nullptr;
+    size_t trace_cap = 0;
+
     AdjWork adj;
     PlyExporter* exporter = nullptr;  // asynchronous PLY writer (export.cu)
     std::vector<int> h_tri;           // host copy of the triangles (M*3)

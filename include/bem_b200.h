@@ -123,11 +123,21 @@ int bem_position_t_inout(bem_ctx* ctx, const double* verts, double* pot, double*
  *    velocity n_w * (beta (costheta_eq - c) + c_nonlinear c^3 / (c^2 - 1)), c = vertex normal . e_x,
  *    n_w the vertex normal with its x component removed, normalised (:126-136, :175-186), and set the
  *    stage potential at the pinned vertices to the solved unknowns (:188).
- * The reference's law: beta = 0.2, costheta_eq = cos(130 deg), c_nonlinear = 0.01 (:122-126).
+ * The reference's law: beta = 0.2, costheta_eq = cos(130 deg), c_nonlinear = 0.01 (:126-130).
  * n_pin = 0 switches pinning off; bem_set_mesh and bem_set_mesh_blocks reset it.  Single systems only;
  * the adjoint refuses pinned vertices. */
 int bem_set_pinned(bem_ctx* ctx, int64_t n_pin, double beta, double costheta_eq, double c_nonlinear);
 int bem_get_pinned(const bem_ctx* ctx, int64_t* n_pin);
+
+/* ---- Remeshing support.  trace_mesh (Bem/Mesh/MeshManip.cpp:1250-1283) for P rays on the device, the
+ * O(P x M) scan of project_and_interpolate (MeshManip.cpp:1426-1697): ray k starts at pos[3k..] with
+ * direction dir[3k..]; among the triangles of the mesh (verts: nverts x 3, trigs: M x 3) whose closed
+ * interior contains the intersection with the triangle's plane, the one with the smallest |s| is taken
+ * (the first in triangle order on ties).  hit[3k..] receives the intersection, tri[k] the triangle and
+ * ok[k] 1; a ray that hits nothing gets ok 0, hit (0,0,0) and triangle 0.  Results are bit-identical to
+ * the host scan.  Uses the context's device and stream only (no mesh needed). */
+int bem_trace_mesh(bem_ctx* ctx, int64_t nverts, const double* verts, int64_t M, const int64_t* trigs, int64_t P,
+                   const double* pos, const double* dir, double* hit, int64_t* tri, int32_t* ok);
 /* LinLinSim::pot_t_multi (LinLinSim.cpp:98-120): Dphi/Dt per vertex for positions `verts`
  * (NULL = mesh), vertex velocities `grads` and time t. */
 int bem_pot_t_multi(bem_ctx* ctx, const double* verts, const double* grads, double t, double* out);

@@ -17,6 +17,18 @@ using namespace Bem;
 
 static real field(vec3 x, real t) { return -0.3 * std::sin(0.7 * t + 0.2 * x.x); }
 
+#ifdef CHECK_SUBCLASS
+// A user's class derived from ColocSim (built with -DCHECK_SUBCLASS against the drop-in): the drop-in
+// steps such classes through their virtual position_t and pot_t_multi, stage by stage, in the
+// reference's RK4/Euler call sequence; the results must agree with ColocSim's own all-GPU step.
+struct UserSim : ColocSim {
+    using ColocSim::ColocSim;
+};
+using Sim = UserSim;
+#else
+using Sim = ColocSim;
+#endif
+
 int main(int argc, char* argv[]) {
     if (argc != 3) {
         std::cerr << "usage: dropin_check <in.ply> <out_prefix>" << std::endl;
@@ -28,7 +40,7 @@ int main(int argc, char* argv[]) {
     // radial perturbation 1 + 0.02 sin(3 theta)-like, deterministic, then away from the wall
     for (vec3& v : M.verts) v = v * (1.0 + 0.02 * std::sin(3.0 * v.z + v.y));
     M.translate(vec3(3.0, 0.0, 0.0));
-    ColocSim sim(M, 1.0, 1.4, 0.0, 1.4, &field);
+    Sim sim(M, 1.0, 1.4, 0.0, 1.4, &field);
     sim.set_bcgstab(false);
     sim.set_phi(0.05);
     sim.set_damping_factor(0.2);

@@ -82,11 +82,14 @@ CHECK = os.path.join(DROP, "dropin_check")
 
 
 @pytest.mark.skipif(not os.path.exists(CHECK), reason="drop-in check driver not built (make -C oracle dropin)")
-def test_dropin_classes_match_reference_classes(tmp_path):
+@pytest.mark.parametrize("driver", ["dropin_check", "dropin_check_sub"])
+def test_dropin_classes_match_reference_classes(tmp_path, driver):
+    # dropin_check_sub: the same driver on a user subclass of ColocSim, stepped through the virtual
+    # position_t / pot_t_multi (the reference's RK4 and Euler call sequence on the host)
     v, f = mesh.icosphere(7)
     write_ply(str(tmp_path / "ico7.ply"), v, f)
-    p = subprocess.run([CHECK, str(tmp_path / "ico7.ply"), str(tmp_path / "gpu")], capture_output=True, text=True,
-                       timeout=600)
+    p = subprocess.run([os.path.join(DROP, driver), str(tmp_path / "ico7.ply"), str(tmp_path / "gpu")],
+                       capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     gold = os.path.join(ROOT, "tests", "golden", "dropin_check")
     for k in range(3):
@@ -136,3 +139,21 @@ def test_dropin_colocsimpin_matches_reference_class(tmp_path):
             assert np.max(np.abs(e[q] - er[q])) <= 1e-6 * max(np.max(np.abs(er[q])), 1e-30), (k, q)
     # the boundary projections of the two remeshes (ColocSimPin.cpp:573-578)
     assert sorted(os.listdir(tmp_path / "borderprojects")) == ["mesh-0.ply", "mesh-1.ply"]
+
+
+PROJECT = os.path.join(DROP, "project_check")
+
+
+@pytest.mark.skipif(not os.path.exists(PROJECT), reason="projection check not built (make -C oracle dropin)")
+@pytest.mark.parametrize("nu,L", [(10, 0.25), (20, 0.12)])
+def test_remesh_projection_bit_identical_to_library(tmp_path, nu, L):
+    # oracle/project_check.cpp: project_and_interpolate of the user's mesh library (both overloads)
+    # against the drop-in's projection with the ray casting on the GPU, compared bit for bit
+    v, f = mesh.icosphere(nu)
+    write_ply(str(tmp_path / "ico.ply"), v, f)
+    p = subprocess.run([PROJECT, str(tmp_path / "ico.ply"), str(L)], capture_output=True, text=True, timeout=600)
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("project ")]
+    assert p.returncode == 0 and len(lines) == 2, (p.stdout[-2000:], p.stderr[-2000:])
+    for ln in lines:
+        print(ln)
+        assert ln.split()[ln.split().index("differing") + 1] == "0", ln
