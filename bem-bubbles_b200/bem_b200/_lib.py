@@ -39,7 +39,8 @@ class Params(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("solves", C.c_int64), ("last_iters", C.c_int32), ("precond_refresh", C.c_int32),
-                ("last_rel_residual", C.c_double), ("ns_steps", C.c_int64), ("gmres_fallbacks", C.c_int64)]
+                ("last_rel_residual", C.c_double), ("ns_steps", C.c_int64), ("gmres_fallbacks", C.c_int64),
+                ("fp64_fallbacks", C.c_int64)]
 
 
 class Profile(C.Structure):

@@ -66,6 +66,7 @@ static void free_all(Ctx& c) {
     c.adj = AdjWork{};
     c.n_pin = 0;
     c.potz = nullptr;
+    c.mixed_backoff = 0;
 }
 
 // ---------------------------------------------------------------- topology preprocessing

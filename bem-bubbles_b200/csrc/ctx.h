@@ -88,6 +88,7 @@ struct Ctx {
     double* Z = nullptr;       // N*m preconditioned directions
     double* hcol = nullptr;    // (m+2) Hessenberg column / dot results
     bool xinv_valid = false;
+    int mixed_backoff = 0;  // solves left that skip the mixed path after it failed (FP64 BiCGSTAB instead)
     int ir_steps = 3;  // refinement steps issued per round of the mixed solve (adapted)
     int gmres_m = 30;
 

@@ -961,11 +961,28 @@ __global__ void k_rowblock_norm2(int n, const double* __restrict__ b, double* __
 // without host synchronisation, with the residual norms of every step kept on the device and read
 // once.  A contraction too weak for refinement hands over to GMRES (same preconditioner, same
 // start vector); a contraction above 0.02 triggers a Newton-Schulz refresh of X.
+// The FP64 BiCGSTAB (the reference's default solver) in place of the mixed solve, for a matrix the
+// mixed path cannot handle: no approximate inverse converges (G singular or nearly so -- the
+// reference's own BiCGSTAB then returns what it returns), or GMRES misses the tolerance.  After a
+// failed inverse the next MIXED_BACKOFF solves go straight here instead of retrying the set-up.
+constexpr int MIXED_BACKOFF = 16;
+static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s, bool backoff) {
+    c.stats.fp64_fallbacks++;
+    c.stats.solves++;
+    if (backoff) c.mixed_backoff = MIXED_BACKOFF;
+    return bicgstab(c, A, b, x, s);
+}
+
 int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
     const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
+    if (c.mixed_backoff > 0) {
+        --c.mixed_backoff;
+        return fp64_fallback(c, A, b, x, s, false);
+    }
     if (!c.xinv_valid) {
         int rc = refresh_inverse(c, A, s, true);
+        if (rc == BEM_ERR_NOT_CONVERGED) return fp64_fallback(c, A, b, x, s, true);
         if (rc) return rc;
     }
     const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
@@ -1019,6 +1036,10 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     if (!converged) {
         c.stats.gmres_fallbacks++;
         rc = gmres_solve(c, A, b, x, s);
+        if (rc == BEM_ERR_NOT_CONVERGED) {
+            c.xinv_valid = false;
+            return fp64_fallback(c, A, b, x, s, true);
+        }
         rho = 1.0;
     } else {
         c.stats.last_rel_residual = rel;
@@ -1027,7 +1048,14 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     // steps for the next solve from the observed contraction, and the refresh policy
     if (converged && rho > 0.0 && rel0 > tol)
         c.ir_steps = std::max(1, std::min(KMAX, (int)ceil(log(tol / rel0) / log(std::max(rho, 1e-6)))));
-    if (rc == BEM_OK && rho > 0.02) rc = refresh_inverse(c, A, s, false);
+    if (rc == BEM_OK && rho > 0.02) {
+        rc = refresh_inverse(c, A, s, false);
+        if (rc == BEM_ERR_NOT_CONVERGED) {  // this solve stands; the next one starts over or falls back
+            c.xinv_valid = false;
+            c.mixed_backoff = MIXED_BACKOFF;
+            rc = BEM_OK;
+        }
+    }
     return rc;
 }
 

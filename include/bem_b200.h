@@ -230,6 +230,9 @@ typedef struct {
     double last_rel_residual; /* final relative residual of the last iterative solve */
     int64_t ns_steps;         /* Newton-Schulz steps taken by the mixed path (set-up and refreshes) */
     int64_t gmres_fallbacks;  /* mixed solves that handed over from refinement to GMRES */
+    int64_t fp64_fallbacks;   /* mixed solves that fell back to the FP64 BiCGSTAB: no approximate inverse
+                                 could be built, or GMRES missed the tolerance (a singular or nearly
+                                 singular G, e.g. a bubble cut by its own wall image) */
 } bem_stats;
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 
