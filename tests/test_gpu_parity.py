@@ -202,6 +202,21 @@ def test_negative_x_raises_like_reference():
         sim.evolve_system_RK4(1e-3, fixdt=True)
 
 
+def test_mixed_solver_falls_back_on_singular_system():
+    # a bubble centred on the wall plane with the wall image on: G = S + S R annihilates the modes odd
+    # in x, so no approximate inverse exists.  The mixed solve hands over to the FP64 BiCGSTAB (the
+    # reference's solver, which returns its iterate there) instead of failing; Euler steps, as the
+    # reference's oscillations driver takes them (no x < 0 check).
+    v, f = mesh.bubble(4, 1.0, (0.0, 0.0, 0.0))
+    sim = ColocSim(v, f, mirror=True, solver="mixed")
+    sim.set_phi(0.05 + 0.01 * v[:, 2])
+    for _ in range(3):
+        sim.evolve_system(1e-3, fixdt=True)
+    st = sim.stats()
+    assert st.fp64_fallbacks >= 1
+    assert np.all(np.isfinite(sim.get_vertices())) and np.all(np.isfinite(sim.get_phi()))
+
+
 def test_mixed_precision_error_headline_size():
     # N = 4002 (config 2 mesh with the seeded 1% radial perturbation): psi of the mixed path
     # against the FP64 LU path at <= 1e-8 relative
