@@ -67,6 +67,8 @@ static void free_all(Ctx& c) {
     c.n_pin = 0;
     c.potz = nullptr;
     c.mixed_backoff = 0;
+    c.ir_base = -1;
+    c.ir_excess = 0;
 }
 
 // ---------------------------------------------------------------- topology preprocessing

@@ -89,6 +89,8 @@ struct Ctx {
     double* hcol = nullptr;    // (m+2) Hessenberg column / dot results
     bool xinv_valid = false;
     int mixed_backoff = 0;  // solves left that skip the mixed path after it failed (FP64 BiCGSTAB instead)
+    int ir_base = -1;       // fewest refinement steps of a solve since the last refresh of X
+    int ir_excess = 0;      // refinement steps paid above ir_base since the last refresh
     int ir_steps = 3;  // refinement steps issued per round of the mixed solve (adapted)
     int gmres_m = 30;
 

@@ -960,7 +960,7 @@ __global__ void k_rowblock_norm2(int n, const double* __restrict__ b, double* __
 // Warm-started from the previous solution (the previous RK4 stage's psi); K steps are issued
 // without host synchronisation, with the residual norms of every step kept on the device and read
 // once.  A contraction too weak for refinement hands over to GMRES (same preconditioner, same
-// start vector); a contraction above 0.02 triggers a Newton-Schulz refresh of X.
+// start vector); a Newton-Schulz refresh of X follows the cost rule at the end.
 // The FP64 BiCGSTAB (the reference's default solver) in place of the mixed solve, for a matrix the
 // mixed path cannot handle: no approximate inverse converges (G singular or nearly so -- the
 // reference's own BiCGSTAB then returns what it returns), or GMRES misses the tolerance.  After a
@@ -1045,10 +1045,26 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         c.stats.last_rel_residual = rel;
     }
     c.stats.solves++;
-    // steps for the next solve from the observed contraction, and the refresh policy
+    // steps for the next solve from the observed contraction
     if (converged && rho > 0.0 && rel0 > tol)
         c.ir_steps = std::max(1, std::min(KMAX, (int)ceil(log(tol / rel0) / log(std::max(rho, 1e-6)))));
-    if (rc == BEM_OK && rho > 0.02) {
+    if (rc != BEM_OK) return rc;
+    // Refresh policy.  X drifts from G^-1 as the surface moves, and each solve then needs a few more
+    // refinement steps than right after a refresh.  A refresh (a Newton-Schulz step: two n^3 BF16x3
+    // GEMMs) costs about REFRESH_COST refinement steps (two n^2 GEMVs); it is taken once the extra
+    // steps paid since the last one add up to that cost (the rent-or-buy rule, within a factor two of
+    // the best schedule in hindsight), or at once when the contraction is too weak for refinement.
+    bool refresh = !converged || rho > 0.2;
+    if (!refresh) {
+        const int k = c.stats.last_iters;
+        if (c.ir_base < 0 || k < c.ir_base) c.ir_base = k;
+        c.ir_excess += k - c.ir_base;
+        const double refresh_cost = 2.0 + n / 100.0;  // GEMM pair vs GEMV pair, measured rates on B200
+        refresh = c.ir_excess > refresh_cost;
+    }
+    if (refresh) {
+        c.ir_base = -1;
+        c.ir_excess = 0;
         rc = refresh_inverse(c, A, s, false);
         if (rc == BEM_ERR_NOT_CONVERGED) {  // this solve stands; the next one starts over or falls back
             c.xinv_valid = false;

@@ -203,17 +203,28 @@ def test_negative_x_raises_like_reference():
 
 
 def test_mixed_solver_falls_back_on_singular_system():
-    # a bubble centred on the wall plane with the wall image on: G = S + S R annihilates the modes odd
-    # in x, so no approximate inverse exists.  The mixed solve hands over to the FP64 BiCGSTAB (the
-    # reference's solver, which returns its iterate there) instead of failing; Euler steps, as the
-    # reference's oscillations driver takes them (no x < 0 check).
+    # G with two equal columns (rank N - 1) and a consistent right-hand side: no approximate inverse
+    # exists, and the mixed solve hands over to the FP64 BiCGSTAB (the reference's solver) instead of
+    # failing
+    v, f = mesh.bubble(4, 1.0, (2.0, 0.0, 0.0))
+    sim = ColocSim(v, f, solver="mixed")
+    G, _ = sim.assemble_matrices()
+    G[:, 1] = G[:, 0]
+    b = G @ np.random.default_rng(2).standard_normal(len(v))
+    x = sim.solve_system(G, b)
+    assert sim.stats().fp64_fallbacks >= 1
+    assert np.linalg.norm(G @ x - b) <= 1e-8 * np.linalg.norm(b)
+
+
+def test_mixed_solver_steps_bubble_cut_by_its_wall_image():
+    # a bubble centred on the wall plane with the wall image on (the reference's oscillations driver
+    # as shipped): G = S + S R nearly annihilates the modes odd in x.  Euler steps (no x < 0 check, as
+    # in the reference) go through, on the mixed path or its FP64 fallback.
     v, f = mesh.bubble(4, 1.0, (0.0, 0.0, 0.0))
     sim = ColocSim(v, f, mirror=True, solver="mixed")
     sim.set_phi(0.05 + 0.01 * v[:, 2])
     for _ in range(3):
         sim.evolve_system(1e-3, fixdt=True)
-    st = sim.stats()
-    assert st.fp64_fallbacks >= 1
     assert np.all(np.isfinite(sim.get_vertices())) and np.all(np.isfinite(sim.get_phi()))
 
 
