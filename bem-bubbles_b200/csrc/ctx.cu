@@ -548,16 +548,17 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     CTX_GUARD(c);
     if (N < 3 || M < 1 || !verts || !trigs) return c->fail(BEM_ERR_ARG, "bad mesh arguments");
     if (N > (int64_t)1 << 20) return c->fail(BEM_ERR_ARG, "mesh too large for dense storage");
-    cudaStreamSynchronize(c->stream);
-    free_all(*c);
     HostTopo h;
     // column-group width: 16 (256 rows per CTA) unless BEM_ASM_CG selects 32 (128 rows) or 48 / 64 (64 rows)
     if (const char* e = getenv("BEM_ASM_CG")) {
         int v = atoi(e);
         if (v == 16 || v == 48 || v == 64 || v == 32) h.cg = v;
     }
+    // a rejected mesh leaves the current one in place
     int rc = build_topology(N, M, trigs, verts, h, c->err);
     if (rc) return rc;
+    cudaStreamSynchronize(c->stream);
+    free_all(*c);
     if ((rc = alloc_mesh(*c, N, M, h))) return rc;
     BEM_CUDA(*c, cudaMemcpy(c->x, verts, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
     c->have_mesh = true;
@@ -597,10 +598,6 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
             return c->fail(BEM_ERR_ARG, "triangle " + std::to_string(j) + " spans two blocks");
     }
     std::vector<int64_t> tr(trigs, trigs + 3 * M), voff(vert_off, vert_off + nblocks + 1);
-    cudaStreamSynchronize(c->stream);
-    const int keep_cg = c->batch_cg;
-    free_all(*c);
-    c->batch_cg = keep_cg;
     HostTopo h;
     if (c->batch_cg == 16 || c->batch_cg == 32 || c->batch_cg == 48 || c->batch_cg == 64) {
         h.cg = c->batch_cg;
@@ -608,8 +605,13 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
         int v = atoi(e);
         if (v == 16 || v == 48 || v == 64 || v == 32) h.cg = v;
     }
+    // a rejected batch leaves the current mesh in place
     int rc = build_topology(N, M, trigs, verts, h, c->err, voff);
     if (rc) return rc;
+    cudaStreamSynchronize(c->stream);
+    const int keep_cg = c->batch_cg;
+    free_all(*c);
+    c->batch_cg = keep_cg;
     Ctx& C = *c;
     C.batch = true;
     C.nblk = nblocks;
