@@ -21,11 +21,24 @@ namespace bemb {
 std::atomic<long long> g_kernel_launches{0};
 
 // ---------------------------------------------------------------- device memory helpers
-static void free_all(Ctx& c) {
+// Blocks kept for re-use that the new mesh did not take.
+static void release_reuse(Ctx& c) {
+    for (auto& blk : c.reuse)
+        if (blk.first) cudaFree(blk.first);
+    c.reuse.clear();
+    c.reuse_pos = 0;
+}
+
+// keep_blocks: the device allocations stay for the next mesh's buffers (see dalloc)
+static void free_all(Ctx& c, bool keep_blocks = false) {
     exporter_release(c);  // writes every queued file first
     if (c.graph_exec) cudaGraphExecDestroy(c.graph_exec);
     c.graph_exec = nullptr;
-    for (void* p : c.allocs) cudaFree(p);
+    release_reuse(c);
+    if (keep_blocks)
+        c.reuse = c.allocs;
+    else
+        for (auto& blk : c.allocs) cudaFree(blk.first);
     c.allocs.clear();
     c.bytes = 0;
     c.topo = Topology{};
@@ -558,8 +571,10 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     int rc = build_topology(N, M, trigs, verts, h, c->err);
     if (rc) return rc;
     cudaStreamSynchronize(c->stream);
-    free_all(*c);
-    if ((rc = alloc_mesh(*c, N, M, h))) return rc;
+    free_all(*c, true);
+    rc = alloc_mesh(*c, N, M, h);
+    release_reuse(*c);
+    if (rc) return rc;
     BEM_CUDA(*c, cudaMemcpy(c->x, verts, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
     c->have_mesh = true;
     // Simulation ctor: V_0 = volume(initial) (Simulation.hpp:42), time = 0
@@ -610,7 +625,7 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
     if (rc) return rc;
     cudaStreamSynchronize(c->stream);
     const int keep_cg = c->batch_cg;
-    free_all(*c);
+    free_all(*c, true);
     c->batch_cg = keep_cg;
     Ctx& C = *c;
     C.batch = true;
@@ -664,6 +679,7 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
         q[4] = C.prm.field_phase;
     }
     if ((rc = dalloc(C, &C.ppar, C.h_ppar.size())) || (rc = upload_ppar(C))) return rc;
+    release_reuse(C);
     prepare_assemble(C);
     BEM_CUDA(C, cudaGetLastError());
     return BEM_OK;

@@ -166,7 +166,12 @@ struct Ctx {
     }
 
     size_t bytes = 0;
-    std::vector<void*> allocs;
+    // device allocations of the current mesh, in allocation order, with their sizes
+    std::vector<std::pair<void*, size_t>> allocs;
+    // allocations of the previous mesh kept for re-use when the mesh changes (remeshing): the k-th
+    // allocation of the new mesh takes the k-th block of the old one if it is large enough
+    std::vector<std::pair<void*, size_t>> reuse;
+    size_t reuse_pos = 0;
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -174,17 +179,33 @@ struct Ctx {
     }
 };
 
-// Device allocation recorded in the context (freed together by free_all).
+// Device allocation recorded in the context (freed together by free_all).  When a mesh replaces
+// another, the allocations are made in the same order as before, so the k-th one re-uses the k-th
+// block of the previous mesh if it is large enough; a block that is too small is replaced by one with
+// 1/8 headroom, since a remeshed surface's vertex count moves by a few per cent either way.
 template <typename T>
 inline int dalloc(Ctx& c, T** p, size_t count) {
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    size_t bytes = count * sizeof(T);
+    if (c.reuse_pos < c.reuse.size()) {
+        const auto blk = c.reuse[c.reuse_pos];
+        c.reuse[c.reuse_pos++] = {nullptr, 0};
+        if (blk.second >= bytes) {
+            *p = (T*)blk.first;
+            c.allocs.push_back(blk);
+            c.bytes += blk.second;
+            return BEM_OK;
+        }
+        cudaFree(blk.first);
+        bytes += bytes / 8;
+    }
+    cudaError_t e = cudaMalloc((void**)p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
         return c.fail(BEM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
-    c.allocs.push_back((void*)*p);
-    c.bytes += count * sizeof(T);
+    c.allocs.push_back({(void*)*p, bytes});
+    c.bytes += bytes;
     return BEM_OK;
 }
 template <typename T>
