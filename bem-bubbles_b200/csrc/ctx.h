@@ -87,6 +87,8 @@ struct Ctx {
     double* V = nullptr;       // N*(m+1) Krylov basis
     double* Z = nullptr;       // N*m preconditioned directions
     double* hcol = nullptr;    // (m+2) Hessenberg column / dot results
+    double* pbicg = nullptr;   // persistent BiCGSTAB: per-row-block dots, barrier and error words
+    bool pbicg_ok = true;      // the persistent BiCGSTAB is usable (cleared after a failed launch or wait)
     bool xinv_valid = false;
     int mixed_backoff = 0;  // solves left that skip the mixed path after it failed (FP64 BiCGSTAB instead)
     int ir_base = -1;       // fewest refinement steps of a solve since the last refresh of X

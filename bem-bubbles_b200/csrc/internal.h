@@ -119,6 +119,10 @@ void launch_pin_zero(Ctx& c, const double* pot, double* potz, cudaStream_t s);
 void launch_pin_exchange(Ctx& c, const double* v, double* b, cudaStream_t s);
 void launch_pin_finish(Ctx& c, const double* x, double* vel, double* pot, cudaStream_t s);
 
+// bicg.cu
+int bicgstab_persistent(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+size_t pbicg_words(int64_t n);  // doubles of the persistent BiCGSTAB's dot and barrier scratch
+
 // remesh.cu
 int trace_mesh(Ctx& c, int64_t Nv, const double* verts, int64_t M, const int64_t* trigs, int64_t P, const double* pos,
                const double* dir, double* hit, int64_t* tri_out, int32_t* ok);

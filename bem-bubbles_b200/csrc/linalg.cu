@@ -302,6 +302,12 @@ __global__ void k_bicg_xr(int n, int nrb, DevScalars* sc, const double* __restri
 }
 
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    // one cooperative kernel per batch of iterations (bicg.cu); these launches are the fallback
+    if (!c.batch && c.pbicg_ok) {
+        const int rc = bicgstab_persistent(c, A, b, x, s);
+        if (rc == BEM_OK || rc == BEM_ERR_NOT_CONVERGED) return rc;
+        c.pbicg_ok = false;
+    }
     const int n = (int)c.topo.N;
     const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
     double* red = c.red;
