@@ -23,6 +23,7 @@ BEM_ERR_STATE = 7
 SOLVER_BICGSTAB = 0
 SOLVER_LU = 1
 SOLVER_MIXED = 2
+FLAG_BICGSTAB_MULTIKERNEL = 1
 
 _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)
@@ -34,7 +35,7 @@ class Params(C.Structure):
                 ("field_amp", C.c_double), ("field_kx", C.c_double), ("field_omega", C.c_double),
                 ("field_phase", C.c_double), ("min_dt", C.c_double), ("dp_balance", C.c_double),
                 ("nopen_eps", C.c_double), ("mirror", C.c_int32), ("solver", C.c_int32),
-                ("mixed_tol", C.c_double), ("max_iters", C.c_int32), ("reserved", C.c_int32)]
+                ("mixed_tol", C.c_double), ("max_iters", C.c_int32), ("flags", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -303,7 +303,7 @@ __global__ void k_bicg_xr(int n, int nrb, DevScalars* sc, const double* __restri
 
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     // one cooperative kernel per batch of iterations (bicg.cu); these launches are the fallback
-    if (!c.batch && c.pbicg_ok) {
+    if (!c.batch && c.pbicg_ok && !(c.prm.flags & BEM_FLAG_BICGSTAB_MULTIKERNEL)) {
         const int rc = bicgstab_persistent(c, A, b, x, s);
         if (rc == BEM_OK || rc == BEM_ERR_NOT_CONVERGED) return rc;
         c.pbicg_ok = false;

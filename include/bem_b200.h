@@ -61,8 +61,12 @@ typedef struct {
     int32_t solver;      /* bem_solver */
     double mixed_tol;    /* relative residual target of BEM_SOLVER_MIXED, default 1e-12 */
     int32_t max_iters;   /* iteration cap for the iterative solvers, 0 = reference default (2N) */
-    int32_t reserved;
+    int32_t flags;       /* BEM_FLAG_* bits, default 0 */
 } bem_params;
+
+/* bem_params.flags: run the FP64 BiCGSTAB as separate kernels per iteration instead of the persistent
+ * cooperative kernel (same iteration; for comparison, or where cooperative launches are unwanted). */
+#define BEM_FLAG_BICGSTAB_MULTIKERNEL 1
 
 /* Fill *p with the reference's defaults. */
 void bem_default_params(bem_params* p);

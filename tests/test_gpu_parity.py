@@ -202,6 +202,26 @@ def test_negative_x_raises_like_reference():
         sim.evolve_system_RK4(1e-3, fixdt=True)
 
 
+@pytest.mark.parametrize("nu", [4, 9, 16])
+def test_persistent_bicgstab_matches_multikernel_and_lu(nu):
+    # the cooperative-kernel BiCGSTAB and its multi-kernel form run the same iteration; both reach
+    # the machine-precision residual and agree with the FP64 LU solution
+    from bem_b200 import _lib as L
+    v, f = mesh.bubble(nu, 1.0, (2.0, 0.0, 0.0))
+    rng = np.random.default_rng(nu)
+    v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None]
+    phi = 0.1 * np.sin(3 * v[:, 2]) + 0.05 * v[:, 0]
+    _, psi_lu = ColocSim(v, f, solver="lu").position_t(phi, return_psi=True)
+    one = ColocSim(v, f, solver="bicgstab")
+    many = ColocSim(v, f, solver="bicgstab")
+    many._update(flags=L.FLAG_BICGSTAB_MULTIKERNEL)
+    for sim in (one, many):
+        _, psi = sim.position_t(phi, return_psi=True)
+        st = sim.stats()
+        assert rel(psi, psi_lu) <= TOL
+        assert st.last_rel_residual <= 1e-14 and 0 < st.last_iters <= 2 * len(v)
+
+
 def test_mixed_solver_falls_back_on_singular_system():
     # G with two equal columns (rank N - 1) and a consistent right-hand side: no approximate inverse
     # exists, and the mixed solve hands over to the FP64 BiCGSTAB (the reference's solver) instead of
