@@ -77,6 +77,8 @@ SIGNATURES = {
     "bem_solve_system": (C.c_int, [C.c_void_p, _D, _D, _D]),
     "bem_position_t": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "bem_position_t_inout": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
+    "bem_set_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
+    "bem_get_state": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "bem_set_pinned": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_double]),
     "bem_get_pinned": (C.c_int, [C.c_void_p, _I64]),
     "bem_trace_mesh": (C.c_int, [C.c_void_p, C.c_int64, _D, C.c_int64, _I64, C.c_int64, _D, _D, _D, _I64,

@@ -119,6 +119,24 @@ class ColocSim:
         a = np.ascontiguousarray(v, dtype=np.float64)
         self._check(self._L.bem_set_vertices(self._h, _d(a)))
 
+    def set_state(self, verts=None, phi=None, psi=None, time=None):
+        """Vertices, phi, psi and time in one call (None skips a part); the arrays are copied before
+        the call returns and the device copies are queued without a wait."""
+        arrs = []
+        for a, shape in ((verts, (self.N, 3)), (phi, (self.N,)), (psi, (self.N,))):
+            arrs.append(None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(shape))
+        t = None if time is None else np.array([float(time)])
+        self._check(self._L.bem_set_state(self._h, *[None if a is None else _d(a) for a in arrs],
+                                          None if t is None else _d(t)))
+
+    def get_state(self, out=None):
+        """(vertices, phi, psi, time) with one wait; `out` = (verts, phi, psi) arrays to fill."""
+        if out is None:
+            out = (np.empty((self.N, 3)), np.empty(self.N), np.empty(self.N))
+        t = np.zeros(1)
+        self._check(self._L.bem_get_state(self._h, _d(out[0]), _d(out[1]), _d(out[2]), _d(t)))
+        return out[0], out[1], out[2], float(t[0])
+
     def set_V_0(self, v):
         self._check(self._L.bem_set_V0(self._h, float(v)))
 

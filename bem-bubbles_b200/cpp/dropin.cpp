@@ -123,20 +123,14 @@ bem_ctx* Simulation::context(Mesh const& m) const {
 void Simulation::push_state() const {
     bem_ctx* c = context(mesh);
     std::vector<double> x = flat(mesh.verts);
-    check(bem_set_vertices(c, x.data()));
-    check(bem_set_phi(c, phi.data()));
-    check(bem_set_psi(c, psi.data()));
-    check(bem_set_time(c, time));
+    check(bem_set_state(c, x.data(), phi.data(), psi.data(), &time));
     check(bem_set_V0(c, V_0));
 }
 
 void Simulation::pull_state() {
     std::vector<double> x(3 * mesh.verts.size());
-    check(bem_get_vertices(ctx_, x.data()));
+    check(bem_get_state(ctx_, x.data(), phi.data(), psi.data(), &time));
     mesh.verts = unflat(x);
-    check(bem_get_phi(ctx_, phi.data()));
-    check(bem_get_psi(ctx_, psi.data()));
-    check(bem_get_time(ctx_, &time));
 }
 
 Eigen::VectorXd Simulation::solve_system(Eigen::MatrixXd const& G, Eigen::VectorXd const& H_phi) const {

@@ -351,8 +351,9 @@ static int check_negative(Ctx& c, cudaStream_t s) {
 }
 
 // One RK4 step on the device state (LinLinSim.cpp:194-257); no host synchronisation unless an
-// iterative solver polls, a field callback is set, or dt is adaptive and requested back.
-static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
+// iterative solver polls, a field callback is set, or dt is adaptive and requested back.  skip: a
+// device flag that, when set, keeps the final update from touching the state.
+static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* skip = nullptr) {
     const int64_t N = c.topo.N;
     BEM_CUDA(c, cudaMemcpyAsync(c.x1, c.x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemcpyAsync(c.p1, c.phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
@@ -376,7 +377,7 @@ static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s) {
     launch_axpy3(N, c.p1, dtp, 1.0, c.kp3, c.ps, s);
     if ((rc = position_t(c, c.xs, c.ps, c.k4, s))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k4, c.kp4, s))) return rc;
-    launch_rk4_final(c, s);
+    launch_rk4_final(c, s, skip);
     return BEM_OK;
 }
 
@@ -532,6 +533,8 @@ int bem_destroy(bem_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_all(*c);
     cudaFree(c->trace_buf);
+    cudaFreeHost(c->h_stage);
+    if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     cudaFree(c->sc);
     cudaFree(c->flag);
     cudaFreeHost(c->h_sc);
@@ -1062,8 +1065,8 @@ int bem_get_psi(bem_ctx* c, double* v) {
 }
 int bem_set_time(bem_ctx* c, double t) {
     CTX_GUARD(c);
-    KLAUNCH(), k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);
-    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    KLAUNCH(), k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);  // the value travels with the launch
+    BEM_CUDA(*c, cudaGetLastError());
     return BEM_OK;
 }
 int bem_get_time(bem_ctx* c, double* t) {
@@ -1074,7 +1077,70 @@ int bem_get_time(bem_ctx* c, double* t) {
 int bem_set_V0(bem_ctx* c, double v) {
     CTX_GUARD(c);
     KLAUNCH(), k_set_V0<<<1, 1, 0, c->stream>>>(c->sc, v);
-    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    BEM_CUDA(*c, cudaGetLastError());
+    return BEM_OK;
+}
+
+// Pinned host staging of the whole state (vertices, phi, psi): 5N doubles, grown on demand.  An
+// event marks the end of the last copy that read or wrote it.
+static int stage_buffer(Ctx& c) {
+    const size_t need = (size_t)5 * (size_t)c.topo.N;
+    if (!c.stage_ev) BEM_CUDA(c, cudaEventCreateWithFlags(&c.stage_ev, cudaEventDisableTiming));
+    BEM_CUDA(c, cudaEventSynchronize(c.stage_ev));  // the previous copies are done with the buffer
+    if (c.stage_cap < need) {
+        cudaFreeHost(c.h_stage);
+        c.h_stage = nullptr;
+        c.stage_cap = 0;
+        BEM_CUDA(c, cudaMallocHost(&c.h_stage, need * sizeof(double)));
+        c.stage_cap = need;
+    }
+    return BEM_OK;
+}
+
+int bem_set_state(bem_ctx* c, const double* verts, const double* phi, const double* psi, const double* time) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const size_t N = (size_t)c->topo.N;
+    int rc = stage_buffer(*c);
+    if (rc) return rc;
+    double* h = c->h_stage;
+    cudaStream_t s = c->stream;
+    // the caller's arrays are copied into the staging buffer before returning; the device copies
+    // run in stream order behind it
+    if (verts) {
+        memcpy(h, verts, 3 * N * sizeof(double));
+        BEM_CUDA(*c, cudaMemcpyAsync(c->x, h, 3 * N * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    if (phi) {
+        memcpy(h + 3 * N, phi, N * sizeof(double));
+        BEM_CUDA(*c, cudaMemcpyAsync(c->phi, h + 3 * N, N * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    if (psi) {
+        memcpy(h + 4 * N, psi, N * sizeof(double));
+        BEM_CUDA(*c, cudaMemcpyAsync(c->psi, h + 4 * N, N * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    if (time) KLAUNCH(), k_set_time<<<1, 1, 0, s>>>(c->sc, *time);
+    BEM_CUDA(*c, cudaEventRecord(c->stage_ev, s));
+    return BEM_OK;
+}
+
+int bem_get_state(bem_ctx* c, double* verts, double* phi, double* psi, double* time) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    const size_t N = (size_t)c->topo.N;
+    int rc = stage_buffer(*c);
+    if (rc) return rc;
+    double* h = c->h_stage;
+    cudaStream_t s = c->stream;
+    if (verts) BEM_CUDA(*c, cudaMemcpyAsync(h, c->x, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (phi) BEM_CUDA(*c, cudaMemcpyAsync(h + 3 * N, c->phi, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (psi) BEM_CUDA(*c, cudaMemcpyAsync(h + 4 * N, c->psi, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (time) BEM_CUDA(*c, cudaMemcpyAsync(time, &c->sc->time, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaEventRecord(c->stage_ev, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    if (verts) memcpy(verts, h, 3 * N * sizeof(double));
+    if (phi) memcpy(phi, h + 3 * N, N * sizeof(double));
+    if (psi) memcpy(psi, h + 4 * N, N * sizeof(double));
     return BEM_OK;
 }
 int bem_get_V0(bem_ctx* c, double* v) {
@@ -1221,12 +1287,25 @@ int bem_evolve_rk4(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
         if (dt_out) *dt_out = dp;
         return batch_steps(*c, dp, 1, false);
     }
-    int rc = check_negative(*c, c->stream);
-    if (rc) return rc;
-    if ((rc = rk4_step(*c, dp, fixdt != 0, c->stream))) return rc;
+    // test_negative before and after the step (LinLinSim.cpp:198, 256) with one host round trip: the
+    // check before the step sets flag[1], which keeps the step's final update from touching the state;
+    // flag[3] is the check after it; both are read with dt once the step is done.
+    cudaStream_t s = c->stream;
+    BEM_CUDA(*c, cudaMemsetAsync(c->flag + 1, 0, 3 * sizeof(int), s));
+    launch_any_negative(*c, c->x, c->flag + 1, s);
+    const int rc = rk4_step(*c, dp, fixdt != 0, s, c->flag + 1);
+    if (rc == BEM_OK) launch_any_negative(*c, c->x, c->flag + 3, s);
     BEM_CUDA(*c, cudaGetLastError());
-    if (dt_out) COPY_OUT(dt_out, &c->sc->dt, 1);
-    return check_negative(*c, c->stream);
+    int f[3] = {0, 0, 0};
+    double dt = 0.0;
+    BEM_CUDA(*c, cudaMemcpyAsync(f, c->flag + 1, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaMemcpyAsync(&dt, &c->sc->dt, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(*c, cudaStreamSynchronize(s));
+    if (f[0]) return c->fail(BEM_ERR_NEGATIVE_X, "negative values");  // state untouched, as the reference
+    if (rc) return rc;
+    if (dt_out) *dt_out = dt;
+    if (f[2]) return c->fail(BEM_ERR_NEGATIVE_X, "negative values");
+    return BEM_OK;
 }
 
 int bem_evolve_rk4_n(bem_ctx* c, double dt, int32_t steps) {

@@ -139,6 +139,11 @@ struct Ctx {
     double pin_beta = 0.0, pin_cos_eq = 0.0, pin_cnl = 0.0;
     double* potz = nullptr;  // N: stage potential with the pinned entries zeroed
 
+    // pinned host staging of bem_set_state / bem_get_state (5N doubles) and the event of its last use
+    double* h_stage = nullptr;
+    size_t stage_cap = 0;
+    cudaEvent_t stage_ev = nullptr;
+
     // remesh ray casting (remesh.cu): one device buffer, grown on demand, kept across meshes
     void* trace_buf = nullptr;
     size_t trace_cap = 0;

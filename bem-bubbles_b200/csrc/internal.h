@@ -107,7 +107,7 @@ void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* fiel
 void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s);
 void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k,
                   double* out, cudaStream_t s);
-void launch_rk4_final(Ctx& c, cudaStream_t s);
+void launch_rk4_final(Ctx& c, cudaStream_t s, const int* skip = nullptr);
 void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStream_t s);
 void launch_vertex_normals(Ctx& c, const double* x, double* out, cudaStream_t s);
 void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cudaStream_t s);

@@ -156,9 +156,9 @@ __global__ void k_rk4_final(int N, const double* __restrict__ x1, double* __rest
                             const double* __restrict__ q1, const double* __restrict__ q2,
                             const double* __restrict__ q3, const double* __restrict__ q4,
                             DevScalars* __restrict__ sc, double eps, double* __restrict__ x,
-                            double* __restrict__ phi) {
+                            double* __restrict__ phi, const int* __restrict__ skip) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+    if (i >= N || (skip && *skip)) return;
     const double dt = sc->dt;
     double av[3];
 #pragma unroll
@@ -190,7 +190,8 @@ __global__ void k_rk4_final(int N, const double* __restrict__ x1, double* __rest
 }
 
 __global__ void k_psi_from_avg(int N, const double* __restrict__ avg, const double* __restrict__ vn,
-                               double* __restrict__ psi, DevScalars* __restrict__ sc) {
+                               double* __restrict__ psi, DevScalars* __restrict__ sc, const int* __restrict__ skip) {
+    if (skip && *skip) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) sc->time += sc->dt;
     if (i >= N) return;
@@ -274,12 +275,13 @@ void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double sca
                   cudaStream_t s) {
     KLAUNCH(), k_axpy_dev<<<nb(n, 256), 256, 0, s>>>(n, a, coef_dev, scale, k, out);
 }
-void launch_rk4_final(Ctx& c, cudaStream_t s) {
+// skip (device flag, may be null): when set, the step leaves x, phi, psi and time untouched
+void launch_rk4_final(Ctx& c, cudaStream_t s, const int* skip) {
     const int N = (int)c.topo.N;
     KLAUNCH(), k_rk4_final<<<nb(N, 128), 128, 0, s>>>(N, c.x1, c.k1, c.k2, c.k3, c.k4, c.p1, c.kp1, c.kp2, c.kp3, c.kp4, c.sc,
-                                           c.prm.nopen_eps, c.x, c.phi);
+                                           c.prm.nopen_eps, c.x, c.phi, skip);
     launch_vertex_normals(c, c.x, c.vn, s);
-    KLAUNCH(), k_psi_from_avg<<<nb(N, 128), 128, 0, s>>>(N, c.k1, c.vn, c.psi, c.sc);
+    KLAUNCH(), k_psi_from_avg<<<nb(N, 128), 128, 0, s>>>(N, c.k1, c.vn, c.psi, c.sc, skip);
 }
 void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStream_t s) {
     const int N = (int)c.topo.N;

@@ -294,13 +294,9 @@ def run_ours(args):
         dist.barrier()
     tw0 = time.perf_counter()
     for _ in range(e2e_steps):
-        sim.set_vertices(hx)
-        sim.set_phi(hphi)
-        sim.set_psi(hpsi)
+        sim.set_state(hx, hphi, hpsi)
         sim.evolve_system_RK4(DT, fixdt=True)
-        hx[:] = sim.get_vertices()
-        hphi[:] = sim.get_phi()
-        hpsi[:] = sim.get_psi()
+        sim.get_state(out=(hx, hphi, hpsi))
     e2e_s = time.perf_counter() - tw0
     if dist:
         e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{device}")

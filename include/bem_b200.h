@@ -91,6 +91,11 @@ int bem_set_phi(bem_ctx* ctx, const double* phi);
 int bem_get_phi(bem_ctx* ctx, double* phi);
 int bem_set_psi(bem_ctx* ctx, const double* psi);
 int bem_get_psi(bem_ctx* ctx, double* psi);
+/* The whole state in one call each way (any pointer may be NULL to skip that part).  bem_set_state
+ * copies the arrays before returning and queues the device copies without waiting for them;
+ * bem_get_state waits once for all of them.  The per-array calls above each wait on their own. */
+int bem_set_state(bem_ctx* ctx, const double* verts, const double* phi, const double* psi, const double* time);
+int bem_get_state(bem_ctx* ctx, double* verts, double* phi, double* psi, double* time);
 /* set_time/get_time, set_V_0 (Simulation.hpp:106-126) */
 int bem_set_time(bem_ctx* ctx, double t);
 int bem_get_time(bem_ctx* ctx, double* t);

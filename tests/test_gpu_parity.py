@@ -248,6 +248,35 @@ def test_mixed_solver_steps_bubble_cut_by_its_wall_image():
     assert np.all(np.isfinite(sim.get_vertices())) and np.all(np.isfinite(sim.get_phi()))
 
 
+def test_state_in_one_call_each_way():
+    v, f = mesh.bubble(4, 1.0, (2.0, 0.0, 0.0))
+    sim = ColocSim(v, f)
+    rng = np.random.default_rng(1)
+    x = v + 0.01 * rng.standard_normal(v.shape)
+    phi, psi = rng.standard_normal(len(v)), rng.standard_normal(len(v))
+    sim.set_state(x, phi, psi, time=0.25)
+    gx, gp, gs, gt = sim.get_state()
+    assert np.array_equal(gx, x) and np.array_equal(gp, phi) and np.array_equal(gs, psi) and gt == 0.25
+    sim.set_state(phi=2 * phi)  # the other parts stay
+    gx, gp, gs, gt = sim.get_state()
+    assert np.array_equal(gx, x) and np.array_equal(gp, 2 * phi) and np.array_equal(gs, psi) and gt == 0.25
+    assert np.array_equal(sim.get_vertices(), x) and np.array_equal(sim.get_phi(), 2 * phi)
+
+
+def test_negative_x_leaves_the_state_untouched():
+    # the reference's test_negative throws before the step changes anything (LinLinSim.cpp:198)
+    v, f = mesh.bubble(3, 1.0, (2.0, 0.0, 0.0))
+    sim = ColocSim(v, f, solver="mixed")
+    x = v.copy()
+    x[5, 0] = -0.01
+    phi = 0.1 * v[:, 1]
+    sim.set_state(x, phi, np.zeros(len(v)), time=1.0)
+    with pytest.raises(IndexError):
+        sim.evolve_system_RK4(1e-3, fixdt=True)
+    gx, gp, gs, gt = sim.get_state()
+    assert np.array_equal(gx, x) and np.array_equal(gp, phi) and np.all(gs == 0.0) and gt == 1.0
+
+
 def test_mixed_precision_error_headline_size():
     # N = 4002 (config 2 mesh with the seeded 1% radial perturbation): psi of the mixed path
     # against the FP64 LU path at <= 1e-8 relative
