@@ -18,6 +18,7 @@
 #include <algorithm>
 
 #include "ctx.h"
+#include "grid_barrier.cuh"
 
 namespace bemb {
 
@@ -81,35 +82,7 @@ __device__ double dot_total(const PBArgs& a, int k) {
     return out;
 }
 
-// Grid-wide barrier with a bounded wait.  Returns false when any CTA's wait expired (the same answer
-// in every thread of the CTA).
-__device__ bool grid_sync(const PBArgs& a) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* gen = a.bar + 1;
-        const unsigned g = *gen;
-        __threadfence();
-        if (atomicAdd(a.bar, 1u) == gridDim.x - 1) {
-            atomicExch(a.bar, 0u);
-            __threadfence();
-            atomicAdd(a.bar + 1, 1u);
-        } else {
-            // poll without sleeping (the wait is a few microseconds), bounded by about a second of clock
-            const long long t0 = clock64();
-            while (*gen == g) {
-                if (clock64() - t0 > 2000000000LL) {
-                    atomicExch(a.err, 1);
-                    break;
-                }
-            }
-        }
-        __threadfence();
-        s_ok = *(volatile int*)a.err == 0;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
+__device__ __forceinline__ bool grid_sync(const PBArgs& a) { return grid_barrier(a.bar, a.err); }
 
 // out = A in (column-major A), tiles (row block, column split) spread over the CTAs; the last CTA
 // of a row block sums the splits in order, writes out and the row block's dots out.u0 -> dots[k0],

@@ -47,6 +47,7 @@ static void free_all(Ctx& c, bool keep_blocks = false) {
     // every pointer into the freed allocations
     c.G = c.H = c.LU = nullptr;
     c.pbicg = nullptr;
+    c.lu_aux = nullptr;
     c.Xinv = c.Tw = c.G32 = nullptr;
     c.tcp = nullptr;
     c.tc_err = nullptr;
@@ -450,7 +451,8 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = dalloc(c, &c.vol_part, (size_t)h.nparts * 64)) || (rc = dalloc(c, &c.vol_cnt, (size_t)h.nparts)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
-        (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)) || (rc = dalloc(c, &c.pbicg, pbicg_words(N))))
+        (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)) || (rc = dalloc(c, &c.pbicg, pbicg_words(N))) ||
+        (!c.batch && (rc = dalloc(c, &c.lu_aux, lu_panel_words()))))
         return rc;
     if (!c.batch && c.prm.solver == BEM_SOLVER_MIXED) {
         if ((rc = alloc_mixed(c))) return rc;

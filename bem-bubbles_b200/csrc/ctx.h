@@ -78,6 +78,8 @@ struct Ctx {
     // LU
     double* LU = nullptr;  // N*N
     int* piv = nullptr;    // N
+    double* lu_aux = nullptr;  // row-distributed panels: candidates, diagonal rows, barrier and error words
+    bool lu_rows_ok = true;    // the row-distributed panel is usable (cleared after a failed launch or wait)
     // mixed: approximate inverse (FP32), Krylov basis
     float* Xinv = nullptr;     // N*N column-major
     float* Tw = nullptr;       // N*N work for the Newton-Schulz refresh

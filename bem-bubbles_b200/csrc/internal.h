@@ -123,6 +123,11 @@ void launch_pin_finish(Ctx& c, const double* x, double* vel, double* pot, cudaSt
 int bicgstab_persistent(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 size_t pbicg_words(int64_t n);  // doubles of the persistent BiCGSTAB's dot and barrier scratch
 
+// lu_panel.cu
+int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s);
+size_t lu_panel_words();   // doubles of Ctx::lu_aux
+int* lu_panel_err(Ctx& c); // device error word of the row-distributed panels
+
 // remesh.cu
 int trace_mesh(Ctx& c, int64_t Nv, const double* verts, int64_t M, const int64_t* trigs, int64_t P, const double* pos,
                const double* dir, double* hit, int64_t* tri_out, int32_t* ok);

@@ -541,15 +541,19 @@ __global__ void __launch_bounds__(1024) k_lu_substitute(int n, const double* __r
     for (int i = tid; i < n; i += blockDim.x) x[i] = sx[i];
 }
 
-int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+// Blocked right-looking factorisation of c.LU (a copy of A).  rows: panels spread over the SMs
+// (lu_panel.cu); otherwise the single-CTA panel.
+static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
     const int n = (int)c.topo.N;
-    if ((size_t)n * sizeof(double) > 200 * 1024)
-        return c.fail(BEM_ERR_ARG, "LU solver: N too large for the single-CTA substitution (N <= 25600)");
     BEM_CUDA(c, cudaMemcpyAsync(c.LU, A, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemsetAsync(c.flag, 0, sizeof(int), s));
+    if (rows) BEM_CUDA(c, cudaMemsetAsync(lu_panel_err(c), 0, sizeof(int), s));
     for (int k0 = 0; k0 < n; k0 += LU_NB) {
         const int nb = std::min(LU_NB, n - k0);
-        KLAUNCH(), k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
+        if (!rows || lu_panel_rows(c, k0, nb, s) != BEM_OK) {
+            if (rows) return BEM_ERR_CUDA;
+            KLAUNCH(), k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
+        }
         KLAUNCH(), k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
         const int rest = n - k0 - nb;
         if (rest > 0) {
@@ -557,6 +561,28 @@ int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
             dim3 g((rest + 63) / 64, (rest + 63) / 64);
             KLAUNCH(), k_lu_gemm<<<g, 256, 0, s>>>(n, k0, nb, c.LU);
         }
+    }
+    if (rows) {
+        int err = 0;
+        BEM_CUDA(c, cudaMemcpyAsync(&err, lu_panel_err(c), sizeof(int), cudaMemcpyDeviceToHost, s));
+        BEM_CUDA(c, cudaStreamSynchronize(s));
+        if (err) return BEM_ERR_CUDA;
+    }
+    return BEM_OK;
+}
+
+int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    if ((size_t)n * sizeof(double) > 200 * 1024)
+        return c.fail(BEM_ERR_ARG, "LU solver: N too large for the single-CTA substitution (N <= 25600)");
+    int rc = BEM_ERR_CUDA;
+    if (c.lu_rows_ok && c.lu_aux) {
+        rc = lu_factor(c, A, s, true);
+        if (rc == BEM_ERR_CUDA) c.lu_rows_ok = false;  // factor again with the single-CTA panel
+    }
+    if (rc != BEM_OK) {
+        rc = lu_factor(c, A, s, false);
+        if (rc) return rc;
     }
     size_t sm = sizeof(double) * (size_t)n;
     static std::atomic<uint64_t> attr{0};
