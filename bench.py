@@ -186,6 +186,69 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class NvmlClockSampler:
+    """NVML sampling of the SM clock and the clock-event reasons every 2 ms (read-only queries), for
+    timed regions too short for nvidia-smi's interval; same summary as ClockSampler."""
+
+    PERIOD_S = 0.002
+
+    def __init__(self, index):
+        import pynvml
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(int(index))
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.samples = []
+        self.stop = threading.Event()
+        self.begin = self.end = 0
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                mask = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((mhz, mask))
+            except nv.NVMLError:
+                pass
+            time.sleep(self.PERIOD_S)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 3.0:
+            time.sleep(0.001)
+        self.begin = len(self.samples)
+        return self
+
+    def __exit__(self, *a):
+        self.end = len(self.samples)
+        self.stop.set()
+        self.t.join(timeout=1.0)
+
+    def summary(self):
+        nv = self.nv
+        w = self.samples[self.begin:self.end] or self.samples[max(0, self.begin - 1):self.begin]
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted({k for _, m in w for k, b in bits.items() if m & b})
+        sm = [mhz for mhz, _ in w]
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "source": "nvml"}
+
+
+def clock_sampler(index):
+    """NVML sampler when the bindings are present, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(index)
+    except Exception:
+        return ClockSampler(index)
+
+
 def cpu_reference_stages(stages, threads, timeout=900):
     """Seconds of each of `stages` RK4 stages of the reference's own code (oracle/_ref)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -266,7 +329,7 @@ def run_ours(args):
     torch.cuda.synchronize(device)
     sim.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(device) as clk:
+    with clock_sampler(device) as clk:
         torch.cuda.nvtx.range_push("timed_region")
         e0.record(ext)
         sim.evolve_rk4_steps(DT, args.steps)
@@ -408,7 +471,7 @@ def run_pair(args):
     for _ in range(args.warmup):
         sim.evolve_rk4_steps(dt, 1)
     st0 = sim.stats()
-    with ClockSampler(device) as clk:
+    with clock_sampler(device) as clk:
         _, el = timed(lambda: sim.evolve_rk4_steps(dt, args.steps))
     st1 = sim.stats()
 
@@ -488,7 +551,7 @@ def run_sweep(args):
         bb.evolve_graph(dt, 1)
     st0 = bb.stats()
     bb.reset_profile()
-    with ClockSampler(device) as clk:
+    with clock_sampler(device) as clk:
         el = timed(lambda: bb.evolve_graph(dt, args.steps))
     launches = int(bb.profile().kernel_launches)
     st1 = bb.stats()
