@@ -125,6 +125,8 @@ size_t pbicg_words(int64_t n);  // doubles of the persistent BiCGSTAB's dot and 
 
 // lu_panel.cu
 int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s);
+int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s);
+void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s);  // the panel's interchanges, other columns
 size_t lu_panel_words();   // doubles of Ctx::lu_aux
 int* lu_panel_err(Ctx& c); // device error word of the row-distributed panels
 

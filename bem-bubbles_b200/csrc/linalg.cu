@@ -541,8 +541,9 @@ __global__ void __launch_bounds__(1024) k_lu_substitute(int n, const double* __r
     for (int i = tid; i < n; i += blockDim.x) x[i] = sx[i];
 }
 
-// Blocked right-looking factorisation of c.LU (a copy of A).  rows: panels spread over the SMs
-// (lu_panel.cu); otherwise the single-CTA panel.
+// Blocked right-looking factorisation of c.LU (a copy of A).  rows: each panel on one thread-block
+// cluster when its rows fit in the cluster's shared memory, else spread over the SMs with grid
+// barriers (lu_panel.cu); otherwise the single-CTA panel.
 static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
     const int n = (int)c.topo.N;
     BEM_CUDA(c, cudaMemcpyAsync(c.LU, A, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s));
@@ -550,11 +551,14 @@ static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
     if (rows) BEM_CUDA(c, cudaMemsetAsync(lu_panel_err(c), 0, sizeof(int), s));
     for (int k0 = 0; k0 < n; k0 += LU_NB) {
         const int nb = std::min(LU_NB, n - k0);
-        if (!rows || lu_panel_rows(c, k0, nb, s) != BEM_OK) {
+        if (!rows || (lu_panel_cluster(c, k0, nb, s) != BEM_OK && lu_panel_rows(c, k0, nb, s) != BEM_OK)) {
             if (rows) return BEM_ERR_CUDA;
             KLAUNCH(), k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
         }
-        KLAUNCH(), k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
+        if (c.lu_aux)
+            lu_panel_swap_rest(c, k0, nb, s);
+        else
+            KLAUNCH(), k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
         const int rest = n - k0 - nb;
         if (rest > 0) {
             KLAUNCH(), k_lu_trsm<<<(rest + 7) / 8, 256, 0, s>>>(n, k0, nb, c.LU);
