@@ -505,40 +505,96 @@ __global__ void __launch_bounds__(256) k_lu_gemm(int n, int k0, int nb, double* 
     }
 }
 
-// x = P b (the recorded interchanges in order), then L y = x (unit lower), U x = y; one CTA,
-// x kept in shared memory when it fits.
-__global__ void __launch_bounds__(1024) k_lu_substitute(int n, const double* __restrict__ A,
-                                                        const int* __restrict__ piv, const double* __restrict__ b,
-                                                        double* __restrict__ x) {
-    extern __shared__ double sx[];
-    const int tid = threadIdx.x;
-    for (int i = tid; i < n; i += blockDim.x) sx[i] = b[i];
+// Triangular solves of the factored system (x = P b, L y = x with unit L, U x = y) in blocks of TS_B
+// columns, with the operations of the column-oriented substitution in the same order per element:
+// each row subtracts the contributions of the columns in increasing order going forward and in
+// decreasing order going back.  A small kernel solves the block's diagonal part; a row-parallel
+// kernel subtracts the block's columns from the other rows.
+constexpr int TS_B = 64;
+
+// y = P b: the recorded interchanges in order (one CTA, the vector in shared memory)
+__global__ void __launch_bounds__(1024) k_lu_permute(int n, const int* __restrict__ piv, const double* __restrict__ b,
+                                                     double* __restrict__ y) {
+    extern __shared__ double sy[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sy[i] = b[i];
     __syncthreads();
-    if (tid == 0)
+    if (threadIdx.x == 0)
         for (int j = 0; j < n; ++j) {
-            int p = piv[j];
+            const int p = piv[j];
             if (p != j) {
-                double t = sx[j];
-                sx[j] = sx[p];
-                sx[p] = t;
+                const double t = sy[j];
+                sy[j] = sy[p];
+                sy[p] = t;
             }
         }
     __syncthreads();
-    for (int j = 0; j < n; ++j) {
-        const double xj = sx[j];
-        if (xj != 0.0)
-            for (int i = j + 1 + tid; i < n; i += blockDim.x) sx[i] -= A[(size_t)j * n + i] * xj;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = sy[i];
+}
+
+// forward: unit lower L on rows [k0, k1)
+__global__ void k_trsv_fwd_diag(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
+    __shared__ double s[TS_B];
+    const int t = threadIdx.x, i = k0 + t;
+    if (i < k1) s[t] = y[i];
+    for (int j = k0; j < k1; ++j) {
         __syncthreads();
+        const double xj = s[j - k0];
+        if (i > j && i < k1) s[t] -= A[(size_t)j * n + i] * xj;
     }
-    for (int j = n - 1; j >= 0; --j) {
-        if (tid == 0) sx[j] /= A[(size_t)j * n + j];
+    __syncthreads();
+    if (i < k1) y[i] = s[t];
+}
+__global__ void k_trsv_fwd_rest(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
+    __shared__ double xs[TS_B];
+    if (threadIdx.x < k1 - k0) xs[threadIdx.x] = y[k0 + threadIdx.x];
+    __syncthreads();
+    const int i = k1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = y[i];
+    for (int j = k0; j < k1; ++j) acc -= A[(size_t)j * n + i] * xs[j - k0];
+    y[i] = acc;
+}
+// backward: upper U on rows [k0, k1), columns from the last
+__global__ void k_trsv_bwd_diag(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
+    __shared__ double s[TS_B];
+    const int t = threadIdx.x, i = k0 + t;
+    if (i < k1) s[t] = y[i];
+    for (int j = k1 - 1; j >= k0; --j) {
         __syncthreads();
-        const double xj = sx[j];
-        if (xj != 0.0)
-            for (int i = tid; i < j; i += blockDim.x) sx[i] -= A[(size_t)j * n + i] * xj;
+        if (i == j) s[t] /= A[(size_t)j * n + j];
         __syncthreads();
+        const double xj = s[j - k0];
+        if (i < j) s[t] -= A[(size_t)j * n + i] * xj;
     }
-    for (int i = tid; i < n; i += blockDim.x) x[i] = sx[i];
+    __syncthreads();
+    if (i < k1) y[i] = s[t];
+}
+__global__ void k_trsv_bwd_rest(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
+    __shared__ double xs[TS_B];
+    if (threadIdx.x < k1 - k0) xs[threadIdx.x] = y[k0 + threadIdx.x];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k0) return;
+    double acc = y[i];
+    for (int j = k1 - 1; j >= k0; --j) acc -= A[(size_t)j * n + i] * xs[j - k0];
+    y[i] = acc;
+}
+
+static void lu_substitute_blocked(Ctx& c, const double* b, double* x, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    static std::atomic<uint64_t> attr{0};
+    if (first_on_device(attr)) cudaFuncSetAttribute(k_lu_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    KLAUNCH(), k_lu_permute<<<1, 1024, sizeof(double) * (size_t)n, s>>>(n, c.piv, b, x);
+    for (int k0 = 0; k0 < n; k0 += TS_B) {
+        const int k1 = std::min(n, k0 + TS_B);
+        KLAUNCH(), k_trsv_fwd_diag<<<1, TS_B, 0, s>>>(n, k0, k1, c.LU, x);
+        if (k1 < n) KLAUNCH(), k_trsv_fwd_rest<<<(n - k1 + 255) / 256, 256, 0, s>>>(n, k0, k1, c.LU, x);
+    }
+    for (int k1 = n; k1 > 0; k1 -= TS_B) {
+        const int k0 = std::max(0, k1 - TS_B);
+        KLAUNCH(), k_trsv_bwd_diag<<<1, TS_B, 0, s>>>(n, k0, k1, c.LU, x);
+        if (k0 > 0) KLAUNCH(), k_trsv_bwd_rest<<<(k0 + 255) / 256, 256, 0, s>>>(n, k0, k1, c.LU, x);
+    }
 }
 
 // Blocked right-looking factorisation of c.LU (a copy of A).  rows: each panel on one thread-block
@@ -578,7 +634,7 @@ static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
 int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
     if ((size_t)n * sizeof(double) > 200 * 1024)
-        return c.fail(BEM_ERR_ARG, "LU solver: N too large for the single-CTA substitution (N <= 25600)");
+        return c.fail(BEM_ERR_ARG, "LU solver: N too large for the in-shared-memory interchange of b (N <= 25600)");
     int rc = BEM_ERR_CUDA;
     if (c.lu_rows_ok && c.lu_aux) {
         rc = lu_factor(c, A, s, true);
@@ -588,10 +644,7 @@ int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
         rc = lu_factor(c, A, s, false);
         if (rc) return rc;
     }
-    size_t sm = sizeof(double) * (size_t)n;
-    static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr)) cudaFuncSetAttribute(k_lu_substitute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    KLAUNCH(), k_lu_substitute<<<1, 1024, sm, s>>>(n, c.LU, c.piv, b, x);
+    lu_substitute_blocked(c, b, x, s);
     int sing = 0;
     BEM_CUDA(c, cudaMemcpyAsync(&sing, c.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));
