@@ -153,3 +153,20 @@ def test_pins_refused_where_unsupported():
         sp._check(sp._L.bem_adjoint_record(sp._h, 1e-3, 1))
     with pytest.raises(Exception):
         sp._check(sp._L.bem_set_pinned(sp._h, sp.N, *sp.drift))
+    # batches of independent bubbles take no pins
+    from bem_b200.batch import BubbleBatch
+    bb = BubbleBatch([mesh.bubble(3, 1.0, (2.0, 0.0, 0.0)), mesh.bubble(2, 0.5, (1.5, 0.0, 0.0))])
+    assert bb._L.bem_set_pinned(bb._h, 2, *sp.drift) != 0
+
+
+def test_new_mesh_clears_the_pins():
+    # bem_set_mesh starts without pinned vertices (the pinned count refers to a vertex order)
+    import ctypes as C
+    from bem_b200 import _lib as L
+    sp = pinned_sim(3)
+    v, f = wall_cap32(3)
+    vv, ff = np.ascontiguousarray(v), np.ascontiguousarray(f, dtype=np.int64)
+    sp._check(sp._L.bem_set_mesh(sp._h, len(vv), vv.ctypes.data_as(L._D), len(ff), ff.ctypes.data_as(L._I64)))
+    n = C.c_int64(-1)
+    sp._check(sp._L.bem_get_pinned(sp._h, C.byref(n)))
+    assert n.value == 0
