@@ -24,6 +24,7 @@ SOLVER_BICGSTAB = 0
 SOLVER_LU = 1
 SOLVER_MIXED = 2
 FLAG_BICGSTAB_MULTIKERNEL = 1
+FLAG_NO_STAGE_PREDICTOR = 2
 
 _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)
@@ -41,7 +42,8 @@ class Params(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("solves", C.c_int64), ("last_iters", C.c_int32), ("precond_refresh", C.c_int32),
                 ("last_rel_residual", C.c_double), ("ns_steps", C.c_int64), ("gmres_fallbacks", C.c_int64),
-                ("fp64_fallbacks", C.c_int64)]
+                ("fp64_fallbacks", C.c_int64),
+                ("total_iters", C.c_int64)]
 
 
 class Profile(C.Structure):

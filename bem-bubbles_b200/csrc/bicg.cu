@@ -363,6 +363,7 @@ int bicgstab_persistent(Ctx& c, const double* A, const double* b, double* x, cud
     }
     c.stats.last_iters = c.h_sc->iters;
     c.stats.last_rel_residual = c.h_sc->rhs_sq > 0 ? sqrt(c.h_sc->rr / c.h_sc->rhs_sq) : 0.0;
+    c.stats.total_iters += c.stats.last_iters;
     c.stats.solves++;
     return BEM_OK;
 }

@@ -81,6 +81,8 @@ static void free_all(Ctx& c, bool keep_blocks = false) {
     c.adj = AdjWork{};
     c.n_pin = 0;
     c.potz = nullptr;
+    c.psih = c.psih_t = nullptr;
+    c.pred_head = 0;
     c.mixed_backoff = 0;
     c.ir_base = -1;
     c.ir_excess = 0;
@@ -305,10 +307,14 @@ static void assemble_system(Ctx& c, const double* x, const double* pot, const do
 // (ColocSimPin.cpp:139-194): the stored psi stands in for pot at the pinned vertices, the pinned
 // vertices take the drift velocity, and pot receives the solved potential there (pot is in/out, as
 // the reference's PotVec& argument).
-static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStream_t s) {
+// stage >= 0: an RK4 stage of the mixed solver's step loop, whose start value comes from the stage
+// predictor and whose solution goes into its history.
+static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStream_t s, int stage = -1) {
     assemble_system(c, x, pot, c.psi, s);
+    if (stage >= 0) launch_stage_predict(c, stage, c.psil, s);
     int rc = solve(c, c.G, c.b, c.psil, s);
     if (rc) return rc;
+    if (stage >= 0) launch_stage_store(c, stage, c.psil, s);
     launch_velocity_prep(c, x, pot, s);
     launch_velocity(c, c.psil, vel, s);
     if (c.n_pin) launch_pin_finish(c, x, vel, pot, s);
@@ -351,14 +357,40 @@ static int check_negative(Ctx& c, cudaStream_t s) {
     return BEM_OK;
 }
 
+static int rk4_stages(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* skip, int st1, int st2, int st3,
+                      int st4);
+
+// The stage predictor's history no longer continues the state (set from outside, or a failed step).
+static void pred_reset(Ctx& c, cudaStream_t s) {
+    if (c.psih_t) cudaMemsetAsync(c.psih_t + PRED_CNT, 0, sizeof(double), s);
+}
+
 // One RK4 step on the device state (LinLinSim.cpp:194-257); no host synchronisation unless an
 // iterative solver polls, a field callback is set, or dt is adaptive and requested back.  skip: a
 // device flag that, when set, keeps the final update from touching the state.
 static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* skip = nullptr) {
+    // the stage predictor serves the mixed solver of a single system (not a batch, whose steps are
+    // captured in a graph, nor the reference's FP64 solvers, which keep their own start values)
+    const bool pred = !c.batch && c.prm.solver == BEM_SOLVER_MIXED && c.psih &&
+                      !(c.prm.flags & BEM_FLAG_NO_STAGE_PREDICTOR);
+    if (!pred) pred_reset(c, s);
+    const int st1 = pred ? 0 : -1, st2 = pred ? 1 : -1, st3 = pred ? 2 : -1, st4 = pred ? 3 : -1;
+    int rc = rk4_stages(c, dp, fixdt, s, skip, st1, st2, st3, st4);
+    if (rc) {
+        pred_reset(c, s);
+        return rc;
+    }
+    if (pred) launch_stage_advance(c, skip, s);
+    return BEM_OK;
+}
+
+// The four stages and the final update; st1..st4: predictor stage indices, or -1 without it.
+static int rk4_stages(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* skip, int st1, int st2, int st3,
+                      int st4) {
     const int64_t N = c.topo.N;
     BEM_CUDA(c, cudaMemcpyAsync(c.x1, c.x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemcpyAsync(c.p1, c.phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-    int rc = position_t(c, c.x1, c.p1, c.k1, s);
+    int rc = position_t(c, c.x1, c.p1, c.k1, s, st1);
     if (rc) return rc;
     if ((rc = pot_t_multi(c, c.x1, c.k1, c.kp1, s))) return rc;
     if (fixdt)
@@ -368,15 +400,15 @@ static int rk4_step(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* sk
     const double* dtp = &c.sc->dt;
     launch_axpy3(3 * N, c.x1, dtp, 0.5, c.k1, c.xs, s);
     launch_axpy3(N, c.p1, dtp, 0.5, c.kp1, c.ps, s);
-    if ((rc = position_t(c, c.xs, c.ps, c.k2, s))) return rc;
+    if ((rc = position_t(c, c.xs, c.ps, c.k2, s, st2))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k2, c.kp2, s))) return rc;
     launch_axpy3(3 * N, c.x1, dtp, 0.5, c.k2, c.xs, s);
     launch_axpy3(N, c.p1, dtp, 0.5, c.kp2, c.ps, s);
-    if ((rc = position_t(c, c.xs, c.ps, c.k3, s))) return rc;
+    if ((rc = position_t(c, c.xs, c.ps, c.k3, s, st3))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k3, c.kp3, s))) return rc;
     launch_axpy3(3 * N, c.x1, dtp, 1.0, c.k3, c.xs, s);
     launch_axpy3(N, c.p1, dtp, 1.0, c.kp3, c.ps, s);
-    if ((rc = position_t(c, c.xs, c.ps, c.k4, s))) return rc;
+    if ((rc = position_t(c, c.xs, c.ps, c.k4, s, st4))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k4, c.kp4, s))) return rc;
     launch_rk4_final(c, s, skip);
     return BEM_OK;
@@ -452,8 +484,11 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)) || (rc = dalloc(c, &c.pbicg, pbicg_words(N))) ||
-        (!c.batch && (rc = dalloc(c, &c.lu_aux, lu_panel_words()))))
+        (!c.batch && (rc = dalloc(c, &c.lu_aux, lu_panel_words()))) ||
+        (!c.batch && (rc = dalloc(c, &c.psih, (size_t)PRED_DEPTH * 4 * n))) ||
+        (!c.batch && (rc = dalloc(c, &c.psih_t, (size_t)PRED_CNT + 1))))
         return rc;
+    if (c.psih_t) BEM_CUDA(c, cudaMemset(c.psih_t, 0, sizeof(double) * (PRED_CNT + 1)));
     if (!c.batch && c.prm.solver == BEM_SOLVER_MIXED) {
         if ((rc = alloc_mixed(c))) return rc;
     }
@@ -540,6 +575,7 @@ int bem_destroy(bem_ctx* c) {
     cudaFree(c->sc);
     cudaFree(c->flag);
     cudaFreeHost(c->h_sc);
+    cudaFreeHost(c->h_red);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return BEM_OK;
@@ -553,6 +589,7 @@ int bem_set_params(bem_ctx* c, const bem_params* p) {
     const bool to_mixed = p->solver == BEM_SOLVER_MIXED && c->prm.solver != BEM_SOLVER_MIXED;
     if (p->mirror != c->prm.mirror) c->xinv_valid = false;
     c->prm = *p;
+    pred_reset(*c, c->stream);
     if (to_mixed) return ensure_mixed_buffers(*c);
     return BEM_OK;
 }
@@ -993,8 +1030,10 @@ int bem_set_state_device(bem_ctx* c, const double* x, const double* phi) {
     NEED_MESH(c);
     const int64_t N = c->topo.N;
     cudaStream_t s = c->stream;
-    if (x) BEM_CUDA(*c, cudaMemcpyAsync(c->x, x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
-    if (phi) BEM_CUDA(*c, cudaMemcpyAsync(c->phi, phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    // copies that keep the stage predictor's history when the state is the one held
+    if (x) launch_state_accept(*c, 3 * N, x, c->x, s);
+    if (phi) launch_state_accept(*c, N, phi, c->phi, s);
+    BEM_CUDA(*c, cudaGetLastError());
     BEM_CUDA(*c, cudaStreamSynchronize(s));
     return BEM_OK;
 }
@@ -1032,6 +1071,7 @@ int bem_num_verts(const bem_ctx* c, int64_t* n) {
 int bem_set_vertices(bem_ctx* c, const double* v) {
     CTX_GUARD(c);
     NEED_MESH(c);
+    pred_reset(*c, c->stream);
     COPY_IN(c->x, v, 3 * c->topo.N);
     return BEM_OK;
 }
@@ -1044,6 +1084,7 @@ int bem_get_vertices(bem_ctx* c, double* v) {
 int bem_set_phi(bem_ctx* c, const double* v) {
     CTX_GUARD(c);
     NEED_MESH(c);
+    pred_reset(*c, c->stream);
     COPY_IN(c->phi, v, c->topo.N);
     return BEM_OK;
 }
@@ -1056,6 +1097,7 @@ int bem_get_phi(bem_ctx* c, double* v) {
 int bem_set_psi(bem_ctx* c, const double* v) {
     CTX_GUARD(c);
     NEED_MESH(c);
+    pred_reset(*c, c->stream);
     COPY_IN(c->psi, v, c->topo.N);
     return BEM_OK;
 }
@@ -1067,6 +1109,7 @@ int bem_get_psi(bem_ctx* c, double* v) {
 }
 int bem_set_time(bem_ctx* c, double t) {
     CTX_GUARD(c);
+    pred_reset(*c, c->stream);
     KLAUNCH(), k_set_time<<<1, 1, 0, c->stream>>>(c->sc, t);  // the value travels with the launch
     BEM_CUDA(*c, cudaGetLastError());
     return BEM_OK;
@@ -1107,21 +1150,26 @@ int bem_set_state(bem_ctx* c, const double* verts, const double* phi, const doub
     if (rc) return rc;
     double* h = c->h_stage;
     cudaStream_t s = c->stream;
-    // the caller's arrays are copied into the staging buffer before returning; the device copies
-    // run in stream order behind it
+    // The caller's arrays are copied into the staging buffer before returning; the device copies run
+    // in stream order behind it.  They land in the stage scratch (x1, p1, kp1, free between steps) and
+    // are accepted from there: a state equal to the one held (a caller that pushes back what it
+    // read) keeps the stage predictor's history.
     if (verts) {
         memcpy(h, verts, 3 * N * sizeof(double));
-        BEM_CUDA(*c, cudaMemcpyAsync(c->x, h, 3 * N * sizeof(double), cudaMemcpyHostToDevice, s));
+        BEM_CUDA(*c, cudaMemcpyAsync(c->x1, h, 3 * N * sizeof(double), cudaMemcpyHostToDevice, s));
+        launch_state_accept(*c, 3 * N, c->x1, c->x, s);
     }
     if (phi) {
         memcpy(h + 3 * N, phi, N * sizeof(double));
-        BEM_CUDA(*c, cudaMemcpyAsync(c->phi, h + 3 * N, N * sizeof(double), cudaMemcpyHostToDevice, s));
+        BEM_CUDA(*c, cudaMemcpyAsync(c->p1, h + 3 * N, N * sizeof(double), cudaMemcpyHostToDevice, s));
+        launch_state_accept(*c, N, c->p1, c->phi, s);
     }
     if (psi) {
         memcpy(h + 4 * N, psi, N * sizeof(double));
-        BEM_CUDA(*c, cudaMemcpyAsync(c->psi, h + 4 * N, N * sizeof(double), cudaMemcpyHostToDevice, s));
+        BEM_CUDA(*c, cudaMemcpyAsync(c->kp1, h + 4 * N, N * sizeof(double), cudaMemcpyHostToDevice, s));
+        launch_state_accept(*c, N, c->kp1, c->psi, s);
     }
-    if (time) KLAUNCH(), k_set_time<<<1, 1, 0, s>>>(c->sc, *time);
+    if (time) launch_time_accept(*c, *time, s);
     BEM_CUDA(*c, cudaEventRecord(c->stage_ev, s));
     return BEM_OK;
 }
@@ -1236,6 +1284,7 @@ int bem_set_pinned(bem_ctx* c, int64_t n_pin, double beta, double costheta_eq, d
     if (n_pin > 0 && c->batch) return c->fail(BEM_ERR_STATE, "pinned vertices: single systems only");
     if (n_pin != c->n_pin) c->xinv_valid = false;  // the exchanged system is another matrix
     c->n_pin = n_pin;
+    pred_reset(*c, c->stream);
     c->pin_beta = beta;
     c->pin_cos_eq = costheta_eq;
     c->pin_cnl = c_nonlinear;
@@ -1326,6 +1375,7 @@ int bem_evolve_euler(bem_ctx* c, double dp, int32_t fixdt, double* dt_out) {
     CTX_GUARD(c);
     NEED_MESH(c);
     if (c->batch) return c->fail(BEM_ERR_STATE, "batches step with RK4 at a fixed dt");
+    pred_reset(*c, c->stream);  // the stage predictor's history holds RK4 stages
     int rc = euler_step(*c, dp, fixdt != 0, c->stream);
     if (rc) return rc;
     BEM_CUDA(*c, cudaGetLastError());

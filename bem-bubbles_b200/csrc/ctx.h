@@ -45,6 +45,8 @@ struct Ctx {
     double* psi = nullptr;  // N
     DevScalars* sc = nullptr;
     DevScalars* h_sc = nullptr;  // pinned mirror
+    double* h_red = nullptr;     // pinned host copy of the mixed solve's residual-norm partials
+    size_t h_red_cap = 0;        // its capacity in doubles
 
     // ---- per-stage work
     double* G = nullptr;       // N*N column-major
@@ -96,6 +98,14 @@ struct Ctx {
     int ir_base = -1;       // fewest refinement steps of a solve since the last refresh of X
     int ir_excess = 0;      // refinement steps paid above ir_base since the last refresh
     int ir_steps = 3;  // refinement steps issued per round of the mixed solve (adapted)
+    // Stage predictor of the mixed solve (single systems): the solutions of the RK4 stages of the last
+    // PRED_DEPTH steps and the stage times, a ring over steps (pred_head: the slot the current step
+    // writes, which holds the oldest step until then).  psih_t[PRED_CNT]: steps in the ring that
+    // continue the current trajectory, kept on the device; a change of state from outside the step
+    // loop clears it.
+    double* psih = nullptr;    // [PRED_DEPTH][4][N]
+    double* psih_t = nullptr;  // [PRED_DEPTH][4] + 1
+    int pred_head = 0;
     int gmres_m = 30;
 
     // ---- block-diagonal batch (batch = true): independent sub-systems (bubbles) sharing the mesh

@@ -108,6 +108,17 @@ void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s);
 void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k,
                   double* out, cudaStream_t s);
 void launch_rk4_final(Ctx& c, cudaStream_t s, const int* skip = nullptr);
+// Stage predictor of the mixed solve (stage.cu): depth of the history; the ring's stage times hold
+// at PRED_CNT the number of steps that continue the current trajectory.  Start value of stage
+// `stage` (0..3) extrapolated from the ring, the stage's solution stored into it, the end of a step;
+// state copies that end the trajectory when a value changes.
+constexpr int PRED_DEPTH = 3;
+constexpr int PRED_CNT = PRED_DEPTH * 4;
+void launch_stage_predict(Ctx& c, int stage, double* x, cudaStream_t s);
+void launch_stage_store(Ctx& c, int stage, const double* x, cudaStream_t s);
+void launch_stage_advance(Ctx& c, const int* skip, cudaStream_t s);
+void launch_state_accept(Ctx& c, int64_t n, const double* src, double* dst, cudaStream_t s);
+void launch_time_accept(Ctx& c, double t, cudaStream_t s);
 void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStream_t s);
 void launch_vertex_normals(Ctx& c, const double* x, double* out, cudaStream_t s);
 void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cudaStream_t s);

@@ -64,39 +64,74 @@ __device__ double block_sum(double v) {
     return r;
 }
 
-// y = A x; A column-major (T = double or float), x and y FP64.  grid (row blocks, column splits).
+// L2 eviction policies of the GEMV's matrix loads (createpolicy, PTX ISA 7.4): the FP64 G streams
+// through with evict_first, the FP32 approximate inverse X (half G's size) is loaded with evict_last
+// so that it can stay in L2 across the refinement steps of one solve while G passes by.
+__device__ __forceinline__ uint64_t l2_policy(bool keep) {
+    uint64_t p;
+    if (keep)
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else
+        asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// One matrix element through the read-only path, without L1 allocation, with the L2 policy pol.
+__device__ __forceinline__ double ld_mat(const double* p, uint64_t pol) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_mat(const float* p, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return (double)v;
+}
+
+// y = A x; A column-major (T = double or float), x and y FP64.  grid (row blocks of GV_ROWS rows,
+// column splits of `chunk` columns, a multiple of GV_UNR).  One row per thread; GV_UNR columns are
+// loaded before they are used.  The column-split partials are summed in a fixed order by the last
+// CTA of each row block (ticket counter), so the result is deterministic.
 // Optional fused dots of the result: d1 = y.u, d2 = y.w partials per row block.
-template <typename T>
 // y, u and w are not __restrict__: callers pass u == y to get y.y.  With cvec != null the result is
 // y = cvec + sgn * (A x) (residuals b - A x, accumulations x + X r); cvec may alias y.
-__global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, const T* __restrict__ A, const double* __restrict__ x,
-                                                  double* y, double* __restrict__ part,
-                                                  unsigned* __restrict__ cnt, const int* __restrict__ gate,
-                                                  int gate_val, const double* u, double* __restrict__ du,
-                                                  const double* w, double* __restrict__ dw, const double* cvec,
-                                                  double sgn) {
+// Measured on B200 at n = 4002, back to back as in the refinement loop: one FP64 and one FP32 GEMV
+// take 45 us together (256 rows x 64 column splits; wider vector loads per thread and TMA-staged
+// columns were both slower, and the serial tail of the split sum cost 5-7 us before its loads were
+// batched).
+constexpr int GV_UNR = 8;
+template <typename T>
+__global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, int chunk, const T* __restrict__ A,
+                                                  const double* __restrict__ x, double* y,
+                                                  double* __restrict__ part, unsigned* __restrict__ cnt,
+                                                  const int* __restrict__ gate, int gate_val, const double* u,
+                                                  double* __restrict__ du, const double* w, double* __restrict__ dw,
+                                                  const double* cvec, double sgn) {
     if (gate && *gate != gate_val) return;
     const int rb = blockIdx.x, cs = blockIdx.y, ncs = gridDim.y;
     const int i = rb * GV_ROWS + threadIdx.x;
-    const int chunk = (n + ncs - 1) / ncs;
-    const int c0 = cs * chunk, c1 = min(n, c0 + chunk);
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    const int c0 = min(n, cs * chunk), c1 = min(n, c0 + chunk);
     if (i < n) {
+        const uint64_t pol = l2_policy(sizeof(T) == 4);
+        double acc0 = 0.0, acc1 = 0.0;
         const T* col = A + (size_t)c0 * n + i;
         int j = c0;
-        for (; j + 3 < c1; j += 4) {
-            T a0 = col[0], a1 = col[(size_t)n], a2 = col[2 * (size_t)n], a3 = col[3 * (size_t)n];
-            acc0 = fma((double)a0, __ldg(x + j), acc0);
-            acc1 = fma((double)a1, __ldg(x + j + 1), acc1);
-            acc2 = fma((double)a2, __ldg(x + j + 2), acc2);
-            acc3 = fma((double)a3, __ldg(x + j + 3), acc3);
-            col += 4 * (size_t)n;
+        for (; j + GV_UNR <= c1; j += GV_UNR) {
+            double a[GV_UNR];
+#pragma unroll
+            for (int q = 0; q < GV_UNR; ++q) a[q] = ld_mat(col + (size_t)q * n, pol);
+#pragma unroll
+            for (int q = 0; q < GV_UNR; q += 2) {
+                acc0 = fma(a[q], __ldg(x + j + q), acc0);
+                acc1 = fma(a[q + 1], __ldg(x + j + q + 1), acc1);
+            }
+            col += (size_t)GV_UNR * n;
         }
         for (; j < c1; ++j) {
-            acc0 = fma((double)col[0], __ldg(x + j), acc0);
+            acc0 = fma(ld_mat(col, pol), __ldg(x + j), acc0);
             col += n;
         }
-        part[(size_t)cs * n + i] = (acc0 + acc1) + (acc2 + acc3);
+        part[(size_t)cs * n + i] = acc0 + acc1;
     }
     __threadfence();
     __shared__ unsigned s_ticket;
@@ -104,30 +139,41 @@ __global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, const T* __restrict__ A
     if (threadIdx.x == 0) s_ticket = atomicAdd(&cnt[rb], 1u);
     __syncthreads();
     if (s_ticket != (unsigned)(ncs - 1)) return;
-    // last CTA of this row block: fixed-order sum of the column-split partials
+    // last CTA of this row block: the column-split partials of each row summed in split order.  This
+    // runs after every other CTA of the row block has finished, so its latency is the kernel's tail:
+    // the partials are loaded 16 at a time before they are added, instead of one dependent L2 round
+    // trip per split.
     __threadfence();
+    constexpr int PB = 16;
     double yi = 0.0;
     if (i < n) {
-        for (int k = 0; k < ncs; ++k) yi += __ldcg(part + (size_t)k * n + i);
+        int k = 0;
+        for (; k + PB <= ncs; k += PB) {
+            double pv[PB];
+#pragma unroll
+            for (int q = 0; q < PB; ++q) pv[q] = __ldcg(part + (size_t)(k + q) * n + i);
+#pragma unroll
+            for (int q = 0; q < PB; ++q) yi += pv[q];
+        }
+        for (; k < ncs; ++k) yi += __ldcg(part + (size_t)k * n + i);
         if (cvec) yi = fma(sgn, yi, cvec[i]);
         y[i] = yi;
     }
     if (du) {
-        double v = (i < n) ? yi * u[i] : 0.0;
-        v = block_sum(v);
+        const double v = block_sum((i < n) ? yi * u[i] : 0.0);
         if (threadIdx.x == 0) du[rb] = v;
     }
     if (dw) {
-        double v = (i < n) ? yi * w[i] : 0.0;
-        v = block_sum(v);
+        const double v = block_sum((i < n) ? yi * w[i] : 0.0);
         if (threadIdx.x == 0) dw[rb] = v;
     }
     if (threadIdx.x == 0) cnt[rb] = 0u;
 }
 
+// Column splits: enough CTAs for about eight per SM, at most 64 (the partials buffer holds 64 n).
 static int gemv_splits(int n) {
-    int rb = (n + GV_ROWS - 1) / GV_ROWS;
-    int cs = std::max(1, std::min(64, (4 * 148 + rb - 1) / rb));
+    const int rb = (n + GV_ROWS - 1) / GV_ROWS;
+    int cs = std::max(1, std::min(64, (8 * 148 + rb - 1) / rb));
     cs = std::min(cs, std::max(1, n / 16));
     return cs;
 }
@@ -136,8 +182,10 @@ template <typename T>
 static void gemv_t(int n, const T* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt,
                    const int* gate = nullptr, int gate_val = 0, const double* u = nullptr, double* du = nullptr,
                    const double* w = nullptr, double* dw = nullptr, const double* cvec = nullptr, double sgn = 1.0) {
-    dim3 grid((n + GV_ROWS - 1) / GV_ROWS, gemv_splits(n));
-    KLAUNCH(), k_gemv<T><<<grid, GV_ROWS, 0, s>>>(n, A, x, y, part, cnt, gate, gate_val, u, du, w, dw, cvec, sgn);
+    const int ncs = gemv_splits(n);
+    const int chunk = ((n + ncs - 1) / ncs + GV_UNR - 1) / GV_UNR * GV_UNR;
+    dim3 grid((n + GV_ROWS - 1) / GV_ROWS, ncs);
+    KLAUNCH(), k_gemv<T><<<grid, GV_ROWS, 0, s>>>(n, chunk, A, x, y, part, cnt, gate, gate_val, u, du, w, dw, cvec, sgn);
 }
 
 void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s, double* part, unsigned* cnt) {
@@ -341,6 +389,7 @@ int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s
     }
     c.stats.last_iters = c.h_sc->iters;
     c.stats.last_rel_residual = c.h_sc->rhs_sq > 0 ? sqrt(c.h_sc->rr / c.h_sc->rhs_sq) : 0.0;
+    c.stats.total_iters += c.stats.last_iters;
     c.stats.solves++;
     return BEM_OK;
 }
@@ -1079,7 +1128,16 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     double* pb = c.red;        // nrb
     double* pr = c.red + nrb;  // (KMAX+1)*nrb
     KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb);
-    std::vector<double> host((size_t)(KMAX + 2) * nrb);
+    // the norms come back through pinned memory: a direct DMA the host sees as soon as it lands
+    const size_t nh = (size_t)(KMAX + 2) * nrb;
+    if (c.h_red_cap < nh) {
+        cudaFreeHost(c.h_red);
+        c.h_red = nullptr;
+        c.h_red_cap = 0;
+        BEM_CUDA(c, cudaMallocHost((void**)&c.h_red, nh * sizeof(double)));
+        c.h_red_cap = nh;
+    }
+    double* host = c.h_red;
     c.stats.last_iters = 0;
     int K = std::max(1, std::min(KMAX, c.ir_steps));
     double rho = 1.0, rel = 1.0, rel0 = -1.0;
@@ -1090,7 +1148,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
             gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, nullptr, 0, nullptr, nullptr, nullptr, nullptr, x, 1.0);
         }
         gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b, -1.0);
-        BEM_CUDA(c, cudaMemcpyAsync(host.data(), c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
+        BEM_CUDA(c, cudaMemcpyAsync(host, c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
         BEM_CUDA(c, cudaStreamSynchronize(s));
         c.stats.last_iters += K;
         double bb = 0.0;
@@ -1133,6 +1191,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     } else {
         c.stats.last_rel_residual = rel;
     }
+    c.stats.total_iters += c.stats.last_iters;
     c.stats.solves++;
     // steps for the next solve from the observed contraction
     if (converged && rho > 0.0 && rel0 > tol)

@@ -288,6 +288,102 @@ void launch_euler_final(Ctx& c, const double* vel, const double* potd, cudaStrea
     KLAUNCH(), k_euler_final<<<nb(N, 128), 128, 0, s>>>(N, vel, potd, c.sc, c.x, c.phi);
     KLAUNCH(), k_euler_time<<<1, 1, 0, s>>>(c.sc);
 }
+// ---------------------------------------------------------------- stage predictor (mixed solve)
+// RK4 stage times relative to the step: t + c_s dt.
+__constant__ double c_stage_c[4] = {0.0, 0.5, 0.5, 1.0};
+
+// Start value of a stage solve: Lagrange extrapolation in time from the same stage of the last m
+// steps (rows r0 newest, r1, r2 of the ring hist, times ht), x = sum_j w_j hist_j with
+// w_j = prod_{k != j} (T - T_k) / (T_j - T_k) and T = t + c_s dt the stage's time.  m is the number
+// of steps in the ring that continue the current trajectory (ht[PRED_CNT]); with none, x keeps the
+// previous stage's solution.  Coinciding times or weights above 16 in magnitude (a step much longer
+// than the history's) fall back to the newest value alone.  The refinement converges to the same
+// FP64 solution from any start; a start whose error is O(dt^m) instead of the previous stage's
+// O(dt) saves refinement steps.
+__global__ void k_stage_predict(int N, const double* __restrict__ hist, const double* __restrict__ ht, int r0, int r1,
+                                int r2, int stage, const DevScalars* __restrict__ sc, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = min(PRED_DEPTH, (int)ht[PRED_CNT]);
+    if (i >= N || m < 1) return;
+    const double T = sc->time + c_stage_c[stage] * sc->dt;
+    const int rows[3] = {r0, r1, r2};
+    double Tk[3] = {0.0, 0.0, 0.0}, w[3] = {1.0, 0.0, 0.0};
+    for (int j = 0; j < m; ++j) Tk[j] = ht[rows[j]];
+    bool ok = true;
+    for (int j = 0; j < m; ++j) {
+        double wj = 1.0;
+        for (int k = 0; k < m; ++k) {
+            if (k == j) continue;
+            const double d = Tk[j] - Tk[k];
+            if (d == 0.0) ok = false;
+            wj *= (T - Tk[k]) / d;
+        }
+        w[j] = wj;
+        if (!(fabs(wj) <= 16.0)) ok = false;
+    }
+    if (!ok || m < 2) {
+        x[i] = hist[(size_t)r0 * N + i];
+        return;
+    }
+    double v = w[0] * hist[(size_t)r0 * N + i];
+    for (int j = 1; j < m; ++j) v = fma(w[j], hist[(size_t)rows[j] * N + i], v);
+    x[i] = v;
+}
+
+__global__ void k_stage_store(int N, double* __restrict__ hist, double* __restrict__ ht, int row, int stage,
+                              const DevScalars* __restrict__ sc, const double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) ht[row] = sc->time + c_stage_c[stage] * sc->dt;
+    if (i < N) hist[(size_t)row * N + i] = x[i];
+}
+
+// End of a step: one more step in the ring, or none when the step's final update was skipped.
+__global__ void k_stage_advance(double* ht, const int* skip) {
+    ht[PRED_CNT] = (skip && *skip) ? 0.0 : fmin(ht[PRED_CNT] + 1.0, (double)PRED_DEPTH);
+}
+
+// dst <- src; a value that differs from the one held ends the predictor's trajectory.
+__global__ void k_state_accept(int64_t n, const double* __restrict__ src, double* __restrict__ dst, double* ht) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = src[i];
+        if (!(v == dst[i]) && ht) ht[PRED_CNT] = 0.0;
+        dst[i] = v;
+    }
+}
+__global__ void k_time_accept(double t, DevScalars* sc, double* ht) {
+    if (!(t == sc->time) && ht) ht[PRED_CNT] = 0.0;
+    sc->time = t;
+}
+
+// ring row of stage `stage` in the step `back` steps before the current one (back = 0: the current)
+static int pred_row(const Ctx& c, int back, int stage) {
+    return ((c.pred_head - back + 2 * PRED_DEPTH) % PRED_DEPTH) * 4 + stage;
+}
+
+void launch_stage_predict(Ctx& c, int stage, double* x, cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    KLAUNCH(), k_stage_predict<<<nb(N, 256), 256, 0, s>>>(N, c.psih, c.psih_t, pred_row(c, 1, stage),
+                                                          pred_row(c, 2, stage), pred_row(c, 3, stage), stage, c.sc, x);
+}
+
+void launch_stage_store(Ctx& c, int stage, const double* x, cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    KLAUNCH(), k_stage_store<<<nb(N, 256), 256, 0, s>>>(N, c.psih, c.psih_t, pred_row(c, 0, stage), stage, c.sc, x);
+}
+
+void launch_stage_advance(Ctx& c, const int* skip, cudaStream_t s) {
+    KLAUNCH(), k_stage_advance<<<1, 1, 0, s>>>(c.psih_t, skip);
+    c.pred_head = (c.pred_head + 1) % PRED_DEPTH;
+}
+
+void launch_state_accept(Ctx& c, int64_t n, const double* src, double* dst, cudaStream_t s) {
+    KLAUNCH(), k_state_accept<<<(int)std::min<int64_t>(nb(n, 256), 1184), 256, 0, s>>>(n, src, dst, c.psih_t);
+}
+
+void launch_time_accept(Ctx& c, double t, cudaStream_t s) {
+    KLAUNCH(), k_time_accept<<<1, 1, 0, s>>>(t, c.sc, c.psih_t);
+}
+
 void launch_get_dt(Ctx& c, const double* vel, const double* potd, double dp, cudaStream_t s) {
     KLAUNCH(), k_get_dt<<<1, 1024, 0, s>>>((int)c.topo.N, vel, potd, dp, c.prm.dp_balance, c.prm.min_dt, c.sc);
 }

@@ -67,6 +67,10 @@ typedef struct {
 /* bem_params.flags: run the FP64 BiCGSTAB as separate kernels per iteration instead of the persistent
  * cooperative kernel (same iteration; for comparison, or where cooperative launches are unwanted). */
 #define BEM_FLAG_BICGSTAB_MULTIKERNEL 1
+/* bem_params.flags: start each RK4 stage solve of BEM_SOLVER_MIXED from the previous stage's solution
+ * instead of the stage predictor (an extrapolation in time from the same stage of the last three
+ * steps).  Either start converges to the same FP64 solution; the predictor saves refinement steps. */
+#define BEM_FLAG_NO_STAGE_PREDICTOR 2
 
 /* Fill *p with the reference's defaults. */
 void bem_default_params(bem_params* p);
@@ -242,6 +246,8 @@ typedef struct {
     int64_t fp64_fallbacks;   /* mixed solves that fell back to the FP64 BiCGSTAB: no approximate inverse
                                  could be built, or GMRES missed the tolerance (a singular or nearly
                                  singular G, e.g. a bubble cut by its own wall image) */
+    int64_t total_iters;      /* iterations of every iterative solve since creation (refinement steps of
+                                 the mixed path, including its GMRES hand-overs; BiCGSTAB iterations) */
 } bem_stats;
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 

@@ -277,6 +277,33 @@ def test_negative_x_leaves_the_state_untouched():
     assert np.array_equal(gx, x) and np.array_equal(gp, phi) and np.all(gs == 0.0) and gt == 1.0
 
 
+def test_stage_predictor_keeps_the_trajectory():
+    # the mixed solver starts each RK4 stage from an extrapolation of the same stage of earlier steps;
+    # any start converges to the same FP64 solution, so the trajectory equals the one started from
+    # the previous stage (BEM_FLAG_NO_STAGE_PREDICTOR), also after the state is pushed back unchanged
+    # (history kept) or changed (history dropped), and with an adaptive step
+    from bem_b200 import _lib as L
+    v, f = mesh.bubble(8, 1.0, (2.0, 0.0, 0.0))
+    rng = np.random.default_rng(3)
+    v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None]
+    sims = [ColocSim(v, f, pressurefield=(-0.8, 2 * np.pi / 5, 0.0), solver="mixed") for _ in range(2)]
+    sims[1]._update(flags=L.FLAG_NO_STAGE_PREDICTOR)
+    for sim in sims:
+        sim.set_phi(0.0)
+        for _ in range(6):
+            sim.evolve_rk4_steps(5e-3, 1)
+        x, p, s = sim.get_vertices(), sim.get_phi(), sim.get_psi()
+        sim.set_state(x, p, s)  # the same state: the predictor's history stays
+        sim.evolve_system_RK4(5e-3, fixdt=True)
+        x, p, s = sim.get_vertices(), sim.get_phi(), sim.get_psi()
+        sim.set_state(x, 1.001 * p, s)  # another state: the history is dropped
+        for _ in range(4):
+            sim.evolve_system_RK4(5e-3, fixdt=False)
+    (xa, pa), (xb, pb) = [(sim.get_vertices(), sim.get_phi()) for sim in sims]
+    assert rel(xa, xb) < 1e-11 and rel(pa, pb) < 1e-11
+    assert sims[0].stats().total_iters > 0 and sims[0].stats().solves == sims[1].stats().solves
+
+
 def test_mixed_precision_error_headline_size():
     # N = 4002 (config 2 mesh with the seeded 1% radial perturbation): psi of the mixed path
     # against the FP64 LU path at <= 1e-8 relative
