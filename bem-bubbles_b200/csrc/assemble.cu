@@ -118,8 +118,12 @@ static void upload_constants() {
     done_mask |= 1ull << (dev & 63);
 }
 
-// Per-triangle record: Interpolator (Interpolator.hpp:15-37) quantities and the 7 quadrature
-// points y_q = a + u_q*ab + v_q*bc.
+// Per-triangle record: Interpolator (Interpolator.hpp:15-37) quantities and what the 7-point rule
+// needs of the quadrature points y_q = a + w_q, w_q = u_q*ab + v_q*bc.  For a row x,
+//   |y_q - x|^2 = |a - x|^2 + u_q (a - x).2ab + v_q (a - x).2bc + |w_q|^2,
+// so a pair costs three dot products with a - x and then two FMAs and an add per point.  Layout:
+// a (0-2), 2ab (3-5), 2bc (6-8), |w_q|^2 (9-15), y_q.x (16-22, for the wall image), unit normal
+// (23-25), area (26), plane offset a.n (27).
 __global__ void k_triangle_records(int M, const double* __restrict__ x, const int* __restrict__ tri,
                                    double* __restrict__ rec) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -132,22 +136,30 @@ __global__ void k_triangle_records(int M, const double* __restrict__ x, const in
     double area = sqrt(nx * nx + ny * ny + nz * nz);
     double ia_ = 1.0 / area;
     double* r = rec + (size_t)t * REC;
+    r[0] = ax;
+    r[1] = ay;
+    r[2] = az;
+    r[3] = 2.0 * abx;
+    r[4] = 2.0 * aby;
+    r[5] = 2.0 * abz;
+    r[6] = 2.0 * bcx;
+    r[7] = 2.0 * bcy;
+    r[8] = 2.0 * bcz;
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
-        double u = c_quv[q][0], v = c_quv[q][1];
-        r[3 * q + 0] = (ax + u * abx) + v * bcx;
-        r[3 * q + 1] = (ay + u * aby) + v * bcy;
-        r[3 * q + 2] = (az + u * abz) + v * bcz;
+        const double u = c_quv[q][0], v = c_quv[q][1];
+        const double wx = u * abx + v * bcx, wy = u * aby + v * bcy, wz = u * abz + v * bcz;
+        r[9 + q] = wx * wx + wy * wy + wz * wz;
+        r[16 + q] = ax + wx;
     }
     const double unx = nx * ia_, uny = ny * ia_, unz = nz * ia_;
-    r[21] = unx;
-    r[22] = uny;
-    r[23] = unz;
-    r[24] = area;
+    r[23] = unx;
+    r[24] = uny;
+    r[25] = unz;
+    r[26] = area;
     // plane offset a.n: every quadrature point y_q satisfies y_q.n = a.n, so (y_q - x).n is one
     // number per (row, triangle) pair
-    r[25] = ax * unx + ay * uny + az * unz;
-    r[26] = r[27] = 0.0;
+    r[27] = ax * unx + ay * uny + az * unz;
 }
 
 // 1/sqrt(r2) for r2 > 0 in FP64: the hardware's approximate reciprocal square root
@@ -186,23 +198,25 @@ struct PairSums {
 template <bool MIRROR>
 __device__ __forceinline__ void regular_pair(const double* __restrict__ r, double xi0, double xi1, double xi2,
                                              PairSums& p) {
-    const double nx = r[21], ny = r[22], nz = r[23], area = r[24], dt = r[25];
+    const double nx = r[23], ny = r[24], nz = r[25], area = r[26], dt = r[27];
     const double xn_yz = fma(xi1, ny, __dmul_rn(xi2, nz));
     const double dn = dt - fma(xi0, nx, xn_yz);  // (y - x).n
+    const double ax = r[0] - xi0, ay = r[1] - xi1, az = r[2] - xi2;
+    const double A = fma(ax, ax, fma(ay, ay, __dmul_rn(az, az)));
+    const double B = fma(ax, r[3], fma(ay, r[4], __dmul_rn(az, r[5])));
+    const double C = fma(ax, r[6], fma(ay, r[7], __dmul_rn(az, r[8])));
+    const double x4 = 4.0 * xi0;
     double kg[7], kh[7], km[7];
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
-        const double yx = r[3 * q];
-        const double zy = r[3 * q + 1] - xi1, zz = r[3 * q + 2] - xi2;
-        const double zx = yx - xi0;
-        const double yz2 = fma(zy, zy, __dmul_rn(zz, zz));
-        const double inv = rsqrt_fp64(fma(zx, zx, yz2));
+        const double r2 = fma(B, c_quv[q][0], fma(C, c_quv[q][1], A + r[9 + q]));
+        const double inv = rsqrt_fp64(r2);
         kg[q] = inv;
         kh[q] = __dmul_rn(__dmul_rn(inv, inv), inv);
         if (MIRROR) {
-            // image point (-y.x, y.y, y.z), image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229)
-            const double mx = -yx - xi0;
-            const double inv2 = rsqrt_fp64(fma(mx, mx, yz2));
+            // image point (-y.x, y.y, y.z), image normal (-n.x, n.y, n.z) (Integrator.hpp:211-229):
+            // |y' - x|^2 = |y - x|^2 + 4 x.x y.x
+            const double inv2 = rsqrt_fp64(fma(x4, r[16 + q], r2));
             kg[q] += inv2;
             km[q] = __dmul_rn(__dmul_rn(inv2, inv2), inv2);
         }
@@ -227,12 +241,11 @@ __device__ __forceinline__ double add_h(const PairSums& p, int k, double acc) {
     return __dadd_rn(acc, fma(p.m[k], p.sm, __dmul_rn(p.h[k], p.sh)));
 }
 
-// Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  Adds G and H of the pair
-// directly into the row's shared-memory accumulators of the owned slots (codes as in k_assemble),
-// so nothing of this rare path lives in the hot loop's registers or in local memory.
+// Singular pair: row i is vertex `shift` of triangle (ta, tb, tc).  gg[m], hh[m]: the G and H
+// contributions to the column of the triangle's vertex at position (m + shift) % 3.
 template <bool MIRROR>
-__device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta, int tb, int tc, int shift, int code,
-                                           double* accG, double* accH, int stride) {
+__device__ __forceinline__ void singular_sums(const double* __restrict__ x, int ta, int tb, int tc, int shift,
+                                              double gg[3], double hh[3]) {
     const int r0 = shift == 0 ? ta : (shift == 1 ? tb : tc);
     const int r1 = shift == 0 ? tb : (shift == 1 ? tc : ta);
     const int r2 = shift == 0 ? tc : (shift == 1 ? ta : tb);
@@ -291,17 +304,72 @@ __device__ __noinline__ void singular_pair(const double* __restrict__ x, int ta,
         rh1 = -(b1 * marea);
         rh2 = -(b2 * marea);
     }
-    // rotated vertex m sits at triangle position (m + shift) % 3
-    const double gg[3] = {rg0, rg1, rg2}, hh[3] = {rh0, rh1, rh2};
+    gg[0] = rg0;
+    gg[1] = rg1;
+    gg[2] = rg2;
+    hh[0] = rh0;
+    hh[1] = rh1;
+    hh[2] = rh2;
+}
+
+// Singular pairs of row i (il within its block of n vertices, G/H block at mbase): the triangles
+// around vertex i in increasing index order (the vertex-to-triangle lists are sorted), each adding
+// its three contributions to G(i, j) and H(i, j) after the tile kernel has written the regular
+// part.  One thread owns row i, so the read-modify-writes do not race.  srow and sb receive the row's
+// singular share of sum_j H(i, j) and sum_j H(i, j) phi_j for the 4 pi rule and the right-hand side.
+// A separate pass because inside the tile loop the rare singular branch cost a fifth of the kernel's
+// time (divergent warps waiting at the staging barriers, and the call in the hot loop).
+template <bool MIRROR>
+__device__ __forceinline__ void singular_row(int i, int il, int n, long long mbase, int vbase,
+                                             const double* __restrict__ x, const int* __restrict__ tri,
+                                             const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
+                                             const double* __restrict__ phi, double* __restrict__ G,
+                                             double* __restrict__ H, double* __restrict__ srow,
+                                             double* __restrict__ sb) {
+    double rs = 0.0, bs = 0.0;
+    for (int e = csr_off[i]; e < csr_off[i + 1]; ++e) {
+        const int t = csr_idx[e];
+        const int ta = tri[3 * t], tb = tri[3 * t + 1], tc = tri[3 * t + 2];
+        const int shift = (i == ta) ? 0 : ((i == tb) ? 1 : 2);
+        double gg[3], hh[3];
+        singular_sums<MIRROR>(x, ta, tb, tc, shift, gg, hh);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const int k = (m + shift) % 3;
-        const int sl = (code >> (SLOT_BITS * k)) & SLOT_NONE;
-        if (sl != SLOT_NONE) {
-            accG[sl * stride] += gg[m];
-            accH[sl * stride] += hh[m];
+        for (int m = 0; m < 3; ++m) {
+            const int k = (m + shift) % 3;
+            const int j = tri[3 * t + k];
+            const size_t o = (size_t)mbase + (size_t)(j - vbase) * n + il;
+            G[o] += gg[m];
+            if (MIRROR) {  // without the wall image the singular double layer vanishes (flat triangle)
+                H[o] += hh[m];
+                rs += hh[m];
+                bs = fma(hh[m], phi[j], bs);
+            }
         }
     }
+    srow[i] = rs;
+    sb[i] = bs;
+}
+
+template <bool MIRROR>
+__global__ void k_singular_rows(int N, const double* __restrict__ x, const int* __restrict__ tri,
+                                const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
+                                const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ H,
+                                double* __restrict__ srow, double* __restrict__ sb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    singular_row<MIRROR>(i, i, N, 0, 0, x, tri, csr_off, csr_idx, phi, G, H, srow, sb);
+}
+
+template <bool MIRROR>
+__global__ void k_singular_rows_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
+                                      const double* __restrict__ x, const int* __restrict__ tri,
+                                      const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
+                                      const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ H,
+                                      double* __restrict__ srow, double* __restrict__ sb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const BlockInfo B = blk[vblk[i]];
+    singular_row<MIRROR>(i, i - B.vbase, B.n, B.mbase, B.vbase, x, tri, csr_off, csr_idx, phi, G, H, srow, sb);
 }
 
 // Column-group tile: the columns of group g (local index gl within its block) for rows
@@ -356,11 +424,7 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
             for (int tt = 0; tt < cnt; ++tt) {
                 const int4 info = reinterpret_cast<const int4*>(sinfo)[tt];
                 const int code = info.x;
-                if (i == info.y || i == info.z || i == info.w) {
-                    const int shift = (i == info.y) ? 0 : ((i == info.z) ? 1 : 2);
-                    singular_pair<MIRROR>(x, info.y, info.z, info.w, shift, code, accG + tid, accH + tid, ROWS);
-                    continue;
-                }
+                if (i == info.y || i == info.z || i == info.w) continue;  // singular: k_singular_rows
                 PairSums p;
                 regular_pair<MIRROR>(srec + tt * REC, xi0, xi1, xi2, p);
                 const int s0 = code & SLOT_NONE, s1 = (code >> SLOT_BITS) & SLOT_NONE,
@@ -441,10 +505,12 @@ __global__ void __launch_bounds__(ROWS, MINB)
 }
 
 // 4 pi rule and right-hand side of one row: H(i,i) -= 4 pi - val, val = -sum_j H(i,j); b = H*phi.
+// srow_i, sb_i: the singular pairs' share of the row sum and of H*phi (added after the tiles').
 // One warp per row: lane l sums the partials of groups l, l+32, ... and the warp adds the lane sums
 // in a fixed butterfly order (deterministic).  il: row within its block; partials at rowHp[g*n + il].
 __device__ __forceinline__ void diag_row(int il, int n, int ngroups, const double* __restrict__ rowHp,
-                                         const double* __restrict__ bp, double phii, double* Hii, double* bi) {
+                                         const double* __restrict__ bp, double srow_i, double sb_i, double phii,
+                                         double* Hii, double* bi) {
     const int lane = threadIdx.x & 31;
     double val = 0.0, bs = 0.0;
     for (int g = lane; g < ngroups; g += 32) {
@@ -457,28 +523,32 @@ __device__ __forceinline__ void diag_row(int il, int n, int ngroups, const doubl
         bs += __shfl_xor_sync(0xffffffffu, bs, o);
     }
     if (lane) return;
+    val -= srow_i;
+    bs += sb_i;
     const double d = -(4.0 * 3.14159265358979323846 - val);
     *Hii += d;
     if (bi) *bi = fma(d, phii, bs);
 }
 
 __global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
+                           const double* __restrict__ srow, const double* __restrict__ sb,
                            const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= N) return;
-    diag_row(i, N, ngroups, rowHp, bp, phi[i], H + (size_t)i * N + i, b ? b + i : nullptr);
+    diag_row(i, N, ngroups, rowHp, bp, srow[i], sb[i], phi[i], H + (size_t)i * N + i, b ? b + i : nullptr);
 }
 
 // The same rule per block of a batch (rows of block vblk[i], its own groups and G/H block).
 __global__ void k_diag_rhs_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
                                  const double* __restrict__ rowHp, const double* __restrict__ bp,
+                                 const double* __restrict__ srow, const double* __restrict__ sb,
                                  const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= N) return;
     const BlockInfo B = blk[vblk[i]];
     const int il = i - B.vbase;
-    diag_row(il, B.n, B.ngroups, rowHp + B.pbase, bp + B.pbase, phi[i], H + (size_t)B.mbase + (size_t)il * B.n + il,
-             b ? b + i : nullptr);
+    diag_row(il, B.n, B.ngroups, rowHp + B.pbase, bp + B.pbase, srow[i], sb[i], phi[i],
+             H + (size_t)B.mbase + (size_t)il * B.n + il, b ? b + i : nullptr);
 }
 
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
@@ -595,14 +665,31 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
         launch_tiles<true>(c, x, phi, G, H, s);
     else
         launch_tiles<false>(c, x, phi, G, H, s);
+    const Topology& T = c.topo;
+    const int nbs = (N + 127) / 128;
+    if (c.batch) {
+        if (c.prm.mirror)
+            KLAUNCH(), k_singular_rows_batch<true><<<nbs, 128, 0, s>>>(N, c.vblk, c.blk, x, T.tri, T.csr_off, T.csr_idx,
+                                                                       phi, G, H, c.srow, c.sb);
+        else
+            KLAUNCH(), k_singular_rows_batch<false><<<nbs, 128, 0, s>>>(N, c.vblk, c.blk, x, T.tri, T.csr_off,
+                                                                        T.csr_idx, phi, G, H, c.srow, c.sb);
+    } else {
+        if (c.prm.mirror)
+            KLAUNCH(), k_singular_rows<true><<<nbs, 128, 0, s>>>(N, x, T.tri, T.csr_off, T.csr_idx, phi, G, H, c.srow,
+                                                                 c.sb);
+        else
+            KLAUNCH(), k_singular_rows<false><<<nbs, 128, 0, s>>>(N, x, T.tri, T.csr_off, T.csr_idx, phi, G, H, c.srow,
+                                                                  c.sb);
+    }
     if (c.prof) {
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }
     if (c.batch)
-        KLAUNCH(), k_diag_rhs_batch<<<(N + 7) / 8, 256, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, phi, H, b);
+        KLAUNCH(), k_diag_rhs_batch<<<(N + 7) / 8, 256, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, c.srow, c.sb, phi, H, b);
     else
-        KLAUNCH(), k_diag_rhs<<<(N + 7) / 8, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, phi, H, b);
+        KLAUNCH(), k_diag_rhs<<<(N + 7) / 8, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, c.srow, c.sb, phi, H, b);
 }
 
 }  // namespace bemb
