@@ -312,64 +312,127 @@ __device__ __forceinline__ void singular_sums(const double* __restrict__ x, int 
     hh[2] = rh2;
 }
 
-// Singular pairs of row i (il within its block of n vertices, G/H block at mbase): the triangles
-// around vertex i in increasing index order (the vertex-to-triangle lists are sorted), each adding
-// its three contributions to G(i, j) and H(i, j) after the tile kernel has written the regular
-// part.  One thread owns row i, so the read-modify-writes do not race.  srow and sb receive the row's
-// singular share of sum_j H(i, j) and sum_j H(i, j) phi_j for the 4 pi rule and the right-hand side.
-// A separate pass because inside the tile loop the rare singular branch cost a fifth of the kernel's
-// time (divergent warps waiting at the staging barriers, and the call in the hot loop).
+// Singular pairs of a row and the row's 4 pi rule, one warp per row (row i, il within its block of n
+// vertices whose G/H block starts at element mbase and whose group partials are rowHp, bp).
+//  * The lanes take the triangles around vertex i (the vertex-to-triangle lists are sorted), 32 at a
+//    time, and evaluate their singular pairs in parallel: entries (lane, m) with column j and the G
+//    and H contributions, staged in shared memory.
+//  * The lane holding the first entry of each column j adds that column's entries to G(i, j) and
+//    H(i, j) one by one in entry order (increasing triangle index), after the tile kernel has written
+//    the regular part.  Entries of one column are never split between two lanes, so nothing races.
+//  * The row's sums sum_j H(i, j) and sum_j H(i, j) phi_j are the group partials of the tiles (a fixed
+//    butterfly order) plus the singular share (entry order); H(i, i) -= 4 pi + sum_j H(i, j) and
+//    b_i = (H phi)_i follow (ColocSim.cpp:85-97).  Every sum has one fixed order, the same as with one
+//    thread per row walking the triangles in order.
+// A separate pass because inside the tile loop the rare singular branch cost a fifth of the tile
+// kernel's time (divergent warps waiting at the staging barriers, and the call in the hot loop).
+constexpr int SD_WARPS = 8;  // rows per CTA
 template <bool MIRROR>
-__device__ __forceinline__ void singular_row(int i, int il, int n, long long mbase, int vbase,
-                                             const double* __restrict__ x, const int* __restrict__ tri,
-                                             const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
-                                             const double* __restrict__ phi, double* __restrict__ G,
-                                             double* __restrict__ H, double* __restrict__ srow,
-                                             double* __restrict__ sb) {
-    double rs = 0.0, bs = 0.0;
-    for (int e = csr_off[i]; e < csr_off[i + 1]; ++e) {
-        const int t = csr_idx[e];
-        const int ta = tri[3 * t], tb = tri[3 * t + 1], tc = tri[3 * t + 2];
-        const int shift = (i == ta) ? 0 : ((i == tb) ? 1 : 2);
-        double gg[3], hh[3];
-        singular_sums<MIRROR>(x, ta, tb, tc, shift, gg, hh);
+__device__ __forceinline__ void singular_diag_row(int i, int il, int n, long long mbase, int vbase, int ngroups,
+                                                  const double* __restrict__ rowHp, const double* __restrict__ bp,
+                                                  const double* __restrict__ x, const int* __restrict__ tri,
+                                                  const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
+                                                  const double* __restrict__ phi, double* __restrict__ G,
+                                                  double* __restrict__ H, double* __restrict__ b) {
+    __shared__ int s_j[SD_WARPS][96];
+    __shared__ double s_g[SD_WARPS][96], s_h[SD_WARPS][96];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double rs = 0.0, bsing = 0.0;  // (lane 0) the singular share of the H row sum and of H phi
+    const int e0 = csr_off[i], e1 = csr_off[i + 1];
+    for (int base = e0; base < e1; base += 32) {
+        const int e = base + lane;
+        int jj[3] = {-1, -1, -1};
+        if (e < e1) {
+            const int t = csr_idx[e];
+            const int ta = tri[3 * t], tb = tri[3 * t + 1], tc = tri[3 * t + 2];
+            const int shift = (i == ta) ? 0 : ((i == tb) ? 1 : 2);
+            double gg[3], hh[3];
+            singular_sums<MIRROR>(x, ta, tb, tc, shift, gg, hh);
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-            const int k = (m + shift) % 3;
-            const int j = tri[3 * t + k];
-            const size_t o = (size_t)mbase + (size_t)(j - vbase) * n + il;
-            G[o] += gg[m];
-            if (MIRROR) {  // without the wall image the singular double layer vanishes (flat triangle)
-                H[o] += hh[m];
-                rs += hh[m];
-                bs = fma(hh[m], phi[j], bs);
+            for (int m = 0; m < 3; ++m) {
+                jj[m] = tri[3 * t + (m + shift) % 3];
+                s_g[w][3 * lane + m] = gg[m];
+                s_h[w][3 * lane + m] = hh[m];
             }
         }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) s_j[w][3 * lane + m] = jj[m];
+        __syncwarp();
+        const int ne = 3 * min(32, e1 - base);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const int j = jj[m], me = 3 * lane + m;
+            if (j < 0) continue;
+            bool first = true;
+            for (int q = 0; q < me; ++q)
+                if (s_j[w][q] == j) {
+                    first = false;
+                    break;
+                }
+            if (!first) continue;
+            const size_t o = (size_t)mbase + (size_t)(j - vbase) * n + il;
+            double gv = G[o], hv = MIRROR ? H[o] : 0.0;
+            for (int q = me; q < ne; ++q)
+                if (s_j[w][q] == j) {
+                    gv += s_g[w][q];
+                    hv += s_h[w][q];
+                }
+            G[o] = gv;
+            if (MIRROR) H[o] = hv;  // without the wall image the singular double layer vanishes (flat triangle)
+        }
+        if (MIRROR && lane == 0)
+            for (int q = 0; q < ne; ++q)
+                if (s_j[w][q] >= 0) {
+                    rs += s_h[w][q];
+                    bsing = fma(s_h[w][q], phi[s_j[w][q]], bsing);
+                }
+        __syncwarp();
     }
-    srow[i] = rs;
-    sb[i] = bs;
+    // 4 pi rule and right-hand side: lane l sums the partials of groups l, l+32, ... and the warp adds
+    // the lane sums in a fixed butterfly order (deterministic)
+    double val = 0.0, bs = 0.0;
+    for (int g = lane; g < ngroups; g += 32) {
+        val -= rowHp[(size_t)g * n + il];
+        bs += bp[(size_t)g * n + il];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        val += __shfl_xor_sync(0xffffffffu, val, o);
+        bs += __shfl_xor_sync(0xffffffffu, bs, o);
+    }
+    if (lane) return;
+    val -= rs;
+    bs += bsing;
+    const double d = -(4.0 * 3.14159265358979323846 - val);
+    const size_t oii = (size_t)mbase + (size_t)il * n + il;
+    H[oii] += d;  // after the warp's singular update of H(i, i) (ordered by the last __syncwarp)
+    if (b) b[i] = fma(d, phi[i], bs);
 }
 
 template <bool MIRROR>
-__global__ void k_singular_rows(int N, const double* __restrict__ x, const int* __restrict__ tri,
-                                const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
-                                const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ H,
-                                double* __restrict__ srow, double* __restrict__ sb) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * SD_WARPS)
+    k_singular_diag(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
+                    const double* __restrict__ x, const int* __restrict__ tri, const int* __restrict__ csr_off,
+                    const int* __restrict__ csr_idx, const double* __restrict__ phi, double* __restrict__ G,
+                    double* __restrict__ H, double* __restrict__ b) {
+    const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
     if (i >= N) return;
-    singular_row<MIRROR>(i, i, N, 0, 0, x, tri, csr_off, csr_idx, phi, G, H, srow, sb);
+    singular_diag_row<MIRROR>(i, i, N, 0, 0, ngroups, rowHp, bp, x, tri, csr_off, csr_idx, phi, G, H, b);
 }
 
+// The same per block of a batch (rows of block vblk[i], its own groups and G/H block).
 template <bool MIRROR>
-__global__ void k_singular_rows_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
-                                      const double* __restrict__ x, const int* __restrict__ tri,
-                                      const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
-                                      const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ H,
-                                      double* __restrict__ srow, double* __restrict__ sb) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * SD_WARPS)
+    k_singular_diag_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
+                          const double* __restrict__ rowHp, const double* __restrict__ bp,
+                          const double* __restrict__ x, const int* __restrict__ tri, const int* __restrict__ csr_off,
+                          const int* __restrict__ csr_idx, const double* __restrict__ phi, double* __restrict__ G,
+                          double* __restrict__ H, double* __restrict__ b) {
+    const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
     if (i >= N) return;
     const BlockInfo B = blk[vblk[i]];
-    singular_row<MIRROR>(i, i - B.vbase, B.n, B.mbase, B.vbase, x, tri, csr_off, csr_idx, phi, G, H, srow, sb);
+    singular_diag_row<MIRROR>(i, i - B.vbase, B.n, B.mbase, B.vbase, B.ngroups, rowHp + B.pbase, bp + B.pbase, x,
+                              tri, csr_off, csr_idx, phi, G, H, b);
 }
 
 // Column-group tile: the columns of group g (local index gl within its block) for rows
@@ -424,7 +487,7 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
             for (int tt = 0; tt < cnt; ++tt) {
                 const int4 info = reinterpret_cast<const int4*>(sinfo)[tt];
                 const int code = info.x;
-                if (i == info.y || i == info.z || i == info.w) continue;  // singular: k_singular_rows
+                if (i == info.y || i == info.z || i == info.w) continue;  // singular: k_singular_diag
                 PairSums p;
                 regular_pair<MIRROR>(srec + tt * REC, xi0, xi1, xi2, p);
                 const int s0 = code & SLOT_NONE, s1 = (code >> SLOT_BITS) & SLOT_NONE,
@@ -502,53 +565,6 @@ __global__ void __launch_bounds__(ROWS, MINB)
         assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp,
                                          bp, td.x, td.w, td.y, B.vbase + B.n, B.n, B.vbase, B.mbase, B.pbase);
     }
-}
-
-// 4 pi rule and right-hand side of one row: H(i,i) -= 4 pi - val, val = -sum_j H(i,j); b = H*phi.
-// srow_i, sb_i: the singular pairs' share of the row sum and of H*phi (added after the tiles').
-// One warp per row: lane l sums the partials of groups l, l+32, ... and the warp adds the lane sums
-// in a fixed butterfly order (deterministic).  il: row within its block; partials at rowHp[g*n + il].
-__device__ __forceinline__ void diag_row(int il, int n, int ngroups, const double* __restrict__ rowHp,
-                                         const double* __restrict__ bp, double srow_i, double sb_i, double phii,
-                                         double* Hii, double* bi) {
-    const int lane = threadIdx.x & 31;
-    double val = 0.0, bs = 0.0;
-    for (int g = lane; g < ngroups; g += 32) {
-        val -= rowHp[(size_t)g * n + il];
-        bs += bp[(size_t)g * n + il];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        val += __shfl_xor_sync(0xffffffffu, val, o);
-        bs += __shfl_xor_sync(0xffffffffu, bs, o);
-    }
-    if (lane) return;
-    val -= srow_i;
-    bs += sb_i;
-    const double d = -(4.0 * 3.14159265358979323846 - val);
-    *Hii += d;
-    if (bi) *bi = fma(d, phii, bs);
-}
-
-__global__ void k_diag_rhs(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
-                           const double* __restrict__ srow, const double* __restrict__ sb,
-                           const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= N) return;
-    diag_row(i, N, ngroups, rowHp, bp, srow[i], sb[i], phi[i], H + (size_t)i * N + i, b ? b + i : nullptr);
-}
-
-// The same rule per block of a batch (rows of block vblk[i], its own groups and G/H block).
-__global__ void k_diag_rhs_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
-                                 const double* __restrict__ rowHp, const double* __restrict__ bp,
-                                 const double* __restrict__ srow, const double* __restrict__ sb,
-                                 const double* __restrict__ phi, double* __restrict__ H, double* __restrict__ b) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= N) return;
-    const BlockInfo B = blk[vblk[i]];
-    const int il = i - B.vbase;
-    diag_row(il, B.n, B.ngroups, rowHp + B.pbase, bp + B.pbase, srow[i], sb[i], phi[i],
-             H + (size_t)B.mbase + (size_t)il * B.n + il, b ? b + i : nullptr);
 }
 
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
@@ -665,31 +681,28 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
         launch_tiles<true>(c, x, phi, G, H, s);
     else
         launch_tiles<false>(c, x, phi, G, H, s);
+    // singular pairs and the 4 pi rule, one warp per row
     const Topology& T = c.topo;
-    const int nbs = (N + 127) / 128;
+    const int nbs = (N + SD_WARPS - 1) / SD_WARPS, nt = 32 * SD_WARPS;
     if (c.batch) {
         if (c.prm.mirror)
-            KLAUNCH(), k_singular_rows_batch<true><<<nbs, 128, 0, s>>>(N, c.vblk, c.blk, x, T.tri, T.csr_off, T.csr_idx,
-                                                                       phi, G, H, c.srow, c.sb);
+            KLAUNCH(), k_singular_diag_batch<true><<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, x, T.tri, T.csr_off,
+                                                                      T.csr_idx, phi, G, H, b);
         else
-            KLAUNCH(), k_singular_rows_batch<false><<<nbs, 128, 0, s>>>(N, c.vblk, c.blk, x, T.tri, T.csr_off,
-                                                                        T.csr_idx, phi, G, H, c.srow, c.sb);
+            KLAUNCH(), k_singular_diag_batch<false><<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, x, T.tri,
+                                                                       T.csr_off, T.csr_idx, phi, G, H, b);
     } else {
         if (c.prm.mirror)
-            KLAUNCH(), k_singular_rows<true><<<nbs, 128, 0, s>>>(N, x, T.tri, T.csr_off, T.csr_idx, phi, G, H, c.srow,
-                                                                 c.sb);
+            KLAUNCH(), k_singular_diag<true><<<nbs, nt, 0, s>>>(N, T.ngroups, c.rowHp, c.bp, x, T.tri, T.csr_off,
+                                                                T.csr_idx, phi, G, H, b);
         else
-            KLAUNCH(), k_singular_rows<false><<<nbs, 128, 0, s>>>(N, x, T.tri, T.csr_off, T.csr_idx, phi, G, H, c.srow,
-                                                                  c.sb);
+            KLAUNCH(), k_singular_diag<false><<<nbs, nt, 0, s>>>(N, T.ngroups, c.rowHp, c.bp, x, T.tri, T.csr_off,
+                                                                 T.csr_idx, phi, G, H, b);
     }
-    if (c.prof) {
+    if (c.prof) {  // the profile's assembly time: tiles, singular pairs and the 4 pi rule
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }
-    if (c.batch)
-        KLAUNCH(), k_diag_rhs_batch<<<(N + 7) / 8, 256, 0, s>>>(N, c.vblk, c.blk, c.rowHp, c.bp, c.srow, c.sb, phi, H, b);
-    else
-        KLAUNCH(), k_diag_rhs<<<(N + 7) / 8, 256, 0, s>>>(N, c.topo.ngroups, c.rowHp, c.bp, c.srow, c.sb, phi, H, b);
 }
 
 }  // namespace bemb

@@ -473,8 +473,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     for (auto p : vec3s)
         if ((rc = dalloc(c, p, 3 * n))) return rc;
     double** vecs[] = {&c.phi, &c.psi, &c.b, &c.psil, &c.kap, &c.fieldv, &c.p1, &c.ps, &c.kp1, &c.kp2,
-                       &c.kp3, &c.kp4, &c.r, &c.r0, &c.pv, &c.vv, &c.yv, &c.zv, &c.sv, &c.tv, &c.invd, &c.potz,
-                       &c.srow, &c.sb};
+                       &c.kp3, &c.kp4, &c.r, &c.r0, &c.pv, &c.vv, &c.yv, &c.zv, &c.sv, &c.tv, &c.invd, &c.potz};
     for (auto p : vecs)
         if ((rc = dalloc(c, p, n))) return rc;
     if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (!c.batch && (rc = dalloc(c, &c.LU, nn))) ||

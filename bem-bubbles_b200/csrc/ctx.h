@@ -70,7 +70,6 @@ struct Ctx {
     double *x1 = nullptr, *xs = nullptr, *k1 = nullptr, *k2 = nullptr, *k3 = nullptr, *k4 = nullptr;
     double *p1 = nullptr, *ps = nullptr, *kp1 = nullptr, *kp2 = nullptr, *kp3 = nullptr, *kp4 = nullptr;
     double* vn = nullptr;  // N*3 vertex normals
-    double *srow = nullptr, *sb = nullptr;  // N: singular pairs' share of the H row sums and of H*phi
 
     // ---- solver work
     double* part = nullptr;        // GEMV partials, up to 64*N
