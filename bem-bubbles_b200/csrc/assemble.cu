@@ -333,11 +333,14 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
                                                   const double* __restrict__ x, const int* __restrict__ tri,
                                                   const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
                                                   const double* __restrict__ phi, double* __restrict__ G,
-                                                  double* __restrict__ H, double* __restrict__ b) {
+                                                  double* __restrict__ H, double* __restrict__ b,
+                                                  const double* __restrict__ x0, const double* __restrict__ gp,
+                                                  double* __restrict__ r0) {
     __shared__ int s_j[SD_WARPS][96];
     __shared__ double s_g[SD_WARPS][96], s_h[SD_WARPS][96];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double rs = 0.0, bsing = 0.0;  // (lane 0) the singular share of the H row sum and of H phi
+    double gx = 0.0;               // (x0) this lane's share of (G x0)_i
     const int e0 = csr_off[i], e1 = csr_off[i + 1];
     for (int base = e0; base < e1; base += 32) {
         const int e = base + lane;
@@ -371,13 +374,15 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
                 }
             if (!first) continue;
             const size_t o = (size_t)mbase + (size_t)(j - vbase) * n + il;
-            double gv = G[o], hv = MIRROR ? H[o] : 0.0;
+            double gv = G[o], hv = MIRROR ? H[o] : 0.0, gsing = 0.0;
             for (int q = me; q < ne; ++q)
                 if (s_j[w][q] == j) {
                     gv += s_g[w][q];
                     hv += s_h[w][q];
+                    gsing += s_g[w][q];
                 }
             G[o] = gv;
+            if (x0) gx = fma(gsing, x0[j], gx);
             if (MIRROR) H[o] = hv;  // without the wall image the singular double layer vanishes (flat triangle)
         }
         if (MIRROR && lane == 0)
@@ -395,10 +400,13 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
         val -= rowHp[(size_t)g * n + il];
         bs += bp[(size_t)g * n + il];
     }
+    if (x0)
+        for (int g = lane; g < ngroups; g += 32) gx += gp[(size_t)g * n + il];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         val += __shfl_xor_sync(0xffffffffu, val, o);
         bs += __shfl_xor_sync(0xffffffffu, bs, o);
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
     }
     if (lane) return;
     val -= rs;
@@ -406,7 +414,9 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
     const double d = -(4.0 * 3.14159265358979323846 - val);
     const size_t oii = (size_t)mbase + (size_t)il * n + il;
     H[oii] += d;  // after the warp's singular update of H(i, i) (ordered by the last __syncwarp)
-    if (b) b[i] = fma(d, phi[i], bs);
+    const double bi = fma(d, phi[i], bs);
+    if (b) b[i] = bi;
+    if (x0) r0[i] = bi - gx;  // the first residual b - G x0 of the solve that follows
 }
 
 template <bool MIRROR>
@@ -414,10 +424,11 @@ __global__ void __launch_bounds__(32 * SD_WARPS)
     k_singular_diag(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
                     const double* __restrict__ x, const int* __restrict__ tri, const int* __restrict__ csr_off,
                     const int* __restrict__ csr_idx, const double* __restrict__ phi, double* __restrict__ G,
-                    double* __restrict__ H, double* __restrict__ b) {
+                    double* __restrict__ H, double* __restrict__ b, const double* __restrict__ x0,
+                    const double* __restrict__ gp, double* __restrict__ r0) {
     const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
     if (i >= N) return;
-    singular_diag_row<MIRROR>(i, i, N, 0, 0, ngroups, rowHp, bp, x, tri, csr_off, csr_idx, phi, G, H, b);
+    singular_diag_row<MIRROR>(i, i, N, 0, 0, ngroups, rowHp, bp, x, tri, csr_off, csr_idx, phi, G, H, b, x0, gp, r0);
 }
 
 // The same per block of a batch (rows of block vblk[i], its own groups and G/H block).
@@ -432,7 +443,7 @@ __global__ void __launch_bounds__(32 * SD_WARPS)
     if (i >= N) return;
     const BlockInfo B = blk[vblk[i]];
     singular_diag_row<MIRROR>(i, i - B.vbase, B.n, B.mbase, B.vbase, B.ngroups, rowHp + B.pbase, bp + B.pbase, x,
-                              tri, csr_off, csr_idx, phi, G, H, b);
+                              tri, csr_off, csr_idx, phi, G, H, b, nullptr, nullptr, nullptr);
 }
 
 // Column-group tile: the columns of group g (local index gl within its block) for rows
@@ -448,7 +459,8 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
                                               double* __restrict__ G, double* __restrict__ H,
                                               double* __restrict__ rowHp, double* __restrict__ bp, int g, int gl,
                                               int row0, int rowend, int n, int vbase, long long mbase,
-                                              long long pbase) {
+                                              long long pbase, const double* __restrict__ x0,
+                                              double* __restrict__ gp) {
     double* accG = smem;                      // [CGT][ROWS]
     double* accH = accG + CGT * ROWS;         // [CGT][ROWS]
     double* srec = accH + CGT * ROWS;         // [ASM_TC][REC]
@@ -509,7 +521,7 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
     }
     if (i < rowend) {
         const int il = i - vbase;
-        double rs = 0.0, bs = 0.0;
+        double rs = 0.0, bs = 0.0, gs = 0.0;
         for (int s = 0; s < CGT; ++s) {
             int v = grp_vert[g * CGT + s];
             if (v < 0) continue;
@@ -519,9 +531,11 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
             H[o] = hv;
             rs += hv;
             bs = fma(hv, phi[v], bs);
+            if (x0) gs = fma(gv, x0[v], gs);
         }
         rowHp[(size_t)pbase + (size_t)gl * n + il] = rs;
         bp[(size_t)pbase + (size_t)gl * n + il] = bs;
+        if (x0) gp[(size_t)pbase + (size_t)gl * n + il] = gs;
     }
 }
 
@@ -532,10 +546,11 @@ __global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __
                                                          const int* __restrict__ grp_tri, const int* __restrict__ grp_slot,
                                                          const int* __restrict__ grp_vert, const double* __restrict__ phi,
                                                          double* __restrict__ G, double* __restrict__ H,
-                                                         double* __restrict__ rowHp, double* __restrict__ bp) {
+                                                         double* __restrict__ rowHp, double* __restrict__ bp,
+                                                         const double* __restrict__ x0, double* __restrict__ gp) {
     extern __shared__ __align__(16) double smem[];
     assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp, bp,
-                                     blockIdx.x, blockIdx.x, blockIdx.y * ROWS, N, N, 0, 0, 0);
+                                     blockIdx.x, blockIdx.x, blockIdx.y * ROWS, N, N, 0, 0, 0, x0, gp);
 }
 
 // Block-diagonal batch: one persistent launch over the work list of every block's tiles
@@ -563,7 +578,8 @@ __global__ void __launch_bounds__(ROWS, MINB)
         const int4 td = tiles[t];
         const BlockInfo B = blk[td.z];
         assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp,
-                                         bp, td.x, td.w, td.y, B.vbase + B.n, B.n, B.vbase, B.mbase, B.pbase);
+                                         bp, td.x, td.w, td.y, B.vbase + B.n, B.n, B.vbase, B.mbase, B.pbase, nullptr,
+                                         nullptr);
     }
 }
 
@@ -574,7 +590,8 @@ void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s) {
 }
 
 template <bool MIRROR, int CGT, int ROWS, int MINB>
-static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
+static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s,
+                           const double* x0) {
     const int N = (int)c.topo.N;
     const size_t sm = sizeof(double) * (2 * CGT * ROWS + ASM_TC * REC) + sizeof(int) * 4 * ASM_TC;
     static std::atomic<uint64_t> attr{0};
@@ -583,7 +600,8 @@ static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G
     dim3 grid(c.topo.ngroups, (N + ROWS - 1) / ROWS);
     KLAUNCH(), k_assemble<MIRROR, CGT, ROWS, MINB><<<grid, ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off,
                                                                           c.topo.grp_tri, c.topo.grp_slot,
-                                                                          c.topo.grp_vert, phi, G, H, c.rowHp, c.bp);
+                                                                          c.topo.grp_vert, phi, G, H, c.rowHp, c.bp, x0,
+                                                                          c.gp);
 }
 
 template <int CGT, int ROWS>
@@ -636,7 +654,8 @@ void prepare_assemble(Ctx& c) {
 }
 
 template <bool MIRROR>
-static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s) {
+static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, double* H, cudaStream_t s,
+                         const double* x0) {
     if (c.batch) {
         switch (c.topo.cg) {
             case 16:
@@ -655,21 +674,26 @@ static void launch_tiles(Ctx& c, const double* x, const double* phi, double* G, 
     }
     switch (c.topo.cg) {
         case 16:
-            launch_tiles_t<MIRROR, 16, 256, 3>(c, x, phi, G, H, s);
+            launch_tiles_t<MIRROR, 16, 256, 3>(c, x, phi, G, H, s, x0);
             break;
         case 64:
-            launch_tiles_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s);
+            launch_tiles_t<MIRROR, 64, 64, 3>(c, x, phi, G, H, s, x0);
             break;
         case 48:
-            launch_tiles_t<MIRROR, 48, 64, 3>(c, x, phi, G, H, s);
+            launch_tiles_t<MIRROR, 48, 64, 3>(c, x, phi, G, H, s, x0);
             break;
         default:
-            launch_tiles_t<MIRROR, 32, 128, 3>(c, x, phi, G, H, s);
+            launch_tiles_t<MIRROR, 32, 128, 3>(c, x, phi, G, H, s, x0);
     }
 }
 
-void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b, cudaStream_t s) {
+// x0, r0 (single systems, may be null): with x0 the assembly also returns r0 = b - G x0, the first
+// residual of a solve started from x0, from the G columns while they are in shared memory (per-group
+// partials of G x0 beside those of H phi).
+void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b, cudaStream_t s,
+                     const double* x0, double* r0) {
     const int N = (int)c.topo.N;
+    if (c.batch || !r0) x0 = nullptr;
     launch_triangle_records(c, x, s);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c.prof) {
@@ -678,9 +702,9 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
         cudaEventRecord(e0, s);
     }
     if (c.prm.mirror)
-        launch_tiles<true>(c, x, phi, G, H, s);
+        launch_tiles<true>(c, x, phi, G, H, s, x0);
     else
-        launch_tiles<false>(c, x, phi, G, H, s);
+        launch_tiles<false>(c, x, phi, G, H, s, x0);
     // singular pairs and the 4 pi rule, one warp per row
     const Topology& T = c.topo;
     const int nbs = (N + SD_WARPS - 1) / SD_WARPS, nt = 32 * SD_WARPS;
@@ -694,10 +718,10 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
     } else {
         if (c.prm.mirror)
             KLAUNCH(), k_singular_diag<true><<<nbs, nt, 0, s>>>(N, T.ngroups, c.rowHp, c.bp, x, T.tri, T.csr_off,
-                                                                T.csr_idx, phi, G, H, b);
+                                                                T.csr_idx, phi, G, H, b, x0, c.gp, r0);
         else
             KLAUNCH(), k_singular_diag<false><<<nbs, nt, 0, s>>>(N, T.ngroups, c.rowHp, c.bp, x, T.tri, T.csr_off,
-                                                                 T.csr_idx, phi, G, H, b);
+                                                                 T.csr_idx, phi, G, H, b, x0, c.gp, r0);
     }
     if (c.prof) {  // the profile's assembly time: tiles, singular pairs and the 4 pi rule
         cudaEventRecord(e1, s);

@@ -293,9 +293,14 @@ static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream
 // G, H and b = H*pot for positions x.  With pinned vertices (ColocSimPin::assemble_matrices,
 // ColocSimPin.cpp:25-118) the pinned columns are exchanged after the 4 pi rule and the right-hand
 // side takes pin_vals at the pinned vertices.
-static void assemble_system(Ctx& c, const double* x, const double* pot, const double* pin_vals, cudaStream_t s) {
+// x0 (may be null, no pinned vertices): the start value of the solve that follows; the assembly then
+// leaves its first residual b - G x0 in c.r (Ctx::r0_ready).
+static void assemble_system(Ctx& c, const double* x, const double* pot, const double* pin_vals, cudaStream_t s,
+                            const double* x0 = nullptr) {
+    c.r0_ready = false;
     if (c.n_pin == 0) {
-        launch_assemble(c, x, pot, c.G, c.H, c.b, s);
+        launch_assemble(c, x, pot, c.G, c.H, c.b, s, x0, x0 ? c.r : nullptr);
+        c.r0_ready = x0 != nullptr && !c.batch;
         return;
     }
     launch_pin_zero(c, pot, c.potz, s);
@@ -310,9 +315,10 @@ static void assemble_system(Ctx& c, const double* x, const double* pot, const do
 // stage >= 0: an RK4 stage of the mixed solver's step loop, whose start value comes from the stage
 // predictor and whose solution goes into its history.
 static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStream_t s, int stage = -1) {
-    assemble_system(c, x, pot, c.psi, s);
-    if (stage >= 0) launch_stage_predict(c, stage, c.psil, s);
+    if (stage >= 0) launch_stage_predict(c, stage, c.psil, s);  // needs no G: before the assembly
+    assemble_system(c, x, pot, c.psi, s, stage >= 0 ? c.psil : nullptr);
     int rc = solve(c, c.G, c.b, c.psil, s);
+    c.r0_ready = false;
     if (rc) return rc;
     if (stage >= 0) launch_stage_store(c, stage, c.psil, s);
     launch_velocity_prep(c, x, pot, s);
@@ -479,7 +485,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     if ((rc = dalloc(c, &c.G, nn)) || (rc = dalloc(c, &c.H, nn)) || (!c.batch && (rc = dalloc(c, &c.LU, nn))) ||
         (rc = dalloc(c, &c.rec, m * REC)) || (rc = dalloc(c, &c.tn, 3 * m)) || (rc = dalloc(c, &c.tg, 3 * m)) ||
         (rc = dalloc(c, &c.tk, m)) || (rc = dalloc(c, &c.rowHp, nrow_part)) ||
-        (rc = dalloc(c, &c.bp, nrow_part)) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
+        (rc = dalloc(c, &c.bp, nrow_part)) || (!c.batch && (rc = dalloc(c, &c.gp, nrow_part))) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
         (rc = dalloc(c, &c.vol_part, (size_t)h.nparts * 64)) || (rc = dalloc(c, &c.vol_cnt, (size_t)h.nparts)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
         (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||

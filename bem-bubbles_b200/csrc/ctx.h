@@ -70,6 +70,8 @@ struct Ctx {
     double *x1 = nullptr, *xs = nullptr, *k1 = nullptr, *k2 = nullptr, *k3 = nullptr, *k4 = nullptr;
     double *p1 = nullptr, *ps = nullptr, *kp1 = nullptr, *kp2 = nullptr, *kp3 = nullptr, *kp4 = nullptr;
     double* vn = nullptr;  // N*3 vertex normals
+    double* gp = nullptr;  // per-group partials of G x0 (the assembly's fused first residual)
+    bool r0_ready = false; // c.r holds b - G x for the start value of the next mixed solve
 
     // ---- solver work
     double* part = nullptr;        // GEMV partials, up to 64*N

@@ -96,7 +96,8 @@ struct QuadTables {
 void quad_tables(QuadTables& t);
 void launch_triangle_records(Ctx& c, const double* x, cudaStream_t s);
 void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, double* H, double* b,
-                     cudaStream_t s);
+                     cudaStream_t s, const double* x0 = nullptr,
+                     double* r0 = nullptr);
 void prepare_assemble(Ctx& c);  // kernel attributes and the persistent grid, outside any capture
 
 // stage.cu

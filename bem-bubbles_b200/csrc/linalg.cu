@@ -1114,11 +1114,15 @@ static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cu
 int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
     const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
+    // the assembly already left r = b - A x for this start value in c.r (a stage of the step loop)
+    bool r0_ready = c.r0_ready;
+    c.r0_ready = false;
     if (c.mixed_backoff > 0) {
         --c.mixed_backoff;
         return fp64_fallback(c, A, b, x, s, false);
     }
     if (!c.xinv_valid) {
+        r0_ready = false;  // the set-up uses c.r as scratch
         int rc = refresh_inverse(c, A, s, true);
         if (rc == BEM_ERR_NOT_CONVERGED) return fp64_fallback(c, A, b, x, s, true);
         if (rc) return rc;
@@ -1144,7 +1148,11 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     bool converged = false;
     for (int round = 0; round < 4; ++round) {
         for (int k = 0; k < K; ++k) {
-            gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr, nullptr, b, -1.0);
+            if (round == 0 && k == 0 && r0_ready)
+                KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, c.r, pr);
+            else
+                gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr, nullptr, b,
+                               -1.0);
             gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, nullptr, 0, nullptr, nullptr, nullptr, nullptr, x, 1.0);
         }
         gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b, -1.0);

@@ -278,10 +278,11 @@ def test_negative_x_leaves_the_state_untouched():
 
 
 def test_stage_predictor_keeps_the_trajectory():
-    # the mixed solver starts each RK4 stage from an extrapolation of the same stage of earlier steps;
-    # any start converges to the same FP64 solution, so the trajectory equals the one started from
-    # the previous stage (BEM_FLAG_NO_STAGE_PREDICTOR), also after the state is pushed back unchanged
-    # (history kept) or changed (history dropped), and with an adaptive step
+    # the mixed solver starts each RK4 stage from an extrapolation of the same stage of earlier steps,
+    # with the first residual b - G x0 formed by the assembly; any start converges to the same FP64
+    # solution, so the trajectory equals the one started from the previous stage with the residual
+    # from a GEMV (BEM_FLAG_NO_STAGE_PREDICTOR), also after the state is pushed back unchanged (history
+    # kept) or changed (history dropped), and with an adaptive step
     from bem_b200 import _lib as L
     v, f = mesh.bubble(8, 1.0, (2.0, 0.0, 0.0))
     rng = np.random.default_rng(3)
