@@ -320,9 +320,8 @@ static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStr
     int rc = solve(c, c.G, c.b, c.psil, s);
     c.r0_ready = false;
     if (rc) return rc;
-    if (stage >= 0) launch_stage_store(c, stage, c.psil, s);
     launch_velocity_prep(c, x, pot, s);
-    launch_velocity(c, c.psil, vel, s);
+    launch_velocity(c, c.psil, vel, s, stage);  // and, for a predicted stage, the history entry
     if (c.n_pin) launch_pin_finish(c, x, vel, pot, s);
     return BEM_OK;
 }
@@ -404,16 +403,13 @@ static int rk4_stages(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* 
     else
         launch_get_dt(c, c.k1, c.kp1, dp, s);
     const double* dtp = &c.sc->dt;
-    launch_axpy3(3 * N, c.x1, dtp, 0.5, c.k1, c.xs, s);
-    launch_axpy3(N, c.p1, dtp, 0.5, c.kp1, c.ps, s);
+    launch_axpy_stage(c, c.k1, c.kp1, dtp, 0.5, s);
     if ((rc = position_t(c, c.xs, c.ps, c.k2, s, st2))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k2, c.kp2, s))) return rc;
-    launch_axpy3(3 * N, c.x1, dtp, 0.5, c.k2, c.xs, s);
-    launch_axpy3(N, c.p1, dtp, 0.5, c.kp2, c.ps, s);
+    launch_axpy_stage(c, c.k2, c.kp2, dtp, 0.5, s);
     if ((rc = position_t(c, c.xs, c.ps, c.k3, s, st3))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k3, c.kp3, s))) return rc;
-    launch_axpy3(3 * N, c.x1, dtp, 1.0, c.k3, c.xs, s);
-    launch_axpy3(N, c.p1, dtp, 1.0, c.kp3, c.ps, s);
+    launch_axpy_stage(c, c.k3, c.kp3, dtp, 1.0, s);
     if ((rc = position_t(c, c.xs, c.ps, c.k4, s, st4))) return rc;
     if ((rc = pot_t_multi(c, c.xs, c.k4, c.kp4, s))) return rc;
     launch_rk4_final(c, s, skip);

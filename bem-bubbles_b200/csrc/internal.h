@@ -102,21 +102,24 @@ void prepare_assemble(Ctx& c);  // kernel attributes and the persistent grid, ou
 
 // stage.cu
 void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s);
-void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s);
+// stage >= 0: psil also goes into the stage predictor's history (the stage's solution)
+void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s, int stage = -1);
 void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* field_host, double* out,
                   cudaStream_t s);
 void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s);
+// xs = x1 + scale dt kx and ps = p1 + scale dt kp (an RK4 stage's state) in one launch
+void launch_axpy_stage(Ctx& c, const double* kx, const double* kp, const double* coef_dev, double scale,
+                       cudaStream_t s);
 void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k,
                   double* out, cudaStream_t s);
 void launch_rk4_final(Ctx& c, cudaStream_t s, const int* skip = nullptr);
 // Stage predictor of the mixed solve (stage.cu): depth of the history; the ring's stage times hold
 // at PRED_CNT the number of steps that continue the current trajectory.  Start value of stage
-// `stage` (0..3) extrapolated from the ring, the stage's solution stored into it, the end of a step;
+// `stage` (0..3) extrapolated from the ring (launch_velocity stores the stage's solution), the end of a step;
 // state copies that end the trajectory when a value changes.
 constexpr int PRED_DEPTH = 3;
 constexpr int PRED_CNT = PRED_DEPTH * 4;
 void launch_stage_predict(Ctx& c, int stage, double* x, cudaStream_t s);
-void launch_stage_store(Ctx& c, int stage, const double* x, cudaStream_t s);
 void launch_stage_advance(Ctx& c, const int* skip, cudaStream_t s);
 void launch_state_accept(Ctx& c, int64_t n, const double* src, double* dst, cudaStream_t s);
 void launch_time_accept(Ctx& c, double t, cudaStream_t s);

@@ -1092,6 +1092,18 @@ __global__ void k_rowblock_norm2(int n, const double* __restrict__ b, double* __
     v = block_sum(v);
     if (threadIdx.x == 0) part[blockIdx.x] = v;
 }
+// the same for two vectors in one launch (||b||^2 and the first residual's)
+__global__ void k_rowblock_norm2x2(int n, const double* __restrict__ b, double* __restrict__ pb,
+                                   const double* __restrict__ r, double* __restrict__ pr) {
+    const int i = blockIdx.x * GV_ROWS + threadIdx.x;
+    double v = (i < n) ? b[i] * b[i] : 0.0, w = (i < n) ? r[i] * r[i] : 0.0;
+    v = block_sum(v);
+    w = block_sum(w);
+    if (threadIdx.x == 0) {
+        pb[blockIdx.x] = v;
+        pr[blockIdx.x] = w;
+    }
+}
 
 // Mixed solve.  Iterative refinement x <- x + X (b - G x): the residual in FP64 against the FP64 G
 // (so the limit is the FP64 solution), the correction through the FP32 approximate inverse X.
@@ -1131,7 +1143,10 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     constexpr int KMAX = 12;
     double* pb = c.red;        // nrb
     double* pr = c.red + nrb;  // (KMAX+1)*nrb
-    KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb);
+    if (r0_ready)
+        KLAUNCH(), k_rowblock_norm2x2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb, c.r, pr);
+    else
+        KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb);
     // the norms come back through pinned memory: a direct DMA the host sees as soon as it lands
     const size_t nh = (size_t)(KMAX + 2) * nrb;
     if (c.h_red_cap < nh) {
@@ -1148,9 +1163,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     bool converged = false;
     for (int round = 0; round < 4; ++round) {
         for (int k = 0; k < K; ++k) {
-            if (round == 0 && k == 0 && r0_ready)
-                KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, c.r, pr);
-            else
+            if (!(round == 0 && k == 0 && r0_ready))  // else the residual and its norms are there
                 gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr, nullptr, b,
                                -1.0);
             gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, nullptr, 0, nullptr, nullptr, nullptr, nullptr, x, 1.0);

@@ -46,11 +46,16 @@ __global__ void k_velocity_prep(int M, const double* __restrict__ x, const int* 
 
 // vertex gradient = mean over incident triangles of (tangent gradient + psi_i * normal)
 // (LinLinSim.cpp:48-59)
+// hist (may be null): the stage predictor's history row that receives psil, with the stage time
+// t + c_s dt in *htime (one launch for both).
 __global__ void k_velocity(int N, const int* __restrict__ off, const int* __restrict__ idx,
                            const double* __restrict__ tn, const double* __restrict__ tg,
-                           const double* __restrict__ psil, double* __restrict__ vel) {
+                           const double* __restrict__ psil, double* __restrict__ vel, double* __restrict__ hist,
+                           double* __restrict__ htime, double cs, const DevScalars* __restrict__ sc) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (hist && i == 0) *htime = sc->time + cs * sc->dt;
     if (i >= N) return;
+    if (hist) hist[i] = psil[i];
     double gx = 0, gy = 0, gz = 0, num = 0;
     const double p = psil[i];
     for (int e = off[i]; e < off[i + 1]; ++e) {
@@ -146,6 +151,19 @@ __global__ void k_axpy_dev(int64_t n, const double* __restrict__ a, const double
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     out[i] = a[i] + (scale * *coef) * k[i];
+}
+
+// The positions and the potential of an RK4 stage in one launch: xs = x1 + scale dt kx (3N),
+// ps = p1 + scale dt kp (N).
+__global__ void k_axpy_stage(int N, const double* __restrict__ x1, const double* __restrict__ kx,
+                             double* __restrict__ xs, const double* __restrict__ p1, const double* __restrict__ kp,
+                             double* __restrict__ ps, const double* __restrict__ coef, double scale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double h = scale * *coef;
+    if (i < 3 * N)
+        xs[i] = x1[i] + h * kx[i];
+    else if (i < 4 * N)
+        ps[i - 3 * N] = p1[i - 3 * N] + h * kp[i - 3 * N];
 }
 
 // RK4 combination, phi update and nopenetration (LinLinSim.cpp:236-253, 162-190).
@@ -247,9 +265,26 @@ static inline int nb(int64_t n, int t) { return (int)((n + t - 1) / t); }
 void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s) {
     KLAUNCH(), k_velocity_prep<<<nb(c.topo.M, 128), 128, 0, s>>>((int)c.topo.M, x, c.topo.tri, pot, c.tn, c.tg);
 }
-void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s) {
+// ring row of stage `stage` in the step `back` steps before the current one (back = 0: the current)
+static int pred_row(const Ctx& c, int back, int stage) {
+    return ((c.pred_head - back + 2 * PRED_DEPTH) % PRED_DEPTH) * 4 + stage;
+}
+
+// The current step's history row of stage `stage`, its time slot and the stage's offset c_s.
+static void stage_history_row(Ctx& c, int stage, double** hist, double** htime, double* cs) {
+    static const double stage_c[4] = {0.0, 0.5, 0.5, 1.0};
+    const int row = pred_row(c, 0, stage);
+    *hist = c.psih + (size_t)row * c.topo.N;
+    *htime = c.psih_t + row;
+    *cs = stage_c[stage];
+}
+
+void launch_velocity(Ctx& c, const double* psil, double* vel, cudaStream_t s, int stage) {
+    double *hist = nullptr, *htime = nullptr;
+    double cs = 0.0;
+    if (stage >= 0) stage_history_row(c, stage, &hist, &htime, &cs);
     KLAUNCH(), k_velocity<<<nb(c.topo.N, 128), 128, 0, s>>>((int)c.topo.N, c.topo.csr_off, c.topo.csr_idx, c.tn, c.tg, psil,
-                                                  vel);
+                                                            vel, hist, htime, cs, c.sc);
 }
 void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s) {
     // chunks per part: enough for the largest part (the kernel exits early in smaller parts)
@@ -274,6 +309,11 @@ void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* fiel
 void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k, double* out,
                   cudaStream_t s) {
     KLAUNCH(), k_axpy_dev<<<nb(n, 256), 256, 0, s>>>(n, a, coef_dev, scale, k, out);
+}
+void launch_axpy_stage(Ctx& c, const double* kx, const double* kp, const double* coef_dev, double scale,
+                       cudaStream_t s) {
+    const int N = (int)c.topo.N;
+    KLAUNCH(), k_axpy_stage<<<nb(4 * (int64_t)N, 256), 256, 0, s>>>(N, c.x1, kx, c.xs, c.p1, kp, c.ps, coef_dev, scale);
 }
 // skip (device flag, may be null): when set, the step leaves x, phi, psi and time untouched
 void launch_rk4_final(Ctx& c, cudaStream_t s, const int* skip) {
@@ -330,13 +370,6 @@ __global__ void k_stage_predict(int N, const double* __restrict__ hist, const do
     x[i] = v;
 }
 
-__global__ void k_stage_store(int N, double* __restrict__ hist, double* __restrict__ ht, int row, int stage,
-                              const DevScalars* __restrict__ sc, const double* __restrict__ x) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) ht[row] = sc->time + c_stage_c[stage] * sc->dt;
-    if (i < N) hist[(size_t)row * N + i] = x[i];
-}
-
 // End of a step: one more step in the ring, or none when the step's final update was skipped.
 __global__ void k_stage_advance(double* ht, const int* skip) {
     ht[PRED_CNT] = (skip && *skip) ? 0.0 : fmin(ht[PRED_CNT] + 1.0, (double)PRED_DEPTH);
@@ -355,20 +388,11 @@ __global__ void k_time_accept(double t, DevScalars* sc, double* ht) {
     sc->time = t;
 }
 
-// ring row of stage `stage` in the step `back` steps before the current one (back = 0: the current)
-static int pred_row(const Ctx& c, int back, int stage) {
-    return ((c.pred_head - back + 2 * PRED_DEPTH) % PRED_DEPTH) * 4 + stage;
-}
 
 void launch_stage_predict(Ctx& c, int stage, double* x, cudaStream_t s) {
     const int N = (int)c.topo.N;
     KLAUNCH(), k_stage_predict<<<nb(N, 256), 256, 0, s>>>(N, c.psih, c.psih_t, pred_row(c, 1, stage),
                                                           pred_row(c, 2, stage), pred_row(c, 3, stage), stage, c.sc, x);
-}
-
-void launch_stage_store(Ctx& c, int stage, const double* x, cudaStream_t s) {
-    const int N = (int)c.topo.N;
-    KLAUNCH(), k_stage_store<<<nb(N, 256), 256, 0, s>>>(N, c.psih, c.psih_t, pred_row(c, 0, stage), stage, c.sc, x);
 }
 
 void launch_stage_advance(Ctx& c, const int* skip, cudaStream_t s) {

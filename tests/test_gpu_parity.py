@@ -54,6 +54,42 @@ def test_assembly_nu10_matches_oracle_and_is_reproducible():
     assert rel(G, Go) < 1e-13 and rel(H, Ho) < 1e-13
 
 
+def _uv_sphere(nlon, nlat, center):
+    # closed UV sphere, outward orientation; the two poles have valence nlon
+    v = [[0.0, 0.0, 1.0]]
+    for a in range(1, nlat):
+        th = np.pi * a / nlat
+        for o in range(nlon):
+            ph = 2 * np.pi * o / nlon
+            v.append([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+    v.append([0.0, 0.0, -1.0])
+    f = []
+    ring = lambda a, o: 1 + (a - 1) * nlon + o % nlon
+    for o in range(nlon):
+        f.append([0, ring(1, o), ring(1, o + 1)])
+        for a in range(1, nlat - 1):
+            f.append([ring(a, o), ring(a + 1, o), ring(a + 1, o + 1)])
+            f.append([ring(a, o), ring(a + 1, o + 1), ring(a, o + 1)])
+        f.append([ring(nlat - 1, o), len(v) - 1, ring(nlat - 1, o + 1)])
+    return np.array(v) + np.array(center), np.array(f, dtype=np.int64)
+
+
+@pytest.mark.parametrize("mirror", [0, 1])
+def test_assembly_high_valence_vertex_matches_oracle(mirror):
+    # poles of valence 40: the singular pass takes the triangles around a vertex 32 at a time, so a
+    # ring of 40 spans two chunks; G, H and the right-hand side against the oracle
+    v, f = _uv_sphere(40, 9, (2.0, 0.0, 0.0))
+    assert mesh.signed_volume(v, f) > 0
+    sim = ColocSim(v, f, mirror=bool(mirror))
+    G, H = sim.assemble_matrices()
+    Go, Ho = O.assemble(v, f, mirror=bool(mirror))
+    assert rel(G, Go) < 1e-13 and rel(H, Ho) < 1e-13
+    # the fused right-hand side: psi from the device solve against the oracle's matrices
+    phi = 0.1 * np.sin(2 * v[:, 2]) + 0.05 * v[:, 1]
+    _, psi = sim.position_t(phi, return_psi=True)
+    assert rel(psi, np.linalg.solve(Go, Ho @ phi)) < 1e-10
+
+
 @pytest.mark.parametrize("cg", ["16", "32", "48", "64"])
 def test_assembly_tile_shapes_agree(cg, monkeypatch):
     # every column-group width of the tile kernel gives the same matrices (two bubbles, nu=7)
