@@ -313,7 +313,8 @@ def test_negative_x_leaves_the_state_untouched():
     assert np.array_equal(gx, x) and np.array_equal(gp, phi) and np.all(gs == 0.0) and gt == 1.0
 
 
-def test_stage_predictor_keeps_the_trajectory():
+@pytest.mark.parametrize("mirror", [False, True])
+def test_stage_predictor_keeps_the_trajectory(mirror):
     # the mixed solver starts each RK4 stage from an extrapolation of the same stage of earlier steps,
     # with the first residual b - G x0 formed by the assembly; any start converges to the same FP64
     # solution, so the trajectory equals the one started from the previous stage with the residual
@@ -323,7 +324,8 @@ def test_stage_predictor_keeps_the_trajectory():
     v, f = mesh.bubble(8, 1.0, (2.0, 0.0, 0.0))
     rng = np.random.default_rng(3)
     v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None]
-    sims = [ColocSim(v, f, pressurefield=(-0.8, 2 * np.pi / 5, 0.0), solver="mixed") for _ in range(2)]
+    sims = [ColocSim(v, f, pressurefield=(-0.8, 2 * np.pi / 5, 0.0), solver="mixed", mirror=mirror)
+            for _ in range(2)]
     sims[1]._update(flags=L.FLAG_NO_STAGE_PREDICTOR)
     for sim in sims:
         sim.set_phi(0.0)
