@@ -396,12 +396,13 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
     // 4 pi rule and right-hand side: lane l sums the partials of groups l, l+32, ... and the warp adds
     // the lane sums in a fixed butterfly order (deterministic)
     double val = 0.0, bs = 0.0;
+    const size_t pr = (size_t)il * ngroups;  // the row's partials, contiguous
     for (int g = lane; g < ngroups; g += 32) {
-        val -= rowHp[(size_t)g * n + il];
-        bs += bp[(size_t)g * n + il];
+        val -= rowHp[pr + g];
+        bs += bp[pr + g];
     }
     if (x0)
-        for (int g = lane; g < ngroups; g += 32) gx += gp[(size_t)g * n + il];
+        for (int g = lane; g < ngroups; g += 32) gx += gp[pr + g];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         val += __shfl_xor_sync(0xffffffffu, val, o);
@@ -459,7 +460,7 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
                                               double* __restrict__ G, double* __restrict__ H,
                                               double* __restrict__ rowHp, double* __restrict__ bp, int g, int gl,
                                               int row0, int rowend, int n, int vbase, long long mbase,
-                                              long long pbase, const double* __restrict__ x0,
+                                              long long pbase, int ngrp, const double* __restrict__ x0,
                                               double* __restrict__ gp) {
     double* accG = smem;                      // [CGT][ROWS]
     double* accH = accG + CGT * ROWS;         // [CGT][ROWS]
@@ -533,9 +534,12 @@ __device__ __forceinline__ void assemble_tile(double* smem, const double* __rest
             bs = fma(hv, phi[v], bs);
             if (x0) gs = fma(gv, x0[v], gs);
         }
-        rowHp[(size_t)pbase + (size_t)gl * n + il] = rs;
-        bp[(size_t)pbase + (size_t)gl * n + il] = bs;
-        if (x0) gp[(size_t)pbase + (size_t)gl * n + il] = gs;
+        // row-major partials (row il, group gl of ngrp): the reduction over groups then reads each
+        // row's partials as one contiguous run
+        const size_t po = (size_t)pbase + (size_t)il * ngrp + gl;
+        rowHp[po] = rs;
+        bp[po] = bs;
+        if (x0) gp[po] = gs;
     }
 }
 
@@ -550,7 +554,7 @@ __global__ void __launch_bounds__(ROWS, MINB) k_assemble(int N, const double* __
                                                          const double* __restrict__ x0, double* __restrict__ gp) {
     extern __shared__ __align__(16) double smem[];
     assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp, bp,
-                                     blockIdx.x, blockIdx.x, blockIdx.y * ROWS, N, N, 0, 0, 0, x0, gp);
+                                     blockIdx.x, blockIdx.x, blockIdx.y * ROWS, N, N, 0, 0, 0, gridDim.x, x0, gp);
 }
 
 // Block-diagonal batch: one persistent launch over the work list of every block's tiles
@@ -578,8 +582,8 @@ __global__ void __launch_bounds__(ROWS, MINB)
         const int4 td = tiles[t];
         const BlockInfo B = blk[td.z];
         assemble_tile<MIRROR, CGT, ROWS>(smem, x, tri, rec, grp_off, grp_tri, grp_slot, grp_vert, phi, G, H, rowHp,
-                                         bp, td.x, td.w, td.y, B.vbase + B.n, B.n, B.vbase, B.mbase, B.pbase, nullptr,
-                                         nullptr);
+                                         bp, td.x, td.w, td.y, B.vbase + B.n, B.n, B.vbase, B.mbase, B.pbase, B.ngroups,
+                                         nullptr, nullptr);
     }
 }
 
