@@ -263,26 +263,28 @@ __global__ void k_total_volume(const double* vol, int np, double* out) {
 }
 
 // ---------------------------------------------------------------- stage building blocks
-static int solve_impl(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+static int solve_impl(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s, SolveTail* tail) {
     if (c.batch) return batch_mixed_solve(c, A, b, x, s);
     switch (c.prm.solver) {
         case BEM_SOLVER_LU:
             return lu_solve(c, A, b, x, s);
         case BEM_SOLVER_MIXED:
-            return mixed_solve(c, A, b, x, s);
+            return mixed_solve(c, A, b, x, s, tail);
         default:
             return bicgstab(c, A, b, x, s);
     }
 }
 
-static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+// tail (may be null): see SolveTail; with profiling on, the solve's time then includes the tail's
+// kernels, which the first round's readback overlaps.
+static int solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s, SolveTail* tail = nullptr) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c.prof) {
         e0 = c.take_event();
         e1 = c.take_event();
         cudaEventRecord(e0, s);
     }
-    int rc = solve_impl(c, A, b, x, s);
+    int rc = solve_impl(c, A, b, x, s, tail);
     if (c.prof) {
         cudaEventRecord(e1, s);
         c.ev_solve.emplace_back(e0, e1);
@@ -313,17 +315,29 @@ static void assemble_system(Ctx& c, const double* x, const double* pot, const do
 // vertices take the drift velocity, and pot receives the solved potential there (pot is in/out, as
 // the reference's PotVec& argument).
 // stage >= 0: an RK4 stage of the mixed solver's step loop, whose start value comes from the stage
-// predictor and whose solution goes into its history.
-static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStream_t s, int stage = -1) {
+// predictor and whose solution goes into its history.  after (may be null): more work on the
+// solution (the stage's Dphi/Dt), enqueued with the velocity.  With the mixed solver, no pinned
+// vertices (whose finishing step writes pot, an input of the velocity) and no field callback (which
+// waits for the host), the velocity and `after` are enqueued behind the solve's first round and run
+// while the host waits for its norms; they are enqueued again if the solution changes after that.
+static int position_t(Ctx& c, const double* x, double* pot, double* vel, cudaStream_t s, int stage = -1,
+                      const std::function<int()>* after = nullptr) {
     if (stage >= 0) launch_stage_predict(c, stage, c.psil, s);  // needs no G: before the assembly
     assemble_system(c, x, pot, c.psi, s, stage >= 0 ? c.psil : nullptr);
-    int rc = solve(c, c.G, c.b, c.psil, s);
+    SolveTail tail;
+    tail.run = [&]() -> int {
+        launch_velocity_prep(c, x, pot, s);
+        launch_velocity(c, c.psil, vel, s, stage);  // and, for a predicted stage, the history entry
+        if (c.n_pin) launch_pin_finish(c, x, vel, pot, s);
+        return after ? (*after)() : BEM_OK;
+    };
+    const bool overlap = after && c.prm.solver == BEM_SOLVER_MIXED && !c.batch && !c.n_pin && !c.field_cb;
+    c.solve_stage = stage;
+    int rc = solve(c, c.G, c.b, c.psil, s, overlap ? &tail : nullptr);
+    c.solve_stage = -1;
     c.r0_ready = false;
     if (rc) return rc;
-    launch_velocity_prep(c, x, pot, s);
-    launch_velocity(c, c.psil, vel, s, stage);  // and, for a predicted stage, the history entry
-    if (c.n_pin) launch_pin_finish(c, x, vel, pot, s);
-    return BEM_OK;
+    return tail.done ? BEM_OK : tail.run();
 }
 
 // Field values for the callback form: positions back to the host, one call per vertex.
@@ -395,23 +409,28 @@ static int rk4_stages(Ctx& c, double dp, bool fixdt, cudaStream_t s, const int* 
     const int64_t N = c.topo.N;
     BEM_CUDA(c, cudaMemcpyAsync(c.x1, c.x, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemcpyAsync(c.p1, c.phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
-    int rc = position_t(c, c.x1, c.p1, c.k1, s, st1);
+    // each stage's Dphi/Dt (and the first stage's dt) go with its velocity (position_t's `after`)
+    const std::function<int()> after1 = [&]() -> int {
+        int r = pot_t_multi(c, c.x1, c.k1, c.kp1, s);
+        if (r) return r;
+        if (fixdt)
+            KLAUNCH(), k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
+        else
+            launch_get_dt(c, c.k1, c.kp1, dp, s);
+        return BEM_OK;
+    };
+    const std::function<int()> after2 = [&]() { return pot_t_multi(c, c.xs, c.k2, c.kp2, s); };
+    const std::function<int()> after3 = [&]() { return pot_t_multi(c, c.xs, c.k3, c.kp3, s); };
+    const std::function<int()> after4 = [&]() { return pot_t_multi(c, c.xs, c.k4, c.kp4, s); };
+    int rc = position_t(c, c.x1, c.p1, c.k1, s, st1, &after1);
     if (rc) return rc;
-    if ((rc = pot_t_multi(c, c.x1, c.k1, c.kp1, s))) return rc;
-    if (fixdt)
-        KLAUNCH(), k_set_dt<<<1, 1, 0, s>>>(c.sc, dp);
-    else
-        launch_get_dt(c, c.k1, c.kp1, dp, s);
     const double* dtp = &c.sc->dt;
     launch_axpy_stage(c, c.k1, c.kp1, dtp, 0.5, s);
-    if ((rc = position_t(c, c.xs, c.ps, c.k2, s, st2))) return rc;
-    if ((rc = pot_t_multi(c, c.xs, c.k2, c.kp2, s))) return rc;
+    if ((rc = position_t(c, c.xs, c.ps, c.k2, s, st2, &after2))) return rc;
     launch_axpy_stage(c, c.k2, c.kp2, dtp, 0.5, s);
-    if ((rc = position_t(c, c.xs, c.ps, c.k3, s, st3))) return rc;
-    if ((rc = pot_t_multi(c, c.xs, c.k3, c.kp3, s))) return rc;
+    if ((rc = position_t(c, c.xs, c.ps, c.k3, s, st3, &after3))) return rc;
     launch_axpy_stage(c, c.k3, c.kp3, dtp, 1.0, s);
-    if ((rc = position_t(c, c.xs, c.ps, c.k4, s, st4))) return rc;
-    if ((rc = pot_t_multi(c, c.xs, c.k4, c.kp4, s))) return rc;
+    if ((rc = position_t(c, c.xs, c.ps, c.k4, s, st4, &after4))) return rc;
     launch_rk4_final(c, s, skip);
     return BEM_OK;
 }
@@ -574,6 +593,7 @@ int bem_destroy(bem_ctx* c) {
     cudaFree(c->trace_buf);
     cudaFreeHost(c->h_stage);
     if (c->stage_ev) cudaEventDestroy(c->stage_ev);
+    if (c->solve_ev) cudaEventDestroy(c->solve_ev);
     cudaFree(c->sc);
     cudaFree(c->flag);
     cudaFreeHost(c->h_sc);

@@ -100,6 +100,12 @@ struct Ctx {
     int ir_base = -1;       // fewest refinement steps of a solve since the last refresh of X
     int ir_excess = 0;      // refinement steps paid above ir_base since the last refresh
     int ir_steps = 3;  // refinement steps issued per round of the mixed solve (adapted)
+    // the same per RK4 stage of the step loop (stages differ in how good their start values are), and
+    // whether that stage's last solve converged in its first round (then its consumers are enqueued
+    // behind that round, see SolveTail); solve_stage: the stage of the current solve, or -1
+    int ir_steps_stage[4] = {3, 3, 3, 3};
+    bool stage_round0[4] = {false, false, false, false};
+    int solve_stage = -1;
     // Stage predictor of the mixed solve (single systems): the solutions of the RK4 stages of the last
     // PRED_DEPTH steps and the stage times, a ring over steps (pred_head: the slot the current step
     // writes, which holds the oldest step until then).  psih_t[PRED_CNT]: steps in the ring that
@@ -157,6 +163,7 @@ struct Ctx {
     double* h_stage = nullptr;
     size_t stage_cap = 0;
     cudaEvent_t stage_ev = nullptr;
+    cudaEvent_t solve_ev = nullptr;  // end of the mixed solve's first-round norm readback
 
     // remesh ray casting (remesh.cu): one device buffer, grown on demand, kept across meshes
     void* trace_buf = nullptr;

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -173,7 +174,15 @@ void gemv(int64_t n, const double* A, const double* x, double* y, cudaStream_t s
           unsigned* counters);
 int bicgstab(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
 int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
-int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s);
+// Work that follows a solve and reads only its solution (an RK4 stage's velocity and Dphi/Dt).  The
+// mixed solve enqueues it behind its first round of refinement steps, before the host waits for
+// that round's residual norms, so the GPU runs it while the host decides; done says whether the
+// enqueued work saw the final solution (else the caller enqueues it again).
+struct SolveTail {
+    std::function<int()> run;
+    bool done = false;
+};
+int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s, SolveTail* tail = nullptr);
 
 int mixed_refresh(Ctx& c, const double* A, cudaStream_t s, bool from_scratch);
 

@@ -1123,7 +1123,7 @@ static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cu
     return bicgstab(c, A, b, x, s);
 }
 
-int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
+int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s, SolveTail* tail) {
     const int n = (int)c.topo.N;
     const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
     // the assembly already left r = b - A x for this start value in c.r (a stage of the step loop)
@@ -1158,10 +1158,17 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     }
     double* host = c.h_red;
     c.stats.last_iters = 0;
-    int K = std::max(1, std::min(KMAX, c.ir_steps));
+    const int st = c.solve_stage;
+    int& ir_steps = st >= 0 ? c.ir_steps_stage[st] : c.ir_steps;
+    int K = std::max(1, std::min(KMAX, ir_steps));
+    if (tail && st >= 0 && !c.stage_round0[st]) tail = nullptr;  // not likely final after one round
+    bool tail_valid = false;  // the tail was enqueued and x has not changed since
     double rho = 1.0, rel = 1.0, rel0 = -1.0;
     bool converged = false;
+    int rounds = 0;
     for (int round = 0; round < 4; ++round) {
+        ++rounds;
+        tail_valid = false;  // a round changes x
         for (int k = 0; k < K; ++k) {
             if (!(round == 0 && k == 0 && r0_ready))  // else the residual and its norms are there
                 gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr, nullptr, b,
@@ -1170,11 +1177,21 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         }
         gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b, -1.0);
         BEM_CUDA(c, cudaMemcpyAsync(host, c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
-        BEM_CUDA(c, cudaStreamSynchronize(s));
+        if (round == 0 && tail) {  // the solution's consumers, speculatively: x is final if this round converges
+            if (!c.solve_ev) BEM_CUDA(c, cudaEventCreateWithFlags(&c.solve_ev, cudaEventDisableTiming));
+            BEM_CUDA(c, cudaEventRecord(c.solve_ev, s));
+            const int trc = tail->run();
+            if (trc) return trc;
+            tail_valid = true;
+            BEM_CUDA(c, cudaEventSynchronize(c.solve_ev));
+        } else {
+            BEM_CUDA(c, cudaStreamSynchronize(s));
+        }
         c.stats.last_iters += K;
         double bb = 0.0;
         for (int q = 0; q < nrb; ++q) bb += host[(size_t)q];
         if (bb == 0.0) {
+            tail_valid = false;
             BEM_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, s));
             rel = 0.0;
             converged = true;
@@ -1201,6 +1218,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         if (rho == 0.0) K = 1;
     }
     int rc = BEM_OK;
+    if (tail) tail->done = tail_valid && converged;
     if (!converged) {
         c.stats.gmres_fallbacks++;
         rc = gmres_solve(c, A, b, x, s);
@@ -1216,7 +1234,8 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     c.stats.solves++;
     // steps for the next solve from the observed contraction
     if (converged && rho > 0.0 && rel0 > tol)
-        c.ir_steps = std::max(1, std::min(KMAX, (int)ceil(log(tol / rel0) / log(std::max(rho, 1e-6)))));
+        ir_steps = std::max(1, std::min(KMAX, (int)ceil(log(tol / rel0) / log(std::max(rho, 1e-6)))));
+    if (st >= 0) c.stage_round0[st] = converged && rounds == 1;
     if (rc != BEM_OK) return rc;
     // Refresh policy.  X drifts from G^-1 as the surface moves, and each solve then needs a few more
     // refinement steps than right after a refresh.  A refresh (a Newton-Schulz step: two n^3 BF16x3
