@@ -343,6 +343,26 @@ def test_stage_predictor_keeps_the_trajectory(mirror):
     assert sims[0].stats().total_iters > 0 and sims[0].stats().solves == sims[1].stats().solves
 
 
+def test_solution_consumers_enqueued_again_after_a_second_round():
+    # the velocity and Dphi/Dt of a stage are enqueued behind the solve's first round; when the
+    # tolerance tightens mid-run (and the predictor's history is dropped), the first round no longer
+    # suffices and they are enqueued again with the final solution: the trajectory still follows the
+    # FP64 LU path
+    v, f = mesh.bubble(6, 1.0, (2.0, 0.0, 0.0))
+    fld = (-0.8, 2 * np.pi / 5, 0.0)
+    mix = ColocSim(v, f, pressurefield=fld, solver="mixed")
+    ref = ColocSim(v, f, pressurefield=fld, solver="lu")
+    for sim in (mix, ref):
+        sim.set_phi(0.1 * v[:, 2])
+    for k in range(8):
+        if k == 4:
+            mix._update(mixed_tol=1e-13)
+        for sim in (mix, ref):
+            sim.evolve_system_RK4(5e-3, fixdt=True)
+    assert rel(mix.get_vertices(), ref.get_vertices()) < 1e-10
+    assert rel(mix.get_phi(), ref.get_phi()) < 1e-10
+
+
 def test_mixed_precision_error_headline_size():
     # N = 4002 (config 2 mesh with the seeded 1% radial perturbation): psi of the mixed path
     # against the FP64 LU path at <= 1e-8 relative
