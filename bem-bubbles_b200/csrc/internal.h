@@ -111,8 +111,6 @@ void launch_part_volumes(Ctx& c, const double* x, double* vol, cudaStream_t s);
 // xs = x1 + scale dt kx and ps = p1 + scale dt kp (an RK4 stage's state) in one launch
 void launch_axpy_stage(Ctx& c, const double* kx, const double* kp, const double* coef_dev, double scale,
                        cudaStream_t s);
-void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k,
-                  double* out, cudaStream_t s);
 void launch_rk4_final(Ctx& c, cudaStream_t s, const int* skip = nullptr);
 // Stage predictor of the mixed solve (stage.cu): depth of the history; the ring's stage times hold
 // at PRED_CNT the number of steps that continue the current trajectory.  Start value of stage

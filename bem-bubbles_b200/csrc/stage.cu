@@ -146,13 +146,6 @@ __global__ void k_pot_t(int N, const double* __restrict__ x, const double* __res
 }
 
 // out = a + (coef * scale) * k, coef from device memory (the step dt), elementwise.
-__global__ void k_axpy_dev(int64_t n, const double* __restrict__ a, const double* __restrict__ coef, double scale,
-                           const double* __restrict__ k, double* __restrict__ out) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    out[i] = a[i] + (scale * *coef) * k[i];
-}
-
 // The positions and the potential of an RK4 stage in one launch: xs = x1 + scale dt kx (3N),
 // ps = p1 + scale dt kp (N).
 __global__ void k_axpy_stage(int N, const double* __restrict__ x1, const double* __restrict__ kx,
@@ -305,10 +298,6 @@ void launch_pot_t(Ctx& c, const double* x, const double* vel, const double* fiel
                                                c.sc, c.prm.p_inf, c.prm.epsilon, c.prm.sigma, c.prm.gamma,
                                                c.prm.field_amp, c.prm.field_kx, c.prm.field_omega,
                                                c.prm.field_phase, 0.0, 1, c.ppar, out);
-}
-void launch_axpy3(int64_t n, const double* a, const double* coef_dev, double scale, const double* k, double* out,
-                  cudaStream_t s) {
-    KLAUNCH(), k_axpy_dev<<<nb(n, 256), 256, 0, s>>>(n, a, coef_dev, scale, k, out);
 }
 void launch_axpy_stage(Ctx& c, const double* kx, const double* kp, const double* coef_dev, double scale,
                        cudaStream_t s) {
