@@ -5,6 +5,7 @@
 // reference's, expression by expression, so the projected positions and interpolated values are
 // bit-identical to the library function's; it runs single-threaded (the library version runs its
 // loop on omp_set_num_threads(100) threads with per-thread copies of both meshes).
+#include <cstdio>
 #include <stdexcept>
 #include <string>
 
@@ -31,6 +32,14 @@ void project_interpolate(bem_ctx* c, Mesh& mesh, CoordVec const& normals, Mesh c
     const int rc = bem_trace_mesh(c, (int64_t)other.verts.size(), x.data(), (int64_t)other.trigs.size(), t.data(),
                                   (int64_t)n, pos.data(), dir.data(), hit.data(), tri.data(), ok.data());
     if (rc != BEM_OK) throw std::runtime_error(std::string("remesh projection: ") + bem_last_error(c));
+    // A ray that meets no old triangle leaves its vertex at the origin with triangle 0, as the
+    // reference's project_and_interpolate does (it ignores trace_mesh's result); say so, since the
+    // resulting mesh is degenerate and its solves slow or ill-posed.
+    size_t missed = 0;
+    for (size_t i = 0; i < n; ++i) missed += ok[i] ? 0 : 1;
+    if (missed)
+        std::fprintf(stderr, "remesh projection: %zu of %zu rays met no triangle of the old surface; those vertices "
+                             "are placed at the origin, as the reference does\n", missed, n);
 
     // quadratic fits over each old vertex and its neighbours (MeshManip.cpp:1438-1448)
     std::vector<FittingTool> fits;
