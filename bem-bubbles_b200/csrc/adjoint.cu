@@ -33,15 +33,16 @@ __constant__ double a_gc[7], a_gs[7], a_gw[7];
 
 static void upload_adj_constants() {
     static std::atomic<uint64_t> done{0};
-    if (!first_on_device(done)) return;
-    QuadTables t;
-    quad_tables(t);
-    cudaMemcpyToSymbol(a_qc, t.qc, sizeof(t.qc));
-    cudaMemcpyToSymbol(a_quv, t.quv, sizeof(t.quv));
-    cudaMemcpyToSymbol(a_w, t.w, sizeof(t.w));
-    cudaMemcpyToSymbol(a_gc, t.gc, sizeof(t.gc));
-    cudaMemcpyToSymbol(a_gs, t.gs, sizeof(t.gs));
-    cudaMemcpyToSymbol(a_gw, t.gw, sizeof(t.gw));
+    once_per_device(done, [] {
+        QuadTables t;
+        quad_tables(t);
+        return cudaMemcpyToSymbol(a_qc, t.qc, sizeof(t.qc)) == cudaSuccess &&
+               cudaMemcpyToSymbol(a_quv, t.quv, sizeof(t.quv)) == cudaSuccess &&
+               cudaMemcpyToSymbol(a_w, t.w, sizeof(t.w)) == cudaSuccess &&
+               cudaMemcpyToSymbol(a_gc, t.gc, sizeof(t.gc)) == cudaSuccess &&
+               cudaMemcpyToSymbol(a_gs, t.gs, sizeof(t.gs)) == cudaSuccess &&
+               cudaMemcpyToSymbol(a_gw, t.gw, sizeof(t.gw)) == cudaSuccess;
+    });
 }
 
 struct v3 {

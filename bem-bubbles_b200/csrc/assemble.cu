@@ -101,21 +101,17 @@ void quad_tables(QuadTables& t) {
 }
 
 static void upload_constants() {
-    static std::mutex mu;
-    static uint64_t done_mask = 0;
-    std::lock_guard<std::mutex> lock(mu);
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (done_mask & (1ull << (dev & 63))) return;
-    QuadTables t;
-    quad_tables(t);
-    cudaMemcpyToSymbol(c_orb, t.orb, sizeof(t.orb));
-    cudaMemcpyToSymbol(c_qc, t.qc, sizeof(t.qc));
-    cudaMemcpyToSymbol(c_quv, t.quv, sizeof(t.quv));
-    cudaMemcpyToSymbol(c_gcos, t.gc, sizeof(t.gc));
-    cudaMemcpyToSymbol(c_gsin, t.gs, sizeof(t.gs));
-    cudaMemcpyToSymbol(c_gw, t.gw, sizeof(t.gw));
-    done_mask |= 1ull << (dev & 63);
+    static std::atomic<uint64_t> done{0};
+    once_per_device(done, [] {
+        QuadTables t;
+        quad_tables(t);
+        return cudaMemcpyToSymbol(c_orb, t.orb, sizeof(t.orb)) == cudaSuccess &&
+               cudaMemcpyToSymbol(c_qc, t.qc, sizeof(t.qc)) == cudaSuccess &&
+               cudaMemcpyToSymbol(c_quv, t.quv, sizeof(t.quv)) == cudaSuccess &&
+               cudaMemcpyToSymbol(c_gcos, t.gc, sizeof(t.gc)) == cudaSuccess &&
+               cudaMemcpyToSymbol(c_gsin, t.gs, sizeof(t.gs)) == cudaSuccess &&
+               cudaMemcpyToSymbol(c_gw, t.gw, sizeof(t.gw)) == cudaSuccess;
+    });
 }
 
 // Per-triangle record: Interpolator (Interpolator.hpp:15-37) quantities and what the 7-point rule
@@ -599,8 +595,10 @@ static void launch_tiles_t(Ctx& c, const double* x, const double* phi, double* G
     const int N = (int)c.topo.N;
     const size_t sm = sizeof(double) * (2 * CGT * ROWS + ASM_TC * REC) + sizeof(int) * 4 * ASM_TC;
     static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr))
-        cudaFuncSetAttribute(k_assemble<MIRROR, CGT, ROWS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    once_per_device(attr, [sm] {
+        return cudaFuncSetAttribute(k_assemble<MIRROR, CGT, ROWS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm) == cudaSuccess;
+    });
     dim3 grid(c.topo.ngroups, (N + ROWS - 1) / ROWS);
     KLAUNCH(), k_assemble<MIRROR, CGT, ROWS, MINB><<<grid, ROWS, sm, s>>>(N, x, c.topo.tri, c.rec, c.topo.grp_off,
                                                                           c.topo.grp_tri, c.topo.grp_slot,
@@ -618,7 +616,9 @@ static void prepare_batch_t(Ctx& c) {
     const size_t sm = tile_smem<CGT, ROWS>();
     auto kern = k_assemble_batch<MIRROR, CGT, ROWS, MINB>;
     static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr)) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    once_per_device(attr, [kern, sm] {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess;
+    });
     if (c.asm_grid_cg != CGT) {  // persistent grid: every CTA slot the SMs can hold
         int per_sm = 0, sms = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ROWS, sm);

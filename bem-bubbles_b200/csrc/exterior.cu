@@ -25,10 +25,11 @@ constexpr int ETHREADS = 128;
 
 static void upload_ext_constants() {
     static std::atomic<uint64_t> done{0};
-    if (!first_on_device(done)) return;
-    QuadTables t;
-    quad_tables(t);
-    cudaMemcpyToSymbol(e_q19, t.q19, sizeof(t.q19));
+    once_per_device(done, [] {
+        QuadTables t;
+        quad_tables(t);
+        return cudaMemcpyToSymbol(e_q19, t.q19, sizeof(t.q19)) == cudaSuccess;
+    });
 }
 
 __global__ void k_ext_records(int M, const double* __restrict__ x, const int* __restrict__ tri,

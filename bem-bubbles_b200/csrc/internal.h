@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <functional>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -18,13 +19,22 @@ namespace bemb {
 extern std::atomic<long long> g_kernel_launches;
 #define KLAUNCH() (::bemb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed))
 
-// True on the first call for this mask on the current device (device-scoped one-time set-up:
-// kernel attributes and __constant__ tables exist once per device, not once per process).
-inline bool first_on_device(std::atomic<uint64_t>& mask) {
+// Device-scoped one-time set-up (kernel attributes and __constant__ tables exist once per device,
+// not once per process): runs setup() on the current device unless it already succeeded there for
+// this mask.  Calls are serialised, so a second thread's first call waits until the set-up is
+// complete instead of launching before it; the device's bit is set only after setup() returned
+// true, so a failed set-up is tried again on the next call.  Returns whether the set-up is in place.
+inline bool once_per_device(std::atomic<uint64_t>& mask, const std::function<bool()>& setup) {
     int dev = 0;
-    cudaGetDevice(&dev);
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
     const uint64_t bit = 1ull << (dev & 63);
-    return !(mask.fetch_or(bit) & bit);
+    if (mask.load(std::memory_order_acquire) & bit) return true;
+    static std::recursive_mutex m;
+    std::lock_guard<std::recursive_mutex> lock(m);
+    if (mask.load(std::memory_order_acquire) & bit) return true;
+    if (!setup()) return false;
+    mask.fetch_or(bit, std::memory_order_release);
+    return true;
 }
 
 // Largest column-group width of the assembly tiles (a CTA owns up to CG_MAX columns of G and H);

@@ -632,7 +632,10 @@ __global__ void k_trsv_bwd_rest(int n, int k0, int k1, const double* __restrict_
 static void lu_substitute_blocked(Ctx& c, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
     static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr)) cudaFuncSetAttribute(k_lu_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_lu_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+               cudaSuccess;
+    });
     KLAUNCH(), k_lu_permute<<<1, 1024, sizeof(double) * (size_t)n, s>>>(n, c.piv, b, x);
     for (int k0 = 0; k0 < n; k0 += TS_B) {
         const int k1 = std::min(n, k0 + TS_B);

@@ -438,9 +438,14 @@ int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s) {
     const size_t smem = sizeof(double) * ((size_t)rows_per * (nb + 1) + 2 * (2 + nb) + 2 * nb);
     if (smem > 200 * 1024) return BEM_ERR_CUDA;
     static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr)) {
-        cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (!once_per_device(attr, [] {
+            return cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+                       cudaSuccess &&
+                   cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+                       cudaSuccess;
+        })) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C);
@@ -485,8 +490,13 @@ int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s) {
     const size_t smem = sizeof(double) * (size_t)rows_per * (nb + 1);
     if (smem > 200 * 1024) return BEM_ERR_CUDA;
     static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr))
-        cudaFuncSetAttribute(k_lu_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (!once_per_device(attr, [] {
+            return cudaFuncSetAttribute(k_lu_panel_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+                   cudaSuccess;
+        })) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_panel_rows, LP_THREADS, smem) != cudaSuccess ||
         per_sm * sms < G)

@@ -41,23 +41,45 @@ static int noalloc_scratch(int device, unsigned char** out) {
 
 }  // namespace bemb
 
-extern "C" int bem_gemm_bf16x3_noalloc(int device, int n, const float* A, const float* B, float* C, void* stream) {
+namespace {
+// Makes `device` current for the call and gives the caller's thread its own current device back on
+// every return path (plug-in callers, e.g. under a framework driving several GPUs, keep theirs).
+struct DeviceScope {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceScope(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ok = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int gemm_noalloc(int device, int n, const float* A, const float* B, float* C, cudaStream_t s) {
     using namespace bemb;
-    if (n <= 0 || !A || !B || !C) return BEM_ERR_ARG;
-    if (n > BEM_NOALLOC_GEMM_MAX_N) return BEM_ERR_ARG;  // the scratch holds planes up to this size
-    if (cudaSetDevice(device) != cudaSuccess) return BEM_ERR_CUDA;
     unsigned char* scratch = nullptr;
     int rc = noalloc_scratch(device, &scratch);
     if (rc) return rc;
     int* err = reinterpret_cast<int*>(scratch + NOALLOC_PLANES_BYTES);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     // the error word must start at zero; the planes are overwritten in full (pads included)
     if (cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) return BEM_ERR_CUDA;
     Ctx c;
-    rc = tc_gemm(c, n, A, B, C, scratch, err, s);
+    rc = tc_gemm(c, n, A, B, C, scratch, err, s);  // reports a refused launch itself
     if (rc) return rc;
     int herr = 0;
     if (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return BEM_ERR_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return BEM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;
     return herr ? BEM_ERR_CUDA : BEM_OK;
+}
+}  // namespace
+
+// The stream must belong to `device` (or be the legacy default stream 0, then that device's).
+extern "C" int bem_gemm_bf16x3_noalloc(int device, int n, const float* A, const float* B, float* C, void* stream) {
+    using namespace bemb;
+    if (n <= 0 || !A || !B || !C) return BEM_ERR_ARG;
+    if (n > BEM_NOALLOC_GEMM_MAX_N) return BEM_ERR_ARG;  // the scratch holds planes up to this size
+    DeviceScope scope(device);
+    if (!scope.ok) return BEM_ERR_CUDA;
+    return gemm_noalloc(device, n, A, B, C, static_cast<cudaStream_t>(stream));
 }

@@ -293,15 +293,24 @@ int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* plane
         return c.fail(BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     const size_t sm = tc_smem_bytes();
     static std::atomic<uint64_t> attr{0};
-    if (first_on_device(attr)) {
-        BEM_CUDA(c, cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        BEM_CUDA(c, cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (!once_per_device(attr, [sm] {
+            return cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm) == cudaSuccess;
+        })) {
+        cudaGetLastError();
+        return c.fail(BEM_ERR_CUDA, "cudaFuncSetAttribute failed for the tensor-core GEMM");
     }
     dim3 grid(npad / TC_BN, npad / TC_BM);
     if (terms == 1)
         KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 1><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
     else
         KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
+    // a launch refused for its configuration (shared memory, grid) leaves C unwritten: report it here,
+    // since a later stream synchronisation does not
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return c.fail(BEM_ERR_CUDA, std::string("tensor-core GEMM launch: ") + cudaGetErrorString(le));
     return BEM_OK;
 }
 
@@ -329,7 +338,7 @@ extern "C" int bem_gemm_bf16x3(int device, int n, const float* A, const float* B
         cudaMemset(err, 0, sizeof(int));
         rc = tc_gemm(c, n, dA, dB, dC, planes, err, 0);
         int herr = 0;
-        if (cudaDeviceSynchronize() != cudaSuccess) rc = BEM_ERR_CUDA;
+        if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = BEM_ERR_CUDA;
         cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
         if (herr) rc = BEM_ERR_CUDA;
         if (rc == BEM_OK) cudaMemcpy(C, dC, nn * 4, cudaMemcpyDeviceToHost);

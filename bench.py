@@ -28,9 +28,14 @@ ours: the mixed-precision path (FP64 assembly, FP64 GMRES, FP32 approximate-inve
 through libbem_b200.so.  value = device time of K steps with the state resident in HBM (CUDA events
 on the library's stream, max over ranks); e2e = the same K steps through the C ABI with host
 buffers, the step's state copied in from pinned memory and the result copied back every step.
-reference: the reference's own CPU code (oracle/_ref, built from the reference sources) on the
-host cores, one RK4 stage per timed step.  With --gpus N > 1 every rank runs an independent replica
-(the path does not shard: replicas only); rank 0 prints one JSON line.
+Beside it: the all-FP64 GPU paths (BiCGSTAB, the reference's default, and LU) each in its own
+context over the same warm-up and K-step window from the same initial state; the mixed trajectory
+against the FP64 one step by step; the one-time set-up of the approximate inverse.
+reference: the reference's own CPU code (oracle/_ref, built from the reference sources) on all host
+cores: real RK4 steps (evolve_system_RK4 with its default BiCGSTAB solve) after untimed warm-up
+steps, up to K timed steps within about two minutes; `steps` is the number actually timed.  With
+--gpus N > 1 every rank runs an independent replica (the path does not shard: replicas only);
+rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -249,18 +254,41 @@ def clock_sampler(index):
         return ClockSampler(index)
 
 
-def cpu_reference_stages(stages, threads, timeout=900):
-    """Seconds of each of `stages` RK4 stages of the reference's own code (oracle/_ref)."""
+def headline_config(ws):
+    """The workload description both arms report (the same dict, so the arms compare like for like)."""
+    return {"workload": "single bubble icosphere nu=20 (N=4002, M=8000), R0=1 at (2,0,0), 1% radial perturbation "
+                        "(seed 0), phi=0, p_inf=1, epsilon=1, gamma=1.4, RK4 dt=5e-3 fixed, "
+                        "p(t)=1-0.8 sin(2 pi t/5)",
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+            "l2": "working set larger than L2 (G+H = 256 MB per stage)"}
+
+
+REF_SOLVER = "BiCGSTAB (the reference default: Jacobi preconditioner, tolerance machine epsilon, <= 2N iterations)"
+
+
+def cpu_reference_steps(warm, steps, threads, budget_s):
+    """Real RK4 steps (evolve_system_RK4 with its default BiCGSTAB solve) of the reference's own code
+    (oracle/_ref) on `threads` host threads: `warm` untimed steps from the workload's initial state
+    (phi = 0, so the first stage's right-hand side is zero; later stages and steps solve in earnest),
+    then up to `steps` timed ones, stopping once budget_s seconds of timed steps are spent.  None when
+    the reference build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     if not O.ref_available(False):
         return None
     v, f = workload()
-    env_threads = dict(threads=threads)
-    out = O.ref_run("stages", v, f, np.zeros(len(v)), steps=stages, lu=0, V0=O.volume(v, f),
-                    amp=FIELD[0], omega=FIELD[1], phase=FIELD[2], **PHYS, **env_threads)
-    return out
+    return O.ref_rk4_timed(v, f, np.zeros(len(v)), warm=warm, steps=steps, budget=budget_s, dt=DT, fixdt=1,
+                           lu=0, V0=O.volume(v, f), amp=FIELD[0], omega=FIELD[1], phase=FIELD[2],
+                           threads=threads, **PHYS)
+
+
+def ref_sample_text(r, warm, threads):
+    k = len(r["seconds"])
+    return (f"{k} timed RK4 steps of the reference code (oracle/_ref: evolve_system_RK4, {REF_SOLVER}) after "
+            f"{warm} untimed steps from the workload's initial state, {threads} OpenMP threads; "
+            f"{int(r['solves'].sum())} BiCGSTAB solves, mean {float(r['iters'].sum()) / max(1, int(r['solves'].sum())):.1f} "
+            f"iterations per solve")
 
 
 def run_reference(args):
@@ -269,27 +297,92 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    secs = cpu_reference_stages(args.warmup + args.steps, threads)
-    if secs is None:
+    # warm-up as in our arm (capped: a reference step takes seconds), then the K timed steps, bounded
+    # to about two minutes of timed work
+    warm = min(args.warmup, 5)
+    r = cpu_reference_steps(warm, args.steps, threads, budget_s=120.0)
+    if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference checkout absent at build time)"}))
         return 0
-    t = np.asarray(secs[args.warmup:])
-    stage_s = float(t.mean())
-    value = 1.0 / (4.0 * stage_s)
+    k = len(r["seconds"])
+    total_s = float(r["seconds"].sum())
+    value = k / total_s
     line = {
-        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 4.0 * stage_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": k,
+        "warmup": warm, "ms_per_step": total_s / k * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": "single bubble icosphere nu=20 (N=4002, M=8000), RK4 dt=5e-3, oscillating far field",
-                   "solver": "BiCGSTAB (reference default)", "sample": "one RK4 stage per timed step"},
+        "impl": "reference", "solver": REF_SOLVER,
+        "config": headline_config(1),
+        "bicgstab": {"solves": int(r["solves"].sum()), "iterations": int(r["iters"].sum()),
+                     "iters_per_solve": float(r["iters"].sum()) / max(1, int(r["solves"].sum()))},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "reference",
-                         "sample": f"{args.steps} RK4 stages at N=4002 (4 stages = 1 step), reference code "
-                                   f"(oracle/_ref) with OpenMP on {threads} threads"},
+                         "sample": ref_sample_text(r, warm, threads)},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def fp64_comparator(solver, device, warmup, steps):
+    """Steps/s of an all-FP64 solver path on the GPU ("bicgstab": the reference's default solver, "lu":
+    its PartialPivLU option) in a context of its own, from the workload's initial state, with the same
+    warm-up and timed window as the mixed arm (CUDA events on the library's stream)."""
+    import torch
+
+    from bem_b200.sim import ColocSim
+
+    v, f = workload()
+    sim = ColocSim(v, f, pressurefield=FIELD, solver=solver, device=device, **PHYS)
+    sim.set_phi(0.0)
+    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=device)
+    for _ in range(warmup):
+        sim.evolve_rk4_steps(DT, 1)
+    sim.sync()
+    st0 = sim.stats()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(ext)
+    sim.evolve_rk4_steps(DT, steps)
+    b.record(ext)
+    b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    st1 = sim.stats()
+    sim.close()
+    out = {"solver": solver, "ms_per_step": ms, "steps_per_s": 1e3 / ms, "steps": steps, "warmup": warmup}
+    if solver == "bicgstab":
+        solves = int(st1.solves - st0.solves)
+        out["iters_per_solve"] = float(st1.total_iters - st0.total_iters) / max(1, solves)
+    return out
+
+
+def trajectory_error(device, steps):
+    """Mixed-precision trajectory against the FP64 BiCGSTAB trajectory: two contexts from the workload's
+    initial state, `steps` RK4 steps each, the state read after every step.  Returns the largest
+    relative difference over the steps of psi (dphi/dn), of x and of phi (max-norm relative to the
+    FP64 path's max |.|)."""
+    from bem_b200.sim import ColocSim
+
+    v, f = workload()
+    sims = [ColocSim(v, f, pressurefield=FIELD, solver=s, device=device, **PHYS) for s in ("mixed", "bicgstab")]
+    worst = {"psi": 0.0, "x": 0.0, "phi": 0.0}
+    per_step_psi = []
+    for sim in sims:
+        sim.set_phi(0.0)
+    for _ in range(steps):
+        st = []
+        for sim in sims:
+            sim.evolve_system_RK4(DT, fixdt=True)
+            st.append(sim.get_state())
+        (xm, pm, sm, _), (x6, p6, s6, _) = st
+        e = {"x": np.max(np.abs(xm - x6)) / np.max(np.abs(x6)),
+             "phi": np.max(np.abs(pm - p6)) / max(np.max(np.abs(p6)), 1e-300),
+             "psi": np.max(np.abs(sm - s6)) / max(np.max(np.abs(s6)), 1e-300)}
+        per_step_psi.append(float(e["psi"]))
+        for k in worst:
+            worst[k] = max(worst[k], float(e[k]))
+    for sim in sims:
+        sim.close()
+    return {"steps": steps, "max_rel_err": worst, "psi_last_step": per_step_psi[-1],
+            "target_psi": 1e-8, "fp64_solver": "bicgstab"}
 
 
 def run_ours(args):
@@ -315,8 +408,16 @@ def run_ours(args):
     sim.set_phi(0.0)
     ext = torch.cuda.ExternalStream(sim.stream_handle(), device=device)
 
-    # warm-up (also builds the preconditioner once)
-    for _ in range(args.warmup):
+    # warm-up; the first step also builds the approximate inverse (the mixed path's one-time set-up),
+    # timed on its own
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.sync()
+    ea.record(ext)
+    sim.evolve_rk4_steps(DT, 1)
+    eb.record(ext)
+    eb.synchronize()
+    first_step_ms = ea.elapsed_time(eb)
+    for _ in range(args.warmup - 1):
         sim.evolve_rk4_steps(DT, 1)
     sim.sync()
 
@@ -324,6 +425,7 @@ def run_ours(args):
     fp64_peak, fp32_peak = measure_fma_peaks(device)
     sim.set_profiling(True)
     sim.reset_profile()
+    st0 = sim.stats()
     if dist:
         dist.barrier()
     torch.cuda.synchronize(device)
@@ -339,11 +441,13 @@ def run_ours(args):
     torch.cuda.synchronize(device)
     elapsed_ms = e0.elapsed_time(e1)
     prof = sim.profile()
+    st1 = sim.stats()
     sim.set_profiling(False)
     if dist:
         elapsed_ms = max_over_ranks(elapsed_ms, dist, f"cuda:{device}")
         dist.barrier()
     value = replica_value(ws, args.steps, elapsed_ms)
+    ms_per_step = elapsed_ms / args.steps
 
     # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region
     hx = torch.empty((N, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -367,24 +471,20 @@ def run_ours(args):
     h2d = N * 3 * 8 + 2 * N * 8
     d2h = N * 3 * 8 + 2 * N * 8
 
-    # accuracy of the mixed path against the FP64 path on the current state: the mixed solve first
-    # (warm-started from its own previous stage, as in the timed steps), then the FP64 BiCGSTAB
-    # solve (zero start) of the same system
+    # accuracy of one solve on the current state: the mixed solve first (warm-started from its own
+    # previous stage, as in the timed steps), then the FP64 BiCGSTAB solve (zero start) of the same system
     phi_now = sim.get_phi()
     _, psimx = sim.position_t(phi_now, return_psi=True)
-    ref_solver = "bicgstab"
-    sim.set_solver(ref_solver)
+    sim.set_solver("bicgstab")
     _, psi64 = sim.position_t(phi_now, return_psi=True)
     psi_err = float(np.max(np.abs(psimx - psi64)) / max(np.max(np.abs(psi64)), 1e-300))
-    # the FP64 path's own speed on the same state
-    fp64_steps = 2
-    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    sim.sync()
-    ev_a.record(ext)
-    sim.evolve_rk4_steps(DT, fp64_steps)
-    ev_b.record(ext)
-    ev_b.synchronize()
-    fp64_ms_per_step = ev_a.elapsed_time(ev_b) / fp64_steps
+    sim.close()
+
+    # the all-FP64 paths on the same GPU, each in its own context over the same window, and the
+    # mixed trajectory against the FP64 one step by step
+    fp64 = {s: fp64_comparator(s, device, args.warmup, args.steps) for s in ("bicgstab", "lu")}
+    best64 = max(fp64.values(), key=lambda d: d["steps_per_s"])
+    traj = trajectory_error(device, args.warmup + args.steps)
 
     if rank != 0:
         if dist:
@@ -398,30 +498,37 @@ def run_ours(args):
     achieved = flops / (avg_asm_ms * 1e-3) / 1e12
     traffic = read_traffic()
 
-    # CPU baseline: the reference's own code on the host cores, bounded sample of 2 stages
+    # CPU baseline: the reference's own RK4 steps on the host cores, a bounded sample
     cpu = None
     if ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         os.environ["OMP_NUM_THREADS"] = str(threads)
-        secs = cpu_reference_stages(2, threads)
-        if secs is not None:
-            cpu = {"value": 1.0 / (4.0 * float(np.mean(secs))), "unit": "steps/s", "cores": threads,
-                   "kind": "reference",
-                   "sample": f"2 RK4 stages at N=4002 of the reference code (oracle/_ref, BiCGSTAB default), "
-                             f"{threads} OpenMP threads; steps/s = 1/(4 x mean stage time)"}
+        r = cpu_reference_steps(1, 3, threads, budget_s=20.0)
+        if r is not None:
+            cpu = {"value": len(r["seconds"]) / float(r["seconds"].sum()), "unit": "steps/s", "cores": threads,
+                   "kind": "reference", "sample": ref_sample_text(r, 1, threads)}
 
+    setup_ms = max(first_step_ms - ms_per_step, 0.0)
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (assembly, residual, state) + f32 (preconditioner)",
-        "data": "synthetic",
-        "config": {"workload": "single bubble icosphere nu=20 (N=4002, M=8000), RK4 dt=5e-3, p(t)=1-0.8 sin(2 pi t/5)",
-                   "solver": args.solver, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                   "l2": "working set larger than L2 (G+H = 256 MB per stage)"},
-        "fp64_gpu": {"solver": ref_solver, "ms_per_step": fp64_ms_per_step,
-                     "steps_per_s": 1e3 / fp64_ms_per_step},
-        "speedup_vs_fp64_gpu": (1e3 / fp64_ms_per_step) and value / ws / (1e3 / fp64_ms_per_step),
+        "data": "synthetic", "solver": args.solver,
+        "config": headline_config(ws),
+        "fp64_gpu": fp64["bicgstab"],
+        "fp64_lu_gpu": fp64["lu"],
+        "speedup_vs_fp64_gpu": value / ws / fp64["bicgstab"]["steps_per_s"],
+        "speedup_vs_best_fp64_gpu": {"solver": best64["solver"], "ratio": value / ws / best64["steps_per_s"]},
         "psi_rel_err_vs_fp64": psi_err,
+        "trajectory_vs_fp64": traj,
+        "setup": {"first_step_ms": first_step_ms, "setup_ms": setup_ms,
+                  "steps_per_s_incl_setup": args.steps / ((elapsed_ms / ws + setup_ms) * 1e-3),
+                  "note": "setup_ms = first warm-up step (builds the approximate inverse) minus a timed step"},
+        "during_timed_steps": {"solves": int(st1.solves - st0.solves),
+                               "refinement_steps_per_solve": float(st1.total_iters - st0.total_iters) /
+                               max(1, int(st1.solves - st0.solves)),
+                               "newton_schulz_steps": int(st1.ns_steps - st0.ns_steps),
+                               "refreshes": int(st1.precond_refresh - st0.precond_refresh)},
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(prof.kernel_launches),
         "roofline": {"bound": "fp64-fma", "kernel": "k_assemble + k_singular_diag (assembly: regular-pair tiles, then singular pairs and the 4 pi rule)", "achieved": achieved,

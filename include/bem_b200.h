@@ -282,8 +282,9 @@ int bem_gemm_bf16x3(int device, int n, const float* A, const float* B, float* C)
 /* Allocation-free form of bem_gemm_bf16x3, for callers that cannot allocate GPU memory (a host
  * framework that owns the device heap, loops that must not allocate after start-up, plug-ins that
  * only receive device pointers).  This entry point has no counterpart in the reference.
- * A, B, C: DEVICE pointers to FP32 column-major n x n matrices owned by the caller; stream: a
- * cudaStream_t (NULL = the legacy default stream).  The call allocates nothing: its scratch (four
+ * A, B, C: DEVICE pointers on `device` to FP32 column-major n x n matrices owned by the caller;
+ * stream: a cudaStream_t that belongs to `device` (NULL = the legacy default stream).  The calling
+ * thread's current device is the same after the call as before it.  The call allocates nothing: its scratch (four
  * bf16 operand planes and an error word) is a static device array of BEM_NOALLOC_GEMM_MAX_N^2 * 8
  * bytes + 256 bytes (8 MB) that every GPU loading this library holds until the process exits.
  * n > BEM_NOALLOC_GEMM_MAX_N returns BEM_ERR_ARG.  The first call on a device looks up the scratch's

@@ -85,8 +85,12 @@ static double dotv(Index n, const double* u, const double* v) {
     return s;
 }
 
+long long g_bicgstab_solves = 0;
+long long g_bicgstab_iters = 0;
+
 void bicgstab_dense(Index n, const double* a, const double* b, double* x, Index max_iters,
                     double tol, Index* iters_out, double* err_out) {
+    ++g_bicgstab_solves;
     std::vector<double> r(n), r0(n), p(n, 0.0), v(n, 0.0), y(n), z(n), s(n), t(n), invd(n);
     for (Index i = 0; i < n; ++i) {
         double d = a[i + i * n];
@@ -134,6 +138,7 @@ void bicgstab_dense(Index n, const double* a, const double* b, double* x, Index 
         ++it;
     }
     *iters_out = it;
+    g_bicgstab_iters += it;
     *err_out = std::sqrt(dotv(n, r.data(), r.data()) / rhs2);
 }
 

@@ -210,3 +210,17 @@ def ref_run(action, verts, tris, phi, mirror=False, timing=False, points=None, p
     if timing:
         return out, r.stderr.decode()
     return out
+
+
+def ref_rk4_timed(verts, tris, phi, warm, steps, budget=0.0, **kw):
+    """Real RK4 steps of the reference's own code (evolve_system_RK4, LinLinSim.cpp:194-257):
+    `warm` untimed steps from (verts, phi), then up to `steps` timed ones, stopping once `budget`
+    seconds of timed steps are spent (0: no limit).  Returns a dict with per-step seconds, BiCGSTAB
+    solves and iterations, and the final state (x, phi, psi, time)."""
+    out = ref_run("rk4_timed", verts, tris, phi, warm=warm, steps=steps, budget=budget, **kw)
+    n = len(verts)
+    k = int(out[0])
+    rec = out[1:1 + 3 * k].reshape(k, 3)
+    st = out[1 + 3 * k:]
+    return {"seconds": rec[:, 0].copy(), "solves": rec[:, 1].astype(int), "iters": rec[:, 2].astype(int),
+            "x": st[:3 * n].reshape(n, 3), "phi": st[3 * n:4 * n], "psi": st[4 * n:5 * n], "time": float(st[5 * n])}

@@ -14,11 +14,15 @@
 //     rk4        -> after each of `steps` RK4 steps: verts (N*3), phi (N), psi (N), time (1)
 //     euler      -> same record layout as rk4, using evolve_system
 //     stages     -> `steps` repetitions of one RK4 stage (position_t + pot_t_multi); writes the
-//                   seconds of each repetition (timing sample for the CPU baseline)
+//                   seconds of each repetition
+//     rk4_timed  -> `warm` untimed RK4 steps (evolve_system_RK4), then up to `steps` timed ones (no new
+//                   step once `budget` seconds of timed steps are spent, budget=0: no limit); writes
+//                   the count K, per timed step: seconds, BiCGSTAB solves, BiCGSTAB iterations
+//                   (timing sample of the reference's own step), then the final verts, phi, psi, time
 //     exterior   -> exterior_pot(points) (LinLinSim.cpp:479-485: assemble, solve, compute_exterior_pot)
 //     exterior_direct -> compute_exterior_pot(points, mesh, phi, psi) with the given psi
 //   in.bin for exterior*: then int64 P, P*3 float64 points, and for exterior_direct N float64 psi
-//   keys: p_inf epsilon sigma gamma V0 amp omega phase dt steps fixdt lu threads timing
+//   keys: p_inf epsilon sigma gamma V0 amp omega phase dt steps warm budget fixdt lu threads timing
 //   amp/omega/phase define the far-field pressure p(x,t) = amp*sin(omega*t + phase).
 #include <cstdint>
 #include <cstdio>
@@ -30,6 +34,7 @@
 #include <vector>
 
 #include "Bem/Simulation/ColocSim.hpp"
+#include <Eigen/IterativeLinearSolvers>
 
 using namespace Bem;
 
@@ -50,7 +55,8 @@ int main(int argc, char** argv) {
     std::map<std::string, double> kv = {{"p_inf", 1.0}, {"epsilon", 1.0}, {"sigma", 0.0}, {"gamma", 1.0},
                                         {"V0", -1.0},   {"amp", 0.0},     {"omega", 0.0}, {"phase", 0.0},
                                         {"dt", 1e-3},   {"steps", 1},     {"fixdt", 1},   {"lu", 1},
-                                        {"threads", 1}, {"t", 0.0},       {"timing", 0}};
+                                        {"threads", 1}, {"t", 0.0},       {"timing", 0},  {"warm", 0},
+                                        {"budget", 0.0}};
     for (int i = 4; i < argc; ++i) {
         const char* eq = std::strchr(argv[i], '=');
         if (!eq) die("bad key=value");
@@ -142,6 +148,34 @@ int main(int argc, char** argv) {
             double tm = sim.get_time();
             put(&tm, 1);
         }
+    } else if (action == "rk4_timed") {
+        const int warm = (int)kv["warm"], steps = (int)kv["steps"];
+        const double budget = kv["budget"];
+        for (int s = 0; s < warm; ++s) sim.evolve_system_RK4(kv["dt"], kv["fixdt"] != 0.0);
+        std::vector<double> recs;
+        double spent = 0.0;
+        for (int s = 0; s < steps && (budget <= 0.0 || spent < budget); ++s) {
+            const long long s0 = Eigen::shim_detail::g_bicgstab_solves, i0 = Eigen::shim_detail::g_bicgstab_iters;
+            auto a0 = std::chrono::steady_clock::now();
+            sim.evolve_system_RK4(kv["dt"], kv["fixdt"] != 0.0);
+            const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - a0).count();
+            spent += sec;
+            recs.push_back(sec);
+            recs.push_back((double)(Eigen::shim_detail::g_bicgstab_solves - s0));
+            recs.push_back((double)(Eigen::shim_detail::g_bicgstab_iters - i0));
+        }
+        const double count = (double)(recs.size() / 3);
+        put(&count, 1);
+        put(recs.data(), recs.size());
+        for (auto const& e : sim.mesh.verts) {
+            double d[3] = {e.x, e.y, e.z};
+            put(d, 3);
+        }
+        PotVec ph = sim.get_phi(), ps = sim.get_psi();
+        put(ph.data(), ph.size());
+        put(ps.data(), ps.size());
+        double tm = sim.get_time();
+        put(&tm, 1);
     } else if (action == "stages") {
         int steps = (int)kv["steps"];
         PotVec p = phi;
