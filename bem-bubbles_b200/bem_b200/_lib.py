@@ -43,7 +43,7 @@ class Stats(C.Structure):
     _fields_ = [("solves", C.c_int64), ("last_iters", C.c_int32), ("precond_refresh", C.c_int32),
                 ("last_rel_residual", C.c_double), ("ns_steps", C.c_int64), ("gmres_fallbacks", C.c_int64),
                 ("fp64_fallbacks", C.c_int64),
-                ("total_iters", C.c_int64)]
+                ("total_iters", C.c_int64), ("wait_expired", C.c_int64)]
 
 
 class Profile(C.Structure):
@@ -90,6 +90,7 @@ SIGNATURES = {
     "bem_evolve_euler": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, _D]),
     "bem_evolve_rk4_n": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "bem_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    "bem_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
     "bem_sync": (C.c_int, [C.c_void_p]),
     "bem_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "bem_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),

@@ -1,8 +1,8 @@
 // Implementation of the drop-in Bem::Simulation / LinLinSim / ColocSim (Bem/Simulation/*.hpp in this
 // directory) over the C ABI of libbem_b200.so.  The per-step hot path -- assembly, solve, vertex
-// velocities, Bernoulli update, RK4/Euler combination -- runs on the GPU; remeshing, PLY export and
-// the exterior potential stay on the host with the user's Bem/Mesh and Bem/Integration libraries,
-// as in the reference.
+// velocities, Bernoulli update, RK4/Euler combination -- runs on the GPU, and so do the exterior
+// potential and the projection step of remeshing; the remesh's topology edits and the PLY export stay
+// on the host with the user's Bem/Mesh library, as in the reference.
 #include <cmath>
 #include <cstdlib>
 #include <set>

@@ -40,6 +40,7 @@ struct PBArgs {
     unsigned* bar;   // [0] arrivals, [1] generation
     int* err;        // barrier wait expired
     DevScalars* sc;  // scalars across launches
+    long long wait_limit;  // bound of each barrier wait, SM clock cycles
 };
 
 __device__ __forceinline__ double wsum(double v) {
@@ -82,7 +83,7 @@ __device__ double dot_total(const PBArgs& a, int k) {
     return out;
 }
 
-__device__ __forceinline__ bool grid_sync(const PBArgs& a) { return grid_barrier(a.bar, a.err); }
+__device__ __forceinline__ bool grid_sync(const PBArgs& a) { return grid_barrier(a.bar, a.err, a.wait_limit); }
 
 // out = A in (column-major A), tiles (row block, column split) spread over the CTAs; the last CTA
 // of a row block sums the splits in order, writes out and the row block's dots out.u0 -> dots[k0],
@@ -342,6 +343,7 @@ int bicgstab_persistent(Ctx& c, const double* A, const double* b, double* x, cud
     a.bar = reinterpret_cast<unsigned*>(c.pbicg + (size_t)D_N * a.nrb);
     a.err = reinterpret_cast<int*>(a.bar + 4);
     a.sc = c.sc;
+    a.wait_limit = c.wait_limit;
     const int maxit = c.prm.max_iters > 0 ? c.prm.max_iters : 2 * n;
     KLAUNCH(), k_pbicg_init<<<a.nrb, PB_ROWS, 0, s>>>(a);
     KLAUNCH(), k_pbicg_init_scalars<<<1, 32, 0, s>>>(a, maxit);
@@ -357,7 +359,10 @@ int bicgstab_persistent(Ctx& c, const double* A, const double* b, double* x, cud
         BEM_CUDA(c, cudaMemcpyAsync(c.h_sc, c.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
         BEM_CUDA(c, cudaMemcpyAsync(&err, a.err, sizeof(int), cudaMemcpyDeviceToHost, s));
         BEM_CUDA(c, cudaStreamSynchronize(s));
-        if (err) return BEM_ERR_CUDA;
+        if (err) {
+            c.stats.wait_expired++;
+            return c.fail(BEM_ERR_CUDA, "persistent BiCGSTAB: a grid barrier wait expired");
+        }
         if (c.h_sc->done) break;
         if (launch * a.budget > 4 * maxit + 64) return c.fail(BEM_ERR_NOT_CONVERGED, "BiCGSTAB: loop guard");
     }

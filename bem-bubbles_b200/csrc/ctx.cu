@@ -1412,6 +1412,13 @@ int bem_get_stats(bem_ctx* c, bem_stats* s) {
     return BEM_OK;
 }
 
+int bem_set_wait_limit(bem_ctx* c, int64_t cycles) {
+    CTX_GUARD(c);
+    if (cycles <= 0) return c->fail(BEM_ERR_ARG, "bem_set_wait_limit: cycles must be positive");
+    c->wait_limit = (long long)cycles;
+    return BEM_OK;
+}
+
 int bem_sync(bem_ctx* c) {
     CTX_GUARD(c);
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));

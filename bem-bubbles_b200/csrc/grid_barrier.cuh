@@ -1,11 +1,18 @@
 // Grid-wide barrier for kernels launched cooperatively (all CTAs co-resident), with a bounded wait.
-// bar[0] counts arrivals, bar[1] is the generation; both start at zero.  A wait longer than about a
-// second of clock sets *err and returns; the caller checks the result and ends the kernel.
+// bar[0] counts arrivals, bar[1] is the generation; both start at zero.  A wait longer than `limit`
+// SM clock cycles (GRID_WAIT_CYCLES, about a second, unless the context sets another bound) sets
+// *err and returns false; the caller then ends the kernel.  Every CTA still arrives at the barrier
+// it reached, so the last arrival resets the count and bumps the generation as usual.  A CTA that
+// passed that barrier before the error word was set leaves at the next one, where the CTA that gave
+// up never arrives, by its own bounded wait: an expired wait ends the kernel within two limits, with
+// no CTA left waiting.
 #pragma once
 
 namespace bemb {
 
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
+constexpr long long GRID_WAIT_CYCLES = 2000000000LL;
+
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, long long limit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -19,7 +26,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
         } else {
             const long long t0 = clock64();
             while (*gen == g) {
-                if (clock64() - t0 > 2000000000LL) {
+                if (clock64() - t0 > limit) {
                     atomicExch(err, 1);
                     break;
                 }

@@ -678,7 +678,10 @@ static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
         int err = 0;
         BEM_CUDA(c, cudaMemcpyAsync(&err, lu_panel_err(c), sizeof(int), cudaMemcpyDeviceToHost, s));
         BEM_CUDA(c, cudaStreamSynchronize(s));
-        if (err) return BEM_ERR_CUDA;
+        if (err) {
+            c.stats.wait_expired++;
+            return BEM_ERR_CUDA;
+        }
     }
     return BEM_OK;
 }

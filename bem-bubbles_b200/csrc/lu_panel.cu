@@ -41,6 +41,7 @@ struct LPArgs {
     double* diag;    // 2 (parity) x nb: the diagonal row before the interchange
     unsigned* bar;   // grid barrier words
     int* err;        // barrier wait expired
+    long long wait_limit;  // bound of each barrier wait, SM clock cycles
 };
 
 __global__ void __launch_bounds__(LP_THREADS) k_lu_panel_rows(LPArgs a) {
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_lu_panel_rows(LPArgs a) {
             for (int c = tid; c < nb; c += LP_THREADS) mine[2 + c] = sp[(bi - r0) * ld + c];
         if (rowj >= r0 && rowj < r1)
             for (int c = tid; c < nb; c += LP_THREADS) diag[c] = sp[(rowj - r0) * ld + c];
-        if (!grid_barrier(a.bar, a.err)) return;
+        if (!grid_barrier(a.bar, a.err, a.wait_limit)) return;
         // the pivot, the same in every CTA: largest |entry| over the candidates, then smallest row (an
         // order-independent rule, reduced over the threads)
         double pv = -1.0;
@@ -513,6 +514,7 @@ int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s) {
     a.diag = lp_diag(c);
     a.bar = lp_bar(c);
     a.err = lu_panel_err(c);  // cleared once per factorisation by the caller
+    a.wait_limit = c.wait_limit;
     BEM_CUDA(c, cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), s));
     void* args[] = {&a};
     KLAUNCH();

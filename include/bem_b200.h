@@ -248,8 +248,19 @@ typedef struct {
                                  singular G, e.g. a bubble cut by its own wall image) */
     int64_t total_iters;      /* iterations of every iterative solve since creation (refinement steps of
                                  the mixed path, including its GMRES hand-overs; BiCGSTAB iterations) */
+    int64_t wait_expired;     /* bounded grid-barrier waits of the persistent kernels (BiCGSTAB, LU
+                                 panel) that gave up; each sent the context to the multi-kernel form */
 } bem_stats;
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
+
+/* Bound, in SM clock cycles, of every grid-wide barrier wait of the persistent kernels (the
+ * cooperative BiCGSTAB and the row-distributed LU panel).  Default 2e9 (about a second at the
+ * B200's clock).  A wait that runs out makes the kernel set its error word and return; the host
+ * reads it, counts it in bem_stats.wait_expired and finishes the solve with the multi-kernel form,
+ * which the context keeps for the rest of its life.  No counterpart in the reference (its solves
+ * run on the host); exists so that this failure path can be tested without a GPU fault.
+ * cycles <= 0 returns BEM_ERR_ARG. */
+int bem_set_wait_limit(bem_ctx* ctx, int64_t cycles);
 
 /* Synchronise the context's stream. */
 int bem_sync(bem_ctx* ctx);

@@ -178,6 +178,14 @@ class State:
 
 
 # ---------------------------------------------------------------- reference harness
+def reference_dir() -> str:
+    """The reference checkout the oracle's recipe compiles from (oracle/Makefile's BEM_REFERENCE: the
+    environment variable of that name, else its default)."""
+    out = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "refdir"], check=True,
+                         capture_output=True, text=True)
+    return out.stdout.strip()
+
+
 def ref_available(mirror=False) -> bool:
     return os.path.exists(os.path.join(REF_DIR, "ref_harness_" + ("mirror" if mirror else "free")))
 

@@ -11,6 +11,7 @@ project's own mesh generator can be checked without the reference present.
 
 Run in the build container (needs the reference checkout and `make -C oracle ref`):
     python tests/golden/make_golden.py [path/to/reference]
+(default: the checkout oracle/Makefile compiles from, BEM_REFERENCE).
 """
 from __future__ import annotations
 
@@ -37,7 +38,8 @@ def two_bubbles(nu, r1=1.0, r2=0.7, c1=2.5, c2=4.5):
     return v, f, phi
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
+    ref_root = ref_root or O.reference_dir()
     if not (O.ref_available(False) and O.ref_available(True)):
         raise SystemExit("build the reference first: make -C oracle ref")
     out = {}

@@ -115,3 +115,25 @@ def test_trace_mesh_misses_report_triangle_zero(sim):
     # from the centre along z the nearest crossing is at a pole of the sphere (top and bottom are at
     # equal |s| on the symmetric sphere; the first triangle in order is kept)
     assert ok[1] == 1 and abs(abs(hit[5]) - 1.0) < 0.05 and abs(hit[3] - 2.0) < 1e-12 and abs(hit[4]) < 1e-12
+
+
+def test_expired_barrier_wait_falls_back_to_the_multikernel_bicgstab():
+    # A grid-barrier bound of one clock cycle runs out at the persistent BiCGSTAB's first barrier: the
+    # kernel sets its error word and returns (no CTA is left waiting), the host counts the expired wait
+    # and finishes the solve with the multi-kernel BiCGSTAB, and psi still matches the LU solution.
+    # The context keeps the multi-kernel form: a second solve does not try the persistent kernel again.
+    v, f = mesh.bubble(6, 1.0, (2.0, 0.0, 0.0))
+    phi = 0.1 * np.sin(3 * v[:, 2]) + 0.05 * v[:, 0]
+    lu = ColocSim(v, f, solver="lu")
+    _, psi_lu = lu.position_t(phi, return_psi=True)
+    lu.close()
+    s = ColocSim(v, f, solver="bicgstab")
+    assert s._L.bem_set_wait_limit(s._h, 0) == L.BEM_ERR_ARG
+    assert s._L.bem_set_wait_limit(s._h, 1) == L.BEM_OK
+    for k in range(2):
+        _, psi = s.position_t(phi, return_psi=True)
+        st = s.stats()
+        assert st.wait_expired == 1, k
+        assert st.last_rel_residual <= 1e-14
+        assert np.max(np.abs(psi - psi_lu)) <= 1e-10 * np.max(np.abs(psi_lu))
+    s.close()

@@ -149,3 +149,19 @@ def test_exterior_potential_bit_exact():
     G, H = O.assemble(v, f)
     psi_l, _ = O.solve(G, O.gemv(H, phi), use_lu=True)
     assert np.array_equal(O.exterior_pot(v, f, phi, psi_l, pts), GOLD["ext_solve"])
+
+
+def test_config1_first_25_of_100_steps_bit_exact():
+    # the oracle against the reference's own 100-step trajectory of the same set-up
+    # (tests/golden/c1_100.npz), up to its first stored record, step 25, bit for bit
+    c1 = np.load(os.path.join(os.path.dirname(__file__), "golden", "c1_100.npz"))
+    assert int(c1["steps"][0]) == 25
+    a = mesh.bubble(7, 1.0, (2.5, 0, 0))
+    b = mesh.bubble(7, 1.0, (5.5, 0, 0))
+    v, f = mesh.join([a, b])
+    n = len(a[0])
+    prm = O.make_params(p_inf=1.0, epsilon=0.0, sigma=0.0, gamma=1.0, V0=O.volume(v, f))
+    S = O.State(v, f, np.r_[np.full(n, -0.5), np.full(n, 0.5)])
+    for s in range(25):
+        S.rk4(1e-3, prm)
+    same(_record(S), c1["records"][0])
