@@ -25,6 +25,7 @@ SOLVER_LU = 1
 SOLVER_MIXED = 2
 FLAG_BICGSTAB_MULTIKERNEL = 1
 FLAG_NO_STAGE_PREDICTOR = 2
+FLAG_STEP_ASSEMBLE_H = 4
 
 _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)
@@ -76,6 +77,7 @@ SIGNATURES = {
     "bem_get_volume": (C.c_int, [C.c_void_p, _D]),
     "bem_set_field_callback": (C.c_int, [C.c_void_p, FIELD_FN, C.c_void_p]),
     "bem_assemble": (C.c_int, [C.c_void_p, _D, _D, _D]),
+    "bem_assemble_rhs": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "bem_solve_system": (C.c_int, [C.c_void_p, _D, _D, _D]),
     "bem_position_t": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "bem_position_t_inout": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),

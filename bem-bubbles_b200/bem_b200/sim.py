@@ -187,6 +187,16 @@ class ColocSim:
         self._check(self._L.bem_assemble(self._h, _d(v) if v is not None else None, _d(G), _d(H)))
         return G, H
 
+    def assemble_rhs(self, pot, verts=None):
+        """(G, b): G and b = H*pot after the 4 pi rule as the step path forms them (position_t,
+        LinLinSim.cpp:26-83), without materialising H."""
+        p = np.ascontiguousarray(pot, dtype=np.float64)
+        G = np.empty((self.N, self.N), order="F")
+        b = np.empty(self.N)
+        v = None if verts is None else np.ascontiguousarray(verts, dtype=np.float64)
+        self._check(self._L.bem_assemble_rhs(self._h, _d(v) if v is not None else None, _d(p), _d(G), _d(b)))
+        return G, b
+
     def solve_system(self, G, b):
         G = np.asfortranarray(G, dtype=np.float64)
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -322,8 +322,12 @@ __device__ __forceinline__ void singular_sums(const double* __restrict__ x, int 
 //    thread per row walking the triangles in order.
 // A separate pass because inside the tile loop the rare singular branch cost a fifth of the tile
 // kernel's time (divergent warps waiting at the staging barriers, and the call in the hot loop).
+// GONLY (the G-only assembly of the step path, no H matrix): the partials bp are the regular pairs'
+// share of sum_j H(i, j) (phi_j - phi_i) and rowHp is unused; the singular pairs add their H entries
+// times (phi_j - phi_i), and b_i = that sum - 4 pi phi_i, which is the reference's
+// sum_j H(i, j) phi_j after the 4 pi rule H(i, i) -= 4 pi + sum_j H(i, j) (ColocSim.cpp:85-97).
 constexpr int SD_WARPS = 8;  // rows per CTA
-template <bool MIRROR>
+template <bool MIRROR, bool GONLY = false>
 __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long long mbase, int vbase, int ngroups,
                                                   const double* __restrict__ rowHp, const double* __restrict__ bp,
                                                   const double* __restrict__ x, const int* __restrict__ tri,
@@ -370,7 +374,7 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
                 }
             if (!first) continue;
             const size_t o = (size_t)mbase + (size_t)(j - vbase) * n + il;
-            double gv = G[o], hv = MIRROR ? H[o] : 0.0, gsing = 0.0;
+            double gv = G[o], hv = (MIRROR && !GONLY) ? H[o] : 0.0, gsing = 0.0;
             for (int q = me; q < ne; ++q)
                 if (s_j[w][q] == j) {
                     gv += s_g[w][q];
@@ -379,14 +383,16 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
                 }
             G[o] = gv;
             if (x0) gx = fma(gsing, x0[j], gx);
-            if (MIRROR) H[o] = hv;  // without the wall image the singular double layer vanishes (flat triangle)
+            if (MIRROR && !GONLY) H[o] = hv;  // without the wall image the singular double layer vanishes (flat triangle)
         }
-        if (MIRROR && lane == 0)
+        if (MIRROR && lane == 0) {
+            const double phii = GONLY ? phi[i] : 0.0;
             for (int q = 0; q < ne; ++q)
                 if (s_j[w][q] >= 0) {
                     rs += s_h[w][q];
-                    bsing = fma(s_h[w][q], phi[s_j[w][q]], bsing);
+                    bsing = fma(s_h[w][q], GONLY ? phi[s_j[w][q]] - phii : phi[s_j[w][q]], bsing);
                 }
+        }
         __syncwarp();
     }
     // 4 pi rule and right-hand side: lane l sums the partials of groups l, l+32, ... and the warp adds
@@ -394,7 +400,7 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
     double val = 0.0, bs = 0.0;
     const size_t pr = (size_t)il * ngroups;  // the row's partials, contiguous
     for (int g = lane; g < ngroups; g += 32) {
-        val -= rowHp[pr + g];
+        if (!GONLY) val -= rowHp[pr + g];
         bs += bp[pr + g];
     }
     if (x0)
@@ -406,17 +412,22 @@ __device__ __forceinline__ void singular_diag_row(int i, int il, int n, long lon
         gx += __shfl_xor_sync(0xffffffffu, gx, o);
     }
     if (lane) return;
-    val -= rs;
     bs += bsing;
-    const double d = -(4.0 * 3.14159265358979323846 - val);
-    const size_t oii = (size_t)mbase + (size_t)il * n + il;
-    H[oii] += d;  // after the warp's singular update of H(i, i) (ordered by the last __syncwarp)
-    const double bi = fma(d, phi[i], bs);
+    double bi;
+    if (GONLY) {
+        bi = fma(-4.0 * 3.14159265358979323846, phi[i], bs);
+    } else {
+        val -= rs;
+        const double d = -(4.0 * 3.14159265358979323846 - val);
+        const size_t oii = (size_t)mbase + (size_t)il * n + il;
+        H[oii] += d;  // after the warp's singular update of H(i, i) (ordered by the last __syncwarp)
+        bi = fma(d, phi[i], bs);
+    }
     if (b) b[i] = bi;
     if (x0) r0[i] = bi - gx;  // the first residual b - G x0 of the solve that follows
 }
 
-template <bool MIRROR>
+template <bool MIRROR, bool GONLY = false>
 __global__ void __launch_bounds__(32 * SD_WARPS)
     k_singular_diag(int N, int ngroups, const double* __restrict__ rowHp, const double* __restrict__ bp,
                     const double* __restrict__ x, const int* __restrict__ tri, const int* __restrict__ csr_off,
@@ -425,7 +436,8 @@ __global__ void __launch_bounds__(32 * SD_WARPS)
                     const double* __restrict__ gp, double* __restrict__ r0) {
     const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
     if (i >= N) return;
-    singular_diag_row<MIRROR>(i, i, N, 0, 0, ngroups, rowHp, bp, x, tri, csr_off, csr_idx, phi, G, H, b, x0, gp, r0);
+    singular_diag_row<MIRROR, GONLY>(i, i, N, 0, 0, ngroups, rowHp, bp, x, tri, csr_off, csr_idx, phi, G, H, b, x0,
+                                     gp, r0);
 }
 
 // The same per block of a batch (rows of block vblk[i], its own groups and G/H block).
@@ -728,6 +740,251 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
                                                                  T.csr_idx, phi, G, H, b, x0, c.gp, r0);
     }
     if (c.prof) {  // the profile's assembly time: tiles, singular pairs and the 4 pi rule
+        cudaEventRecord(e1, s);
+        c.ev_asm.emplace_back(e0, e1);
+    }
+}
+
+
+// ------------------------------------------------------------------------------------------------
+// G-only assembly of the step path (triangle patches)
+// ------------------------------------------------------------------------------------------------
+// The RK4 step needs G and b = H phi (after the 4 pi rule), never H itself.  Each triangle belongs
+// to exactly one patch (Topology::patch_*), so every regular (row, triangle) pair is evaluated once:
+// a CTA owns one patch and ROWS rows, accumulates the patch's columns (at most PCOLS vertices) in
+// shared memory and, per row, b's regular share sum_t sum_k H_k(i, t) (phi_k - phi_i) in a register.
+// The patch's triangle records are contiguous (patch order) and arrive in shared memory by one bulk
+// copy (cp.async.bulk, completion counted on an mbarrier) while the threads clear their accumulators.
+// A column whose vertex has all its triangles in the patch is complete and goes straight to G; the
+// columns of vertices shared with other patches go to halo columns, which k_halo_reduce sums into G in
+// increasing patch order.  The singular pairs and b's 4 pi term follow in k_singular_diag<., true>.
+// Per G entry the order is: the regular pairs of each patch in increasing triangle order, the patches
+// in increasing order, then the singular pairs; no atomics, so results are bit-reproducible.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// An mbarrier counting one arrival, initialised before any thread uses it.
+__device__ __forceinline__ void copy_bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to
+// shared memory, its completion counted on `bar` (the arrival that also announces the bytes).
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"((unsigned long long)__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Bounded wait for phase `parity` of `bar`: false after `limit` polls.
+__device__ __forceinline__ bool copy_bar_wait(uint64_t* bar, uint32_t parity, int limit) {
+    const uint32_t a = smem_addr(bar);
+    for (int it = 0; it < limit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+constexpr int COPY_WAIT_POLLS = 1 << 22;  // each poll may suspend the thread for a while: seconds in all
+
+// Patch-order triangle records (PREC doubles): the k_triangle_records layout (0-27), the potential
+// at the three vertices (28-30), the vertex ids (31, 21 bits each, as the bits of a double) and the
+// column slots of the three vertices in the patch (32, 8 bits each); 33 is padding.
+__global__ void k_patch_records(int M, const double* __restrict__ x, const double* __restrict__ phi,
+                                const int* __restrict__ tri, const int* __restrict__ ptri,
+                                const int* __restrict__ pslot, double* __restrict__ prec) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const int t = ptri[p];
+    const int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
+    const double ax = x[3 * ia], ay = x[3 * ia + 1], az = x[3 * ia + 2];
+    const double abx = x[3 * ib] - ax, aby = x[3 * ib + 1] - ay, abz = x[3 * ib + 2] - az;
+    const double bcx = x[3 * ic] - x[3 * ib], bcy = x[3 * ic + 1] - x[3 * ib + 1], bcz = x[3 * ic + 2] - x[3 * ib + 2];
+    const double nx = aby * bcz - abz * bcy, ny = abz * bcx - abx * bcz, nz = abx * bcy - aby * bcx;
+    const double area = sqrt(nx * nx + ny * ny + nz * nz);
+    const double ia_ = 1.0 / area;
+    double* r = prec + (size_t)p * PREC;
+    r[0] = ax;
+    r[1] = ay;
+    r[2] = az;
+    r[3] = 2.0 * abx;
+    r[4] = 2.0 * aby;
+    r[5] = 2.0 * abz;
+    r[6] = 2.0 * bcx;
+    r[7] = 2.0 * bcy;
+    r[8] = 2.0 * bcz;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        const double u = c_quv[q][0], v = c_quv[q][1];
+        const double wx = u * abx + v * bcx, wy = u * aby + v * bcy, wz = u * abz + v * bcz;
+        r[9 + q] = wx * wx + wy * wy + wz * wz;
+        r[16 + q] = ax + wx;
+    }
+    const double unx = nx * ia_, uny = ny * ia_, unz = nz * ia_;
+    r[23] = unx;
+    r[24] = uny;
+    r[25] = unz;
+    r[26] = area;
+    r[27] = ax * unx + ay * uny + az * unz;
+    r[28] = phi[ia];
+    r[29] = phi[ib];
+    r[30] = phi[ic];
+    r[31] = __longlong_as_double((long long)ia | ((long long)ib << 21) | ((long long)ic << 42));
+    r[32] = __longlong_as_double((long long)pslot[p]);
+    r[33] = 0.0;
+}
+
+template <int ROWS>
+constexpr size_t patch_smem() {
+    return sizeof(double) * ((size_t)PT_MAX * PREC + (size_t)PCOLS * ROWS);
+}
+
+// One CTA per (patch, row tile of ROWS rows), one row per thread.
+template <bool MIRROR, int ROWS, int MINB>
+__global__ void __launch_bounds__(ROWS, MINB)
+    k_assemble_patch(int N, int npatch, const double* __restrict__ prec, const int* __restrict__ patch_off,
+                     const int* __restrict__ patch_col, const int* __restrict__ patch_dst,
+                     const double* __restrict__ x, const double* __restrict__ phi, double* __restrict__ G,
+                     double* __restrict__ halo, double* __restrict__ bp, const double* __restrict__ x0,
+                     double* __restrict__ gp, int* __restrict__ err) {
+    extern __shared__ __align__(16) double psmem[];
+    double* srec = psmem;                  // [PT_MAX][PREC], the patch's records
+    double* acc = psmem + PT_MAX * PREC;   // [PCOLS][ROWS], this CTA's rows of the patch's columns
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_col[PCOLS], s_dst[PCOLS];
+    const int p = blockIdx.x, tid = threadIdx.x;
+    const int i = blockIdx.y * ROWS + tid;
+    const int t0 = patch_off[p], nt = patch_off[p + 1] - t0;
+    if (tid == 0) copy_bar_init(&bar);
+    __syncthreads();
+    if (tid == 0) bulk_copy_g2s(srec, prec + (size_t)t0 * PREC, (uint32_t)(nt * PREC * sizeof(double)), &bar);
+    if (tid < PCOLS) {
+        s_col[tid] = patch_col[p * PCOLS + tid];
+        s_dst[tid] = patch_dst[p * PCOLS + tid];
+    }
+#pragma unroll 8
+    for (int s = 0; s < PCOLS; ++s) acc[s * ROWS + tid] = 0.0;
+    const bool row = i < N;
+    double xi0 = 0.0, xi1 = 0.0, xi2 = 0.0, phii = 0.0;
+    if (row) {
+        xi0 = x[3 * i];
+        xi1 = x[3 * i + 1];
+        xi2 = x[3 * i + 2];
+        phii = phi[i];
+    }
+    if (!__syncthreads_and(copy_bar_wait(&bar, 0, COPY_WAIT_POLLS))) {
+        // the records did not arrive in time: record the error, let the copy land (bounded) before the
+        // CTA's shared memory is released, and leave this tile unwritten (the host reports the error)
+        if (tid == 0) {
+            atomicExch(err, 1);
+            copy_bar_wait(&bar, 0, COPY_WAIT_POLLS);
+        }
+        return;
+    }
+    if (!row) return;
+    double hb = 0.0;  // sum over this patch's regular pairs of sum_k H_k (phi_k - phi_i)
+    for (int t = 0; t < nt; ++t) {
+        const double* r = srec + t * PREC;
+        const long long ids = __double_as_longlong(r[31]);
+        if (i == (int)(ids & 0x1FFFFF) || i == (int)((ids >> 21) & 0x1FFFFF) || i == (int)(ids >> 42))
+            continue;  // singular pair: k_singular_diag
+        PairSums ps;
+        regular_pair<MIRROR>(r, xi0, xi1, xi2, ps);
+        const int code = (int)__double_as_longlong(r[32]);
+        const int s0 = code & 255, s1 = (code >> 8) & 255, s2 = (code >> 16) & 255;
+        acc[s0 * ROWS + tid] = fma(ps.g[0], ps.area, acc[s0 * ROWS + tid]);
+        acc[s1 * ROWS + tid] = fma(ps.g[1], ps.area, acc[s1 * ROWS + tid]);
+        acc[s2 * ROWS + tid] = fma(ps.g[2], ps.area, acc[s2 * ROWS + tid]);
+        const double e0 = r[28] - phii, e1 = r[29] - phii, e2 = r[30] - phii;
+        hb = fma(fma(ps.h[0], e0, fma(ps.h[1], e1, __dmul_rn(ps.h[2], e2))), ps.sh, hb);
+        if (MIRROR) hb = fma(fma(ps.m[0], e0, fma(ps.m[1], e1, __dmul_rn(ps.m[2], e2))), ps.sm, hb);
+    }
+    double gs = 0.0;
+    for (int s = 0; s < PCOLS; ++s) {
+        const int v = s_col[s];
+        if (v < 0) break;
+        const double gv = acc[s * ROWS + tid];
+        const int h = s_dst[s];
+        if (h < 0)
+            G[(size_t)v * N + i] = gv;
+        else
+            halo[(size_t)h * N + i] = gv;
+        if (x0) gs = fma(gv, x0[v], gs);
+    }
+    const size_t po = (size_t)i * npatch + p;  // row-major partials, as the column-group tiles write them
+    bp[po] = hb;
+    if (x0) gp[po] = gs;
+}
+
+// G(:, v) of each partial vertex: its halo columns summed in increasing patch order.
+__global__ void k_halo_reduce(int N, const int* __restrict__ halo_vert, const int* __restrict__ halo_off,
+                              const double* __restrict__ halo, double* __restrict__ G) {
+    const int k = blockIdx.x, i = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int h0 = halo_off[k], h1 = halo_off[k + 1];
+    double s = halo[(size_t)h0 * N + i];
+    for (int h = h0 + 1; h < h1; ++h) s += halo[(size_t)h * N + i];
+    G[(size_t)halo_vert[k] * N + i] = s;
+}
+
+constexpr int PATCH_ROWS = 256;
+
+template <bool MIRROR>
+static void launch_patch_tiles(Ctx& c, const double* x, const double* phi, double* G, const double* x0,
+                               cudaStream_t s) {
+    const Topology& T = c.topo;
+    const int N = (int)T.N;
+    constexpr size_t sm = patch_smem<PATCH_ROWS>();
+    auto kern = k_assemble_patch<MIRROR, PATCH_ROWS, 3>;
+    static std::atomic<uint64_t> attr{0};
+    once_per_device(attr, [kern] {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess;
+    });
+    dim3 grid(T.npatch, (N + PATCH_ROWS - 1) / PATCH_ROWS);
+    KLAUNCH(), kern<<<grid, PATCH_ROWS, sm, s>>>(N, T.npatch, c.prec, T.patch_off, T.patch_col, T.patch_dst, x, phi, G,
+                                                 c.halo, c.bp, x0, c.gp, c.asm_err);
+}
+
+// G (the context's G) and b = H phi after the 4 pi rule for positions x, potential phi, without H; with
+// x0 (may be null) also r0 = b - G x0.  Single systems without pinned vertices.
+void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cudaStream_t s, const double* x0,
+                       double* r0) {
+    const Topology& T = c.topo;
+    const int N = (int)T.N, M = (int)T.M;
+    if (!r0) x0 = nullptr;
+    upload_constants();
+    KLAUNCH(), k_patch_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, phi, T.tri, T.patch_tri, T.patch_slot, c.prec);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c.prof) {
+        e0 = c.take_event();
+        e1 = c.take_event();
+        cudaEventRecord(e0, s);
+    }
+    if (c.prm.mirror)
+        launch_patch_tiles<true>(c, x, phi, c.G, x0, s);
+    else
+        launch_patch_tiles<false>(c, x, phi, c.G, x0, s);
+    if (T.npartial > 0)
+        KLAUNCH(), k_halo_reduce<<<dim3(T.npartial, (N + 255) / 256), 256, 0, s>>>(N, T.halo_vert, T.halo_off, c.halo,
+                                                                                c.G);
+    const int nbs = (N + SD_WARPS - 1) / SD_WARPS, nt = 32 * SD_WARPS;
+    if (c.prm.mirror)
+        KLAUNCH(), k_singular_diag<true, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
+                                                                  T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
+    else
+        KLAUNCH(), k_singular_diag<false, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
+                                                                   T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
+    if (c.prof) {  // the profile's assembly time: tiles, halo reduction, singular pairs and the 4 pi rule
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }

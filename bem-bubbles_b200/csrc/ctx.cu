@@ -46,6 +46,8 @@ static void free_all(Ctx& c, bool keep_blocks = false) {
     c.xinv_valid = false;
     // every pointer into the freed allocations
     c.G = c.H = c.LU = nullptr;
+    c.prec = c.halo = nullptr;
+    c.asm_err = nullptr;
     c.pbicg = nullptr;
     c.lu_aux = nullptr;
     c.Xinv = c.Tw = c.G32 = nullptr;
@@ -95,7 +97,110 @@ struct HostTopo {
         part_tidx, tri_rot;
     int ngroups = 0, nparts = 0;
     std::vector<int> blk_gbase;  // first group of each block (+ end), batches only
+    // triangle patches of the G-only assembly (Topology::patch_*, halo_*); single systems only
+    std::vector<int> patch_off, patch_tri, patch_slot, patch_col, patch_dst, halo_vert, halo_off;
+    int npatch = 0, nhalo = 0;
 };
+
+// Triangle patches: recursive coordinate bisection of the triangle centroids into patches of at most
+// PT_MAX triangles, a patch split again while it touches more than PCOLS vertices.  A vertex whose
+// incident triangles all lie in one patch is a complete column of that patch (the tile writes its
+// G column); any other vertex is partial: each patch touching it writes a halo column, in increasing
+// patch order, and the halo reduction sums them into its G column.
+static void build_patches(int64_t N, int64_t M, const double* verts, HostTopo& h) {
+    std::vector<double> cen((size_t)(3 * M));
+    for (int64_t j = 0; j < M; ++j)
+        for (int d = 0; d < 3; ++d) {
+            const int* t = &h.tri[(size_t)(3 * j)];
+            cen[(size_t)(3 * j + d)] = (verts[3 * (size_t)t[0] + d] + verts[3 * (size_t)t[1] + d] + verts[3 * (size_t)t[2] + d]) / 3.0;
+        }
+    std::vector<int> idx((size_t)M);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::vector<std::vector<int>> leaves;
+    struct Rec {
+        static int ncols(const std::vector<int>& tri, const int* b, const int* e) {
+            std::vector<int> vs;
+            for (const int* p = b; p != e; ++p)
+                for (int k = 0; k < 3; ++k) vs.push_back(tri[(size_t)(3 * *p + k)]);
+            std::sort(vs.begin(), vs.end());
+            return (int)(std::unique(vs.begin(), vs.end()) - vs.begin());
+        }
+        static void go(std::vector<int>& idx, int lo, int hi, const std::vector<double>& xyz,
+                       const std::vector<int>& tri, std::vector<std::vector<int>>& out) {
+            const int n = hi - lo;
+            if (n <= PT_MAX && (n == 1 || ncols(tri, idx.data() + lo, idx.data() + hi) <= PCOLS)) {
+                out.emplace_back(idx.begin() + lo, idx.begin() + hi);
+                return;
+            }
+            double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+            for (int k = lo; k < hi; ++k)
+                for (int d = 0; d < 3; ++d) {
+                    mn[d] = std::min(mn[d], xyz[3 * (size_t)idx[(size_t)k] + d]);
+                    mx[d] = std::max(mx[d], xyz[3 * (size_t)idx[(size_t)k] + d]);
+                }
+            int ax = 0;
+            for (int d = 1; d < 3; ++d)
+                if (mx[d] - mn[d] > mx[ax] - mn[ax]) ax = d;
+            std::stable_sort(idx.begin() + lo, idx.begin() + hi,
+                             [&](int a, int b) { return xyz[3 * (size_t)a + ax] < xyz[3 * (size_t)b + ax]; });
+            // full patches of PT_MAX on the left where the count allows; halves once a patch of
+            // PT_MAX or fewer triangles is still too wide
+            const int nparts = (n + PT_MAX - 1) / PT_MAX;
+            const int left = nparts > 1 ? (nparts / 2) * PT_MAX : n / 2;
+            go(idx, lo, lo + left, xyz, tri, out);
+            go(idx, lo + left, hi, xyz, tri, out);
+        }
+    };
+    Rec::go(idx, 0, (int)M, cen, h.tri, leaves);
+    const int np = (int)leaves.size();
+    h.npatch = np;
+    h.patch_off.assign((size_t)np + 1, 0);
+    h.patch_tri.clear();
+    h.patch_slot.clear();
+    h.patch_col.assign((size_t)np * PCOLS, -1);
+    h.patch_dst.assign((size_t)np * PCOLS, -1);
+    std::vector<int> touch_cnt((size_t)N, 0);
+    for (int p = 0; p < np; ++p) {
+        auto& L = leaves[(size_t)p];
+        std::sort(L.begin(), L.end());  // the reference's per-column order: increasing triangle index
+        std::vector<int> vs;
+        for (int t : L)
+            for (int k = 0; k < 3; ++k) vs.push_back(h.tri[(size_t)(3 * t + k)]);
+        std::sort(vs.begin(), vs.end());
+        vs.erase(std::unique(vs.begin(), vs.end()), vs.end());
+        for (size_t s = 0; s < vs.size(); ++s) {
+            h.patch_col[(size_t)p * PCOLS + s] = vs[s];
+            touch_cnt[(size_t)vs[s]]++;
+        }
+        for (int t : L) {
+            int code = 0;
+            for (int k = 0; k < 3; ++k) {
+                const int v = h.tri[(size_t)(3 * t + k)];
+                const int s = (int)(std::lower_bound(vs.begin(), vs.end(), v) - vs.begin());
+                code |= s << (8 * k);
+            }
+            h.patch_tri.push_back(t);
+            h.patch_slot.push_back(code);
+        }
+        h.patch_off[(size_t)p + 1] = (int)h.patch_tri.size();
+    }
+    // halo columns of the partial vertices: vertex by vertex, each vertex's in increasing patch order
+    std::vector<int> hbase((size_t)N, -1), hnext((size_t)N, 0);
+    h.halo_vert.clear();
+    h.halo_off.assign(1, 0);
+    for (int64_t v = 0; v < N; ++v)
+        if (touch_cnt[(size_t)v] > 1) {
+            hbase[(size_t)v] = h.halo_off.back();
+            h.halo_vert.push_back((int)v);
+            h.halo_off.push_back(h.halo_off.back() + touch_cnt[(size_t)v]);
+        }
+    h.nhalo = h.halo_off.back();
+    for (int p = 0; p < np; ++p)
+        for (int s = 0; s < PCOLS; ++s) {
+            const int v = h.patch_col[(size_t)p * PCOLS + s];
+            if (v >= 0 && hbase[(size_t)v] >= 0) h.patch_dst[(size_t)p * PCOLS + s] = hbase[(size_t)v] + hnext[(size_t)v]++;
+        }
+}
 
 // blocks: vertex offsets of independent sub-systems (size nblocks + 1); column groups never span
 // two of them.  Empty: one block [0, N).
@@ -239,6 +344,7 @@ static int build_topology(int64_t N, int64_t M, const int64_t* trigs, const doub
         }
         h.grp_off[(size_t)g + 1] = (int)h.grp_tri.size();
     }
+    if (blocks.empty()) build_patches(N, M, verts, h);
     return BEM_OK;
 }
 
@@ -301,7 +407,10 @@ static void assemble_system(Ctx& c, const double* x, const double* pot, const do
                             const double* x0 = nullptr) {
     c.r0_ready = false;
     if (c.n_pin == 0) {
-        launch_assemble(c, x, pot, c.G, c.H, c.b, s, x0, x0 ? c.r : nullptr);
+        if (!c.batch && c.topo.npatch > 0 && !(c.prm.flags & BEM_FLAG_STEP_ASSEMBLE_H))
+            launch_assemble_g(c, x, pot, c.b, s, x0, x0 ? c.r : nullptr);  // the step needs no H
+        else
+            launch_assemble(c, x, pot, c.G, c.H, c.b, s, x0, x0 ? c.r : nullptr);
         c.r0_ready = x0 != nullptr && !c.batch;
         return;
     }
@@ -366,12 +475,22 @@ static int pot_t_multi(Ctx& c, const double* x, const double* vel, double* out, 
     return BEM_OK;
 }
 
+// Error word of the G-only assembly (a bulk copy of triangle records that did not complete in time),
+// read after the stream synchronised; cleared once reported.
+static int check_assembly_error(Ctx& c, const int& word, cudaStream_t s) {
+    if (!word) return BEM_OK;
+    cudaMemsetAsync(c.asm_err, 0, sizeof(int), s);
+    return c.fail(BEM_ERR_CUDA, "assembly: a bulk copy of triangle records did not complete (bounded wait expired)");
+}
+
 static int check_negative(Ctx& c, cudaStream_t s) {
-    int f = 0;
+    int f = 0, ae = 0;
     BEM_CUDA(c, cudaMemsetAsync(c.flag + 1, 0, sizeof(int), s));
     launch_any_negative(c, c.x, c.flag + 1, s);
     BEM_CUDA(c, cudaMemcpyAsync(&f, c.flag + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (c.asm_err) BEM_CUDA(c, cudaMemcpyAsync(&ae, c.asm_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));
+    if (int rc = check_assembly_error(c, ae, s)) return rc;
     if (f) return c.fail(BEM_ERR_NEGATIVE_X, "negative values");  // test_negative, LinLinSim.cpp:148-159
     return BEM_OK;
 }
@@ -481,10 +600,19 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = upload(c, &t.part_off, h.part_off)) || (rc = upload(c, &t.part_tidx, h.part_tidx)) ||
         (rc = upload(c, &t.tri_rot, h.tri_rot)))
         return rc;
+    t.npatch = h.npatch;
+    t.nhalo = h.nhalo;
+    t.npartial = (int)h.halo_vert.size();
+    if (h.npatch > 0 &&
+        ((rc = upload(c, &t.patch_off, h.patch_off)) || (rc = upload(c, &t.patch_tri, h.patch_tri)) ||
+         (rc = upload(c, &t.patch_slot, h.patch_slot)) || (rc = upload(c, &t.patch_col, h.patch_col)) ||
+         (rc = upload(c, &t.patch_dst, h.patch_dst)) || (t.npartial > 0 && (rc = upload(c, &t.halo_vert, h.halo_vert))) ||
+         (rc = upload(c, &t.halo_off, h.halo_off))))
+        return rc;
     const size_t n = (size_t)N, m = (size_t)M;
     // dense N x N, or the packed blocks of a batch
     const size_t nn = c.batch ? (size_t)c.blk_elems : n * n;
-    size_t nrow_part = (size_t)h.ngroups * n;
+    size_t nrow_part = (size_t)std::max(h.ngroups, h.npatch) * n;
     if (c.batch) {
         nrow_part = 0;
         for (auto& B : c.h_blk) nrow_part += (size_t)B.ngroups * B.n;
@@ -510,6 +638,15 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (!c.batch && (rc = dalloc(c, &c.psih_t, (size_t)PRED_CNT + 1))))
         return rc;
     if (c.psih_t) BEM_CUDA(c, cudaMemset(c.psih_t, 0, sizeof(double) * (PRED_CNT + 1)));
+    if (h.npatch > 0) {
+        // the step path writes no H: its storage holds the halo columns when they fit
+        if ((rc = dalloc(c, &c.prec, m * PREC)) || (rc = dalloc(c, &c.asm_err, 4))) return rc;
+        if ((size_t)h.nhalo <= n)
+            c.halo = c.H;
+        else if ((rc = dalloc(c, &c.halo, (size_t)h.nhalo * n)))
+            return rc;
+        BEM_CUDA(c, cudaMemset(c.asm_err, 0, sizeof(int) * 4));
+    }
     if (!c.batch && c.prm.solver == BEM_SOLVER_MIXED) {
         if ((rc = alloc_mixed(c))) return rc;
     }
@@ -1254,6 +1391,28 @@ int bem_assemble(bem_ctx* c, const double* verts, double* G, double* H) {
     if (H) COPY_OUT(H, c->H, nn);
     BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
     return BEM_OK;
+}
+
+int bem_assemble_rhs(bem_ctx* c, const double* verts, const double* pot, double* G, double* b) {
+    CTX_GUARD(c);
+    NEED_MESH(c);
+    if (!pot) return c->fail(BEM_ERR_ARG, "bem_assemble_rhs: pot is required");
+    if (c->batch) return c->fail(BEM_ERR_STATE, "bem_assemble_rhs: single systems only");
+    const int64_t N = c->topo.N;
+    const double* x = c->x;
+    if (verts) {
+        COPY_IN(c->xs, verts, 3 * N);
+        x = c->xs;
+    }
+    COPY_IN(c->p1, pot, N);
+    assemble_system(*c, x, c->p1, c->psi, c->stream);
+    BEM_CUDA(*c, cudaGetLastError());
+    if (G) COPY_OUT(G, c->G, N * N);
+    if (b) COPY_OUT(b, c->b, N);
+    int ae = 0;
+    if (c->asm_err) BEM_CUDA(*c, cudaMemcpyAsync(&ae, c->asm_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    BEM_CUDA(*c, cudaStreamSynchronize(c->stream));
+    return check_assembly_error(*c, ae, c->stream);
 }
 
 int bem_solve_system(bem_ctx* c, const double* G, const double* b, double* x) {

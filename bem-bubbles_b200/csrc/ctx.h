@@ -96,6 +96,11 @@ struct Ctx {
     double* pbicg = nullptr;   // persistent BiCGSTAB: per-row-block dots, barrier and error words
     bool pbicg_ok = true;      // the persistent BiCGSTAB is usable (cleared after a failed launch or wait)
     long long wait_limit = 2000000000LL;  // bound of the persistent kernels' grid-barrier waits, SM cycles
+    // G-only assembly of the step path: patch-ordered triangle records, halo columns (nhalo x N; the
+    // storage of H when nhalo <= N, since the step path does not write H), error word of its bulk copies
+    double* prec = nullptr;
+    double* halo = nullptr;
+    int* asm_err = nullptr;
     bool xinv_valid = false;
     int mixed_backoff = 0;  // solves left that skip the mixed path after it failed (FP64 BiCGSTAB instead)
     int ir_base = -1;       // fewest refinement steps of a solve since the last refresh of X

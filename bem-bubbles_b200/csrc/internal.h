@@ -48,6 +48,12 @@ constexpr int SLOT_NONE = 127;
 constexpr int ASM_TC = 40;
 // Doubles per triangle record: 7 quadrature points (21), unit normal (3), area (1), pad (3).
 constexpr int REC = 28;
+// Triangle patches of the G-only assembly (the step path): every triangle belongs to exactly one
+// patch of at most PT_MAX triangles touching at most PCOLS vertices (the patch's columns); a patch
+// record of PREC doubles per triangle (272 bytes, a multiple of 16 for the bulk copy).
+constexpr int PT_MAX = 32;
+constexpr int PCOLS = 32;
+constexpr int PREC = 34;
 // Fixed block count of the vector kernels, so reductions have a fixed, deterministic shape.
 constexpr int VBLK = 128;
 constexpr int VTHR = 256;
@@ -72,6 +78,16 @@ struct Topology {
     int* tri_rot = nullptr;      // M*3: triangles rotated so the largest vertex id comes first,
                                  // the vertex order split_by_loose_parts leaves (Mesh.cpp:410-426)
     std::vector<int> h_part_of_vert;
+    // triangle patches (single systems; npatch = 0 for batches)
+    int npatch = 0;
+    int* patch_off = nullptr;    // npatch+1 into patch_tri
+    int* patch_tri = nullptr;    // M: triangle ids, patch by patch, increasing inside a patch
+    int* patch_slot = nullptr;   // M: the column slots of the triangle's 3 vertices, 8 bits each
+    int* patch_col = nullptr;    // npatch*PCOLS: vertex of each column slot, -1 padding
+    int* patch_dst = nullptr;    // npatch*PCOLS: halo column of a partial slot, -1 for a complete column
+    int npartial = 0, nhalo = 0; // vertices with contributions from several patches; their halo columns
+    int* halo_vert = nullptr;    // npartial
+    int* halo_off = nullptr;     // npartial+1: halo columns of partial vertex k (patch order)
 };
 
 // Control block of the iterative solvers and RK4 scalars, resident on the device.
@@ -110,6 +126,9 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
                      cudaStream_t s, const double* x0 = nullptr,
                      double* r0 = nullptr);
 void prepare_assemble(Ctx& c);  // kernel attributes and the persistent grid, outside any capture
+// G and b (no H) through the triangle-patch kernels: single systems without pinned vertices
+void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cudaStream_t s,
+                       const double* x0 = nullptr, double* r0 = nullptr);
 
 // stage.cu
 void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s);

@@ -71,6 +71,10 @@ typedef struct {
  * instead of the stage predictor (an extrapolation in time from the same stage of the last three
  * steps).  Either start converges to the same FP64 solution; the predictor saves refinement steps. */
 #define BEM_FLAG_NO_STAGE_PREDICTOR 2
+/* bem_params.flags: the step path (position_t, RK4, Euler) assembles H as well, with the column-group
+ * kernel of bem_assemble, instead of the G-only triangle-patch kernel that forms b = H phi without
+ * H.  Both give the same G and b to rounding; for comparison. */
+#define BEM_FLAG_STEP_ASSEMBLE_H 4
 
 /* Fill *p with the reference's defaults. */
 void bem_default_params(bem_params* p);
@@ -117,6 +121,12 @@ int bem_set_field_callback(bem_ctx* ctx, bem_field_fn fn, void* user);
 /* ColocSim::assemble_matrices (Bem/Simulation/ColocSim.cpp:21-110) for the given vertex positions
  * (NULL = the context's mesh).  G and H are host N x N column-major outputs; either may be NULL. */
 int bem_assemble(bem_ctx* ctx, const double* verts, double* G, double* H);
+/* G and the right-hand side b = H*pot (after the 4 pi rule) as the step path forms them for
+ * position_t (LinLinSim.cpp:26-83: assemble_matrices, then H*phi), for positions `verts` (NULL =
+ * the context's mesh).  Single systems without pinned vertices use the G-only triangle-patch kernel,
+ * which never forms H; otherwise the bem_assemble kernel.  G (N x N column-major) and b (N) are host
+ * outputs; either may be NULL. */
+int bem_assemble_rhs(bem_ctx* ctx, const double* verts, const double* pot, double* G, double* b);
 /* Simulation::solve_system (Simulation.cpp:40-71): x = G^{-1} b with the context's solver. */
 int bem_solve_system(bem_ctx* ctx, const double* G, const double* b, double* x);
 /* LinLinSim::position_t (LinLinSim.cpp:26-83): vertex velocities for positions `verts` (NULL = mesh)
