@@ -653,7 +653,10 @@ static void launch_batch_t(Ctx& c, const double* x, const double* phi, double* G
 // Tile shapes: 16 columns x 256 rows (24 warps/SM, more boundary triangles), 32 x 128 (12 warps/SM),
 // 48 x 64 and 64 x 64 (fewer boundary triangles, 6 warps/SM); all at 3 CTAs per SM within the 228 KB
 // of shared memory.
+void prepare_assemble_g(Ctx& c);
+
 void prepare_assemble(Ctx& c) {
+    if (c.topo.npatch > 0) prepare_assemble_g(c);
     if (!c.batch) return;
     c.asm_grid_cg = 0;
     if (c.prm.mirror) {
@@ -849,32 +852,38 @@ constexpr size_t patch_smem() {
     return sizeof(double) * ((size_t)PT_MAX * PREC + (size_t)PCOLS * ROWS);
 }
 
-// One CTA per (patch, row tile of ROWS rows), one row per thread.
+// One CTA per tile {patch, first row} of the work list, ROWS rows of the patch's block, one row per
+// thread.  G, the halo columns and the row partials are addressed through the patch's PatchInfo, so
+// the same kernel serves a single system (one block) and a batch of independent bubbles.
 template <bool MIRROR, int ROWS, int MINB>
 __global__ void __launch_bounds__(ROWS, MINB)
-    k_assemble_patch(int N, int npatch, const double* __restrict__ prec, const int* __restrict__ patch_off,
-                     const int* __restrict__ patch_col, const int* __restrict__ patch_dst,
-                     const double* __restrict__ x, const double* __restrict__ phi, double* __restrict__ G,
-                     double* __restrict__ halo, double* __restrict__ bp, const double* __restrict__ x0,
-                     double* __restrict__ gp, int* __restrict__ err) {
+    k_assemble_patch(const int2* __restrict__ work, const PatchInfo* __restrict__ pinfo,
+                     const double* __restrict__ prec, const int* __restrict__ patch_col,
+                     const long long* __restrict__ patch_dst, const double* __restrict__ x,
+                     const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ halo,
+                     double* __restrict__ bp, const double* __restrict__ x0, double* __restrict__ gp,
+                     int* __restrict__ err) {
     extern __shared__ __align__(16) double psmem[];
     double* srec = psmem;                  // [PT_MAX][PREC], the patch's records
     double* acc = psmem + PT_MAX * PREC;   // [PCOLS][ROWS], this CTA's rows of the patch's columns
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_col[PCOLS], s_dst[PCOLS];
-    const int p = blockIdx.x, tid = threadIdx.x;
-    const int i = blockIdx.y * ROWS + tid;
-    const int t0 = patch_off[p], nt = patch_off[p + 1] - t0;
+    __shared__ int s_col[PCOLS];
+    __shared__ long long s_dst[PCOLS];
+    const int tid = threadIdx.x;
+    const int2 wk = work[blockIdx.x];
+    const int p = wk.x;
+    const PatchInfo P = pinfo[p];
+    const int i = wk.y + tid;  // row (global vertex index)
     if (tid == 0) copy_bar_init(&bar);
     __syncthreads();
-    if (tid == 0) bulk_copy_g2s(srec, prec + (size_t)t0 * PREC, (uint32_t)(nt * PREC * sizeof(double)), &bar);
+    if (tid == 0) bulk_copy_g2s(srec, prec + (size_t)P.t0 * PREC, (uint32_t)(P.nt * PREC * sizeof(double)), &bar);
     if (tid < PCOLS) {
         s_col[tid] = patch_col[p * PCOLS + tid];
         s_dst[tid] = patch_dst[p * PCOLS + tid];
     }
 #pragma unroll 8
     for (int s = 0; s < PCOLS; ++s) acc[s * ROWS + tid] = 0.0;
-    const bool row = i < N;
+    const bool row = i < P.vbase + P.n;
     double xi0 = 0.0, xi1 = 0.0, xi2 = 0.0, phii = 0.0;
     if (row) {
         xi0 = x[3 * i];
@@ -893,7 +902,7 @@ __global__ void __launch_bounds__(ROWS, MINB)
     }
     if (!row) return;
     double hb = 0.0;  // sum over this patch's regular pairs of sum_k H_k (phi_k - phi_i)
-    for (int t = 0; t < nt; ++t) {
+    for (int t = 0; t < P.nt; ++t) {
         const double* r = srec + t * PREC;
         const long long ids = __double_as_longlong(r[31]);
         if (i == (int)(ids & 0x1FFFFF) || i == (int)((ids >> 21) & 0x1FFFFF) || i == (int)(ids >> 42))
@@ -909,60 +918,76 @@ __global__ void __launch_bounds__(ROWS, MINB)
         hb = fma(fma(ps.h[0], e0, fma(ps.h[1], e1, __dmul_rn(ps.h[2], e2))), ps.sh, hb);
         if (MIRROR) hb = fma(fma(ps.m[0], e0, fma(ps.m[1], e1, __dmul_rn(ps.m[2], e2))), ps.sm, hb);
     }
+    const int il = i - P.vbase;
     double gs = 0.0;
     for (int s = 0; s < PCOLS; ++s) {
         const int v = s_col[s];
         if (v < 0) break;
         const double gv = acc[s * ROWS + tid];
-        const int h = s_dst[s];
+        const long long h = s_dst[s];
         if (h < 0)
-            G[(size_t)v * N + i] = gv;
+            G[P.mbase + (long long)(v - P.vbase) * P.n + il] = gv;
         else
-            halo[(size_t)h * N + i] = gv;
+            halo[h + il] = gv;
         if (x0) gs = fma(gv, x0[v], gs);
     }
-    const size_t po = (size_t)i * npatch + p;  // row-major partials, as the column-group tiles write them
+    const long long po = P.pbase + (long long)il * P.np + P.lp;  // the row's partials are contiguous
     bp[po] = hb;
     if (x0) gp[po] = gs;
 }
 
-// G(:, v) of each partial vertex: its halo columns summed in increasing patch order.
-__global__ void k_halo_reduce(int N, const int* __restrict__ halo_vert, const int* __restrict__ halo_off,
-                              const double* __restrict__ halo, double* __restrict__ G) {
-    const int k = blockIdx.x, i = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const int h0 = halo_off[k], h1 = halo_off[k + 1];
-    double s = halo[(size_t)h0 * N + i];
-    for (int h = h0 + 1; h < h1; ++h) s += halo[(size_t)h * N + i];
-    G[(size_t)halo_vert[k] * N + i] = s;
+// G column of each partial vertex: its halo columns summed in increasing patch order.
+__global__ void k_halo_reduce(const PartialCol* __restrict__ pcol, const double* __restrict__ halo,
+                              double* __restrict__ G) {
+    const PartialCol pc = pcol[blockIdx.x];
+    const int i = blockIdx.y * blockDim.x + threadIdx.x;
+    if (i >= pc.n) return;
+    const double* h = halo + pc.hpos + i;
+    double s = h[0];
+    for (int c = 1; c < pc.cnt; ++c) s += h[(size_t)c * pc.n];
+    G[pc.gpos + i] = s;
 }
 
-constexpr int PATCH_ROWS = 256;
+// The G-only singular pass of a batch: rows of block vblk[i], its patches' row partials.
+template <bool MIRROR>
+__global__ void __launch_bounds__(32 * SD_WARPS)
+    k_singular_diag_batch_g(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
+                            const double* __restrict__ bp, const double* __restrict__ x, const int* __restrict__ tri,
+                            const int* __restrict__ csr_off, const int* __restrict__ csr_idx,
+                            const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ b) {
+    const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
+    if (i >= N) return;
+    const BlockInfo B = blk[vblk[i]];
+    singular_diag_row<MIRROR, true>(i, i - B.vbase, B.n, B.mbase, B.vbase, B.npatch, nullptr, bp + B.ppbase, x, tri,
+                                    csr_off, csr_idx, phi, G, nullptr, b, nullptr, nullptr, nullptr);
+}
 
 template <bool MIRROR>
-static void launch_patch_tiles(Ctx& c, const double* x, const double* phi, double* G, const double* x0,
-                               cudaStream_t s) {
-    const Topology& T = c.topo;
-    const int N = (int)T.N;
-    constexpr size_t sm = patch_smem<PATCH_ROWS>();
-    auto kern = k_assemble_patch<MIRROR, PATCH_ROWS, 3>;
+static bool prepare_patch_t() {
     static std::atomic<uint64_t> attr{0};
-    once_per_device(attr, [kern] {
-        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess;
+    return once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_assemble_patch<MIRROR, PATCH_ROWS, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)patch_smem<PATCH_ROWS>()) == cudaSuccess;
     });
-    dim3 grid(T.npatch, (N + PATCH_ROWS - 1) / PATCH_ROWS);
-    KLAUNCH(), kern<<<grid, PATCH_ROWS, sm, s>>>(N, T.npatch, c.prec, T.patch_off, T.patch_col, T.patch_dst, x, phi, G,
-                                                 c.halo, c.bp, x0, c.gp, c.asm_err);
+}
+
+// Kernel attributes and __constant__ tables of the G-only assembly, outside any stream capture.
+void prepare_assemble_g(Ctx& c) {
+    upload_constants();
+    if (c.prm.mirror)
+        prepare_patch_t<true>();
+    else
+        prepare_patch_t<false>();
 }
 
 // G (the context's G) and b = H phi after the 4 pi rule for positions x, potential phi, without H; with
-// x0 (may be null) also r0 = b - G x0.  Single systems without pinned vertices.
+// x0 (may be null; single systems) also r0 = b - G x0.  No pinned vertices.
 void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cudaStream_t s, const double* x0,
                        double* r0) {
     const Topology& T = c.topo;
     const int N = (int)T.N, M = (int)T.M;
-    if (!r0) x0 = nullptr;
-    upload_constants();
+    if (!r0 || c.batch) x0 = nullptr;
+    prepare_assemble_g(c);
     KLAUNCH(), k_patch_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, phi, T.tri, T.patch_tri, T.patch_slot, c.prec);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c.prof) {
@@ -970,20 +995,32 @@ void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cu
         e1 = c.take_event();
         cudaEventRecord(e0, s);
     }
+    constexpr size_t sm = patch_smem<PATCH_ROWS>();
     if (c.prm.mirror)
-        launch_patch_tiles<true>(c, x, phi, c.G, x0, s);
+        KLAUNCH(), k_assemble_patch<true, PATCH_ROWS, 3><<<T.nwork, PATCH_ROWS, sm, s>>>(
+                       T.pwork, T.pinfo, c.prec, T.patch_col, T.patch_dst, x, phi, c.G, c.halo, c.bp, x0, c.gp,
+                       c.asm_err);
     else
-        launch_patch_tiles<false>(c, x, phi, c.G, x0, s);
+        KLAUNCH(), k_assemble_patch<false, PATCH_ROWS, 3><<<T.nwork, PATCH_ROWS, sm, s>>>(
+                       T.pwork, T.pinfo, c.prec, T.patch_col, T.patch_dst, x, phi, c.G, c.halo, c.bp, x0, c.gp,
+                       c.asm_err);
     if (T.npartial > 0)
-        KLAUNCH(), k_halo_reduce<<<dim3(T.npartial, (N + 255) / 256), 256, 0, s>>>(N, T.halo_vert, T.halo_off, c.halo,
-                                                                                c.G);
+        KLAUNCH(), k_halo_reduce<<<dim3(T.npartial, (T.max_block_n + 255) / 256), 256, 0, s>>>(T.pcol, c.halo, c.G);
     const int nbs = (N + SD_WARPS - 1) / SD_WARPS, nt = 32 * SD_WARPS;
-    if (c.prm.mirror)
+    if (c.batch) {
+        if (c.prm.mirror)
+            KLAUNCH(), k_singular_diag_batch_g<true><<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.bp, x, T.tri, T.csr_off,
+                                                                        T.csr_idx, phi, c.G, b);
+        else
+            KLAUNCH(), k_singular_diag_batch_g<false><<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.bp, x, T.tri, T.csr_off,
+                                                                         T.csr_idx, phi, c.G, b);
+    } else if (c.prm.mirror) {
         KLAUNCH(), k_singular_diag<true, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
                                                                   T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
-    else
+    } else {
         KLAUNCH(), k_singular_diag<false, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
                                                                    T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
+    }
     if (c.prof) {  // the profile's assembly time: tiles, halo reduction, singular pairs and the 4 pi rule
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);

@@ -97,26 +97,31 @@ struct HostTopo {
         part_tidx, tri_rot;
     int ngroups = 0, nparts = 0;
     std::vector<int> blk_gbase;  // first group of each block (+ end), batches only
-    // triangle patches of the G-only assembly (Topology::patch_*, halo_*); single systems only
-    std::vector<int> patch_off, patch_tri, patch_slot, patch_col, patch_dst, halo_vert, halo_off;
-    int npatch = 0, nhalo = 0;
+    // triangle patches of the G-only assembly (Topology::patch_*, pinfo, pcol)
+    std::vector<PatchInfo> pinfo;
+    std::vector<int> patch_tri, patch_slot, patch_col;
+    std::vector<long long> patch_dst;
+    std::vector<PartialCol> pcol;
+    std::vector<int> blk_npatch;  // patches of each block
+    long long halo_elems = 0;
+    int max_block_n = 0;
 };
 
-// Triangle patches: recursive coordinate bisection of the triangle centroids into patches of at most
-// PT_MAX triangles, a patch split again while it touches more than PCOLS vertices.  A vertex whose
-// incident triangles all lie in one patch is a complete column of that patch (the tile writes its
-// G column); any other vertex is partial: each patch touching it writes a halo column, in increasing
-// patch order, and the halo reduction sums them into its G column.
-static void build_patches(int64_t N, int64_t M, const double* verts, HostTopo& h) {
+// Triangle patches of the G-only assembly, block by block (a single system is one block): recursive
+// coordinate bisection of the block's triangle centroids into patches of at most PT_MAX triangles, a
+// patch split again while it touches more than PCOLS vertices.  A vertex whose incident triangles
+// all lie in one patch is a complete column of that patch (the tile writes its G column); any other
+// vertex is partial: each patch touching it writes a halo column, in increasing patch order, and the
+// halo reduction sums them into its G column.  mbase and pbase: the element offsets of each block's G
+// block and row partials (batches: the packed layout; a single system: 0).
+static void build_patches(int64_t N, int64_t M, const double* verts, HostTopo& h, const std::vector<int64_t>& blocks,
+                          const std::vector<long long>& mbase) {
     std::vector<double> cen((size_t)(3 * M));
     for (int64_t j = 0; j < M; ++j)
         for (int d = 0; d < 3; ++d) {
             const int* t = &h.tri[(size_t)(3 * j)];
             cen[(size_t)(3 * j + d)] = (verts[3 * (size_t)t[0] + d] + verts[3 * (size_t)t[1] + d] + verts[3 * (size_t)t[2] + d]) / 3.0;
         }
-    std::vector<int> idx((size_t)M);
-    std::iota(idx.begin(), idx.end(), 0);
-    std::vector<std::vector<int>> leaves;
     struct Rec {
         static int ncols(const std::vector<int>& tri, const int* b, const int* e) {
             std::vector<int> vs;
@@ -151,54 +156,86 @@ static void build_patches(int64_t N, int64_t M, const double* verts, HostTopo& h
             go(idx, lo + left, hi, xyz, tri, out);
         }
     };
-    Rec::go(idx, 0, (int)M, cen, h.tri, leaves);
-    const int np = (int)leaves.size();
-    h.npatch = np;
-    h.patch_off.assign((size_t)np + 1, 0);
+    const int nb = (int)blocks.size() - 1;
+    // triangles of each block (a triangle lies in the block of its vertices)
+    std::vector<int> blk_of_vert((size_t)N, 0);
+    for (int b = 0; b < nb; ++b)
+        for (int64_t v = blocks[(size_t)b]; v < blocks[(size_t)b + 1]; ++v) blk_of_vert[(size_t)v] = b;
+    std::vector<std::vector<int>> btri((size_t)nb);
+    for (int64_t j = 0; j < M; ++j) btri[(size_t)blk_of_vert[(size_t)h.tri[(size_t)(3 * j)]]].push_back((int)j);
+    h.pinfo.clear();
     h.patch_tri.clear();
     h.patch_slot.clear();
-    h.patch_col.assign((size_t)np * PCOLS, -1);
-    h.patch_dst.assign((size_t)np * PCOLS, -1);
+    h.patch_col.clear();
+    h.blk_npatch.assign((size_t)nb, 0);
+    h.max_block_n = 0;
     std::vector<int> touch_cnt((size_t)N, 0);
-    for (int p = 0; p < np; ++p) {
-        auto& L = leaves[(size_t)p];
-        std::sort(L.begin(), L.end());  // the reference's per-column order: increasing triangle index
-        std::vector<int> vs;
-        for (int t : L)
-            for (int k = 0; k < 3; ++k) vs.push_back(h.tri[(size_t)(3 * t + k)]);
-        std::sort(vs.begin(), vs.end());
-        vs.erase(std::unique(vs.begin(), vs.end()), vs.end());
-        for (size_t s = 0; s < vs.size(); ++s) {
-            h.patch_col[(size_t)p * PCOLS + s] = vs[s];
-            touch_cnt[(size_t)vs[s]]++;
-        }
-        for (int t : L) {
-            int code = 0;
-            for (int k = 0; k < 3; ++k) {
-                const int v = h.tri[(size_t)(3 * t + k)];
-                const int s = (int)(std::lower_bound(vs.begin(), vs.end(), v) - vs.begin());
-                code |= s << (8 * k);
+    long long pb = 0;
+    for (int b = 0; b < nb; ++b) {
+        const int vb = (int)blocks[(size_t)b], n = (int)(blocks[(size_t)b + 1] - blocks[(size_t)b]);
+        h.max_block_n = std::max(h.max_block_n, n);
+        std::vector<std::vector<int>> leaves;
+        auto& idx = btri[(size_t)b];
+        if (!idx.empty()) Rec::go(idx, 0, (int)idx.size(), cen, h.tri, leaves);
+        const int np = (int)leaves.size();
+        h.blk_npatch[(size_t)b] = np;
+        for (int lp = 0; lp < np; ++lp) {
+            auto& L = leaves[(size_t)lp];
+            std::sort(L.begin(), L.end());  // the reference's per-column order: increasing triangle index
+            std::vector<int> vs;
+            for (int t : L)
+                for (int k = 0; k < 3; ++k) vs.push_back(h.tri[(size_t)(3 * t + k)]);
+            std::sort(vs.begin(), vs.end());
+            vs.erase(std::unique(vs.begin(), vs.end()), vs.end());
+            const size_t c0 = h.patch_col.size();
+            h.patch_col.resize(c0 + PCOLS, -1);
+            for (size_t s = 0; s < vs.size(); ++s) {
+                h.patch_col[c0 + s] = vs[s];
+                touch_cnt[(size_t)vs[s]]++;
             }
-            h.patch_tri.push_back(t);
-            h.patch_slot.push_back(code);
+            PatchInfo P{};
+            P.t0 = (int)h.patch_tri.size();
+            P.nt = (int)L.size();
+            P.vbase = vb;
+            P.n = n;
+            P.np = np;
+            P.lp = lp;
+            P.mbase = mbase[(size_t)b];
+            P.pbase = pb;
+            for (int t : L) {
+                int code = 0;
+                for (int k = 0; k < 3; ++k) {
+                    const int v = h.tri[(size_t)(3 * t + k)];
+                    const int sl = (int)(std::lower_bound(vs.begin(), vs.end(), v) - vs.begin());
+                    code |= sl << (8 * k);
+                }
+                h.patch_tri.push_back(t);
+                h.patch_slot.push_back(code);
+            }
+            h.pinfo.push_back(P);
         }
-        h.patch_off[(size_t)p + 1] = (int)h.patch_tri.size();
+        pb += (long long)np * n;
     }
     // halo columns of the partial vertices: vertex by vertex, each vertex's in increasing patch order
-    std::vector<int> hbase((size_t)N, -1), hnext((size_t)N, 0);
-    h.halo_vert.clear();
-    h.halo_off.assign(1, 0);
+    std::vector<long long> hbase((size_t)N, -1);
+    std::vector<int> hnext((size_t)N, 0);
+    h.pcol.clear();
+    long long pos = 0;
     for (int64_t v = 0; v < N; ++v)
         if (touch_cnt[(size_t)v] > 1) {
-            hbase[(size_t)v] = h.halo_off.back();
-            h.halo_vert.push_back((int)v);
-            h.halo_off.push_back(h.halo_off.back() + touch_cnt[(size_t)v]);
+            const int b = blk_of_vert[(size_t)v];
+            const int vb = (int)blocks[(size_t)b], n = (int)(blocks[(size_t)b + 1] - blocks[(size_t)b]);
+            hbase[(size_t)v] = pos;
+            h.pcol.push_back(PartialCol{pos, mbase[(size_t)b] + (long long)(v - vb) * n, touch_cnt[(size_t)v], n});
+            pos += (long long)touch_cnt[(size_t)v] * n;
         }
-    h.nhalo = h.halo_off.back();
-    for (int p = 0; p < np; ++p)
+    h.halo_elems = pos;
+    h.patch_dst.assign(h.patch_col.size(), -1);
+    for (size_t p = 0; p < h.pinfo.size(); ++p)
         for (int s = 0; s < PCOLS; ++s) {
-            const int v = h.patch_col[(size_t)p * PCOLS + s];
-            if (v >= 0 && hbase[(size_t)v] >= 0) h.patch_dst[(size_t)p * PCOLS + s] = hbase[(size_t)v] + hnext[(size_t)v]++;
+            const int v = h.patch_col[p * PCOLS + s];
+            if (v >= 0 && hbase[(size_t)v] >= 0)
+                h.patch_dst[p * PCOLS + s] = hbase[(size_t)v] + (long long)(hnext[(size_t)v]++) * h.pinfo[p].n;
         }
 }
 
@@ -344,7 +381,6 @@ static int build_topology(int64_t N, int64_t M, const int64_t* trigs, const doub
         }
         h.grp_off[(size_t)g + 1] = (int)h.grp_tri.size();
     }
-    if (blocks.empty()) build_patches(N, M, verts, h);
     return BEM_OK;
 }
 
@@ -407,7 +443,7 @@ static void assemble_system(Ctx& c, const double* x, const double* pot, const do
                             const double* x0 = nullptr) {
     c.r0_ready = false;
     if (c.n_pin == 0) {
-        if (!c.batch && c.topo.npatch > 0 && !(c.prm.flags & BEM_FLAG_STEP_ASSEMBLE_H))
+        if (c.topo.npatch > 0 && !(c.prm.flags & BEM_FLAG_STEP_ASSEMBLE_H))
             launch_assemble_g(c, x, pot, c.b, s, x0, x0 ? c.r : nullptr);  // the step needs no H
         else
             launch_assemble(c, x, pot, c.G, c.H, c.b, s, x0, x0 ? c.r : nullptr);
@@ -600,23 +636,34 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = upload(c, &t.part_off, h.part_off)) || (rc = upload(c, &t.part_tidx, h.part_tidx)) ||
         (rc = upload(c, &t.tri_rot, h.tri_rot)))
         return rc;
-    t.npatch = h.npatch;
-    t.nhalo = h.nhalo;
-    t.npartial = (int)h.halo_vert.size();
-    if (h.npatch > 0 &&
-        ((rc = upload(c, &t.patch_off, h.patch_off)) || (rc = upload(c, &t.patch_tri, h.patch_tri)) ||
+    t.npatch = (int)h.pinfo.size();
+    t.npartial = (int)h.pcol.size();
+    t.halo_elems = h.halo_elems;
+    t.max_block_n = h.max_block_n;
+    std::vector<int2> work;  // tiles of the patch kernel: {patch, first row}
+    for (int p = 0; p < t.npatch; ++p) {
+        const PatchInfo& P = h.pinfo[(size_t)p];
+        for (int r0 = P.vbase; r0 < P.vbase + P.n; r0 += PATCH_ROWS) work.push_back(make_int2(p, r0));
+    }
+    t.nwork = (int)work.size();
+    if (t.npatch > 0 &&
+        ((rc = upload(c, &t.pinfo, h.pinfo)) || (rc = upload(c, &t.patch_tri, h.patch_tri)) ||
          (rc = upload(c, &t.patch_slot, h.patch_slot)) || (rc = upload(c, &t.patch_col, h.patch_col)) ||
-         (rc = upload(c, &t.patch_dst, h.patch_dst)) || (t.npartial > 0 && (rc = upload(c, &t.halo_vert, h.halo_vert))) ||
-         (rc = upload(c, &t.halo_off, h.halo_off))))
+         (rc = upload(c, &t.patch_dst, h.patch_dst)) || (t.npartial > 0 && (rc = upload(c, &t.pcol, h.pcol))) ||
+         (rc = upload(c, &t.pwork, work))))
         return rc;
     const size_t n = (size_t)N, m = (size_t)M;
     // dense N x N, or the packed blocks of a batch
     const size_t nn = c.batch ? (size_t)c.blk_elems : n * n;
-    size_t nrow_part = (size_t)std::max(h.ngroups, h.npatch) * n;
+    // row partials of the column-group tiles and of the patch tiles (the larger of the two layouts)
+    size_t nrow_part = (size_t)h.ngroups * n, nrow_patch = 0;
+    for (const PatchInfo& P : h.pinfo)
+        if (P.lp == 0) nrow_patch += (size_t)P.np * P.n;
     if (c.batch) {
         nrow_part = 0;
         for (auto& B : c.h_blk) nrow_part += (size_t)B.ngroups * B.n;
     }
+    nrow_part = std::max(nrow_part, nrow_patch);
     const int ncs = 64;
     double** vec3s[] = {&c.x, &c.x1, &c.xs, &c.k1, &c.k2, &c.k3, &c.k4, &c.vn};
     for (auto p : vec3s)
@@ -638,12 +685,12 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (!c.batch && (rc = dalloc(c, &c.psih_t, (size_t)PRED_CNT + 1))))
         return rc;
     if (c.psih_t) BEM_CUDA(c, cudaMemset(c.psih_t, 0, sizeof(double) * (PRED_CNT + 1)));
-    if (h.npatch > 0) {
+    if (t.npatch > 0) {
         // the step path writes no H: its storage holds the halo columns when they fit
         if ((rc = dalloc(c, &c.prec, m * PREC)) || (rc = dalloc(c, &c.asm_err, 4))) return rc;
-        if ((size_t)h.nhalo <= n)
+        if ((size_t)h.halo_elems <= nn)
             c.halo = c.H;
-        else if ((rc = dalloc(c, &c.halo, (size_t)h.nhalo * n)))
+        else if ((rc = dalloc(c, &c.halo, (size_t)h.halo_elems)))
             return rc;
         BEM_CUDA(c, cudaMemset(c.asm_err, 0, sizeof(int) * 4));
     }
@@ -772,6 +819,7 @@ int bem_set_mesh(bem_ctx* c, int64_t N, const double* verts, int64_t M, const in
     // a rejected mesh leaves the current one in place
     int rc = build_topology(N, M, trigs, verts, h, c->err);
     if (rc) return rc;
+    build_patches(N, M, verts, h, {0, N}, {0});
     cudaStreamSynchronize(c->stream);
     free_all(*c, true);
     rc = alloc_mesh(*c, N, M, h);
@@ -848,6 +896,18 @@ int bem_set_mesh_blocks(bem_ctx* c, int64_t N, const double* verts, int64_t M, c
         pb += (long long)B.ngroups * B.n;
         for (int g = B.gbase; g < B.gbase + B.ngroups; ++g)
             for (int r0 = B.vbase; r0 < B.vbase + B.n; r0 += rows) tiles.push_back(make_int4(g, r0, b, g - B.gbase));
+    }
+    {  // triangle patches of the G-only assembly, block by block
+        std::vector<long long> mbases((size_t)nblocks);
+        for (int b = 0; b < nblocks; ++b) mbases[(size_t)b] = C.h_blk[(size_t)b].mbase;
+        build_patches(N, M, verts, h, voff, mbases);
+        long long ppb = 0;
+        for (int b = 0; b < nblocks; ++b) {
+            BlockInfo& B = C.h_blk[(size_t)b];
+            B.npatch = h.blk_npatch[(size_t)b];
+            B.ppbase = ppb;
+            ppb += (long long)B.npatch * B.n;
+        }
     }
     C.blk_elems = mb;
     C.ntiles = (int)tiles.size();

@@ -54,6 +54,20 @@ constexpr int REC = 28;
 constexpr int PT_MAX = 32;
 constexpr int PCOLS = 32;
 constexpr int PREC = 34;
+constexpr int PATCH_ROWS = 256;  // rows per CTA of the patch tiles
+// A patch: its triangles [t0, t0 + nt) of Topology::patch_tri, and the sub-system (block) it lies in:
+// first vertex vbase and n vertices, G block at element mbase, row partials at pbase + row*np + lp
+// (np patches in the block, lp this patch's index among them).
+struct PatchInfo {
+    int t0, nt, vbase, n, np, lp;
+    long long mbase, pbase;
+};
+// A vertex whose G column sums the halo columns of several patches: cnt columns of n elements from
+// element hpos of the halo buffer, in increasing patch order; its G column starts at element gpos.
+struct PartialCol {
+    long long hpos, gpos;
+    int cnt, n;
+};
 // Fixed block count of the vector kernels, so reductions have a fixed, deterministic shape.
 constexpr int VBLK = 128;
 constexpr int VTHR = 256;
@@ -78,16 +92,19 @@ struct Topology {
     int* tri_rot = nullptr;      // M*3: triangles rotated so the largest vertex id comes first,
                                  // the vertex order split_by_loose_parts leaves (Mesh.cpp:410-426)
     std::vector<int> h_part_of_vert;
-    // triangle patches (single systems; npatch = 0 for batches)
+    // triangle patches of the G-only assembly (the whole mesh, or block by block for a batch)
     int npatch = 0;
-    int* patch_off = nullptr;    // npatch+1 into patch_tri
-    int* patch_tri = nullptr;    // M: triangle ids, patch by patch, increasing inside a patch
-    int* patch_slot = nullptr;   // M: the column slots of the triangle's 3 vertices, 8 bits each
-    int* patch_col = nullptr;    // npatch*PCOLS: vertex of each column slot, -1 padding
-    int* patch_dst = nullptr;    // npatch*PCOLS: halo column of a partial slot, -1 for a complete column
-    int npartial = 0, nhalo = 0; // vertices with contributions from several patches; their halo columns
-    int* halo_vert = nullptr;    // npartial
-    int* halo_off = nullptr;     // npartial+1: halo columns of partial vertex k (patch order)
+    PatchInfo* pinfo = nullptr;     // npatch
+    int* patch_tri = nullptr;       // M: triangle ids, patch by patch, increasing inside a patch
+    int* patch_slot = nullptr;      // M: the column slots of the triangle's 3 vertices, 8 bits each
+    int* patch_col = nullptr;       // npatch*PCOLS: vertex of each column slot, -1 padding
+    long long* patch_dst = nullptr; // npatch*PCOLS: element offset of a partial slot's halo column, -1 complete
+    int npartial = 0;               // vertices shared between patches
+    PartialCol* pcol = nullptr;     // npartial
+    int max_block_n = 0;            // rows of the largest block (the halo reduction's grid)
+    long long halo_elems = 0;       // doubles of the halo columns
+    int2* pwork = nullptr;          // tiles {patch, first row}, PATCH_ROWS rows each
+    int nwork = 0;
 };
 
 // Control block of the iterative solvers and RK4 scalars, resident on the device.
@@ -109,8 +126,9 @@ struct DevScalars {
 // GEMV column splits number ncs with partials at pofs.
 struct BlockInfo {
     int n, vbase, gbase, ngroups;
-    int rbase, ncs, pad0, pad1;
+    int rbase, ncs, npatch, pad1;   // npatch: patches of the block (G-only assembly)
     long long mbase, pbase, pofs;
+    long long ppbase;               // the G-only assembly's row partials of the block
 };
 
 struct Ctx;
@@ -126,9 +144,10 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
                      cudaStream_t s, const double* x0 = nullptr,
                      double* r0 = nullptr);
 void prepare_assemble(Ctx& c);  // kernel attributes and the persistent grid, outside any capture
-// G and b (no H) through the triangle-patch kernels: single systems without pinned vertices
+// G and b (no H) through the triangle-patch kernels: systems without pinned vertices
 void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cudaStream_t s,
                        const double* x0 = nullptr, double* r0 = nullptr);
+void prepare_assemble_g(Ctx& c);  // its kernel attributes and constants, outside any capture
 
 // stage.cu
 void launch_velocity_prep(Ctx& c, const double* x, const double* pot, cudaStream_t s);
