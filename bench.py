@@ -113,8 +113,8 @@ def dist_env():
 
 
 def read_traffic():
-    """DRAM bytes per assembly launch from the committed ncu summary (profiles/), or None."""
-    p = os.path.join(ROOT, "profiles", "assemble_nu20_ncu.md")
+    """DRAM bytes per launch of the assembly tile kernel from the committed ncu summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "assemble_patch_nu20_ncu.md")
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -531,7 +531,7 @@ def run_ours(args):
                                "refreshes": int(st1.precond_refresh - st0.precond_refresh)},
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(prof.kernel_launches),
-        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble + k_singular_diag (assembly: regular-pair tiles, then singular pairs and the 4 pi rule)", "achieved": achieved,
+        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble_patch + k_halo_reduce + k_singular_diag (G-only assembly: regular pairs by triangle patch, shared columns summed, then singular pairs and the 4 pi rule); traffic: the tile kernel", "achieved": achieved,
                      "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
                      "peak_source": "measured live: FP64 FMA-loop kernel (bem_measure_fma_peaks)",
                      "flops_per_launch": flops, "avg_launch_ms": avg_asm_ms,
@@ -749,7 +749,7 @@ def run_sweep(args):
         "e2e": {"value": e2e_value, "unit": "bubble-steps/s", "h2d_bytes_per_step": 40 * N,
                 "d2h_bytes_per_step": 40 * N},
         "gpu_launches": launches,
-        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble_batch + k_singular_diag_batch (persistent, all bubbles)",
+        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble_patch + k_halo_reduce + k_singular_diag_batch_g (G-only assembly of every bubble)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "flops_per_launch": flops, "avg_launch_ms": avg_asm_ms,
                      "peak_source": "measured live: FP64 FMA-loop kernel (bem_measure_fma_peaks)"},
