@@ -47,6 +47,7 @@ static void free_all(Ctx& c, bool keep_blocks = false) {
     // every pointer into the freed allocations
     c.G = c.H = c.LU = nullptr;
     c.prec = c.halo = nullptr;
+    c.rf_bar = nullptr;
     c.asm_err = nullptr;
     c.pbicg = nullptr;
     c.lu_aux = nullptr;
@@ -687,7 +688,9 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     if (c.psih_t) BEM_CUDA(c, cudaMemset(c.psih_t, 0, sizeof(double) * (PRED_CNT + 1)));
     if (t.npatch > 0) {
         // the step path writes no H: its storage holds the halo columns when they fit
-        if ((rc = dalloc(c, &c.prec, m * PREC)) || (rc = dalloc(c, &c.asm_err, 4))) return rc;
+        if ((rc = dalloc(c, &c.prec, m * PREC)) || (rc = dalloc(c, &c.asm_err, 4)) || (rc = dalloc(c, &c.rf_bar, 4)))
+            return rc;
+        BEM_CUDA(c, cudaMemset(c.rf_bar, 0, sizeof(int) * 4));
         if ((size_t)h.halo_elems <= nn)
             c.halo = c.H;
         else if ((rc = dalloc(c, &c.halo, (size_t)h.halo_elems)))

@@ -95,6 +95,8 @@ struct Ctx {
     double* hcol = nullptr;    // (m+2) Hessenberg column / dot results
     double* pbicg = nullptr;   // persistent BiCGSTAB: per-row-block dots, barrier and error words
     bool pbicg_ok = true;      // the persistent BiCGSTAB is usable (cleared after a failed launch or wait)
+    int* rf_bar = nullptr;     // the mixed solve's round kernel: grid barrier words [0..1], error word [2]
+    bool refine_ok = true;     // its cooperative launch is usable (cleared after a failed launch or wait)
     long long wait_limit = 2000000000LL;  // bound of the persistent kernels' grid-barrier waits, SM cycles
     // G-only assembly of the step path: patch-ordered triangle records, halo columns (nhalo x N; the
     // storage of H when nhalo <= N, since the step path does not write H), error word of its bulk copies

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "grid_barrier.cuh"
 
 namespace bemb {
 
@@ -100,15 +101,15 @@ __device__ __forceinline__ double ld_mat(const float* p, uint64_t pol) {
 // columns were both slower, and the serial tail of the split sum cost 5-7 us before its loads were
 // batched).
 constexpr int GV_UNR = 8;
-template <typename T>
-__global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, int chunk, const T* __restrict__ A,
-                                                  const double* __restrict__ x, double* y,
-                                                  double* __restrict__ part, unsigned* __restrict__ cnt,
-                                                  const int* __restrict__ gate, int gate_val, const double* u,
-                                                  double* __restrict__ du, const double* w, double* __restrict__ dw,
-                                                  const double* cvec, double sgn) {
-    if (gate && *gate != gate_val) return;
-    const int rb = blockIdx.x, cs = blockIdx.y, ncs = gridDim.y;
+// One tile (row block rb, column split cs of `chunk` columns, ncs splits) of y = A x, the split sum
+// by the last CTA of the row block, and its fused dots.  COHERENT: x, cvec and the partials may have
+// been written earlier in the same kernel (the persistent refinement), so they are read through L2
+// (ld.global.cg) rather than the read-only path; the arithmetic is the same either way.
+template <typename T, bool COHERENT>
+__device__ __forceinline__ void gemv_tile(int n, int chunk, int ncs, int rb, int cs, const T* __restrict__ A,
+                                          const double* x, double* y, double* __restrict__ part,
+                                          unsigned* __restrict__ cnt, const double* u, double* __restrict__ du,
+                                          const double* w, double* __restrict__ dw, const double* cvec, double sgn) {
     const int i = rb * GV_ROWS + threadIdx.x;
     const int c0 = min(n, cs * chunk), c1 = min(n, c0 + chunk);
     if (i < n) {
@@ -122,13 +123,13 @@ __global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, int chunk, const T* __r
             for (int q = 0; q < GV_UNR; ++q) a[q] = ld_mat(col + (size_t)q * n, pol);
 #pragma unroll
             for (int q = 0; q < GV_UNR; q += 2) {
-                acc0 = fma(a[q], __ldg(x + j + q), acc0);
-                acc1 = fma(a[q + 1], __ldg(x + j + q + 1), acc1);
+                acc0 = fma(a[q], COHERENT ? __ldcg(x + j + q) : __ldg(x + j + q), acc0);
+                acc1 = fma(a[q + 1], COHERENT ? __ldcg(x + j + q + 1) : __ldg(x + j + q + 1), acc1);
             }
             col += (size_t)GV_UNR * n;
         }
         for (; j < c1; ++j) {
-            acc0 = fma(ld_mat(col, pol), __ldg(x + j), acc0);
+            acc0 = fma(ld_mat(col, pol), COHERENT ? __ldcg(x + j) : __ldg(x + j), acc0);
             col += n;
         }
         part[(size_t)cs * n + i] = acc0 + acc1;
@@ -156,18 +157,40 @@ __global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, int chunk, const T* __r
             for (int q = 0; q < PB; ++q) yi += pv[q];
         }
         for (; k < ncs; ++k) yi += __ldcg(part + (size_t)k * n + i);
-        if (cvec) yi = fma(sgn, yi, cvec[i]);
+        if (cvec) yi = fma(sgn, yi, COHERENT ? __ldcg(cvec + i) : cvec[i]);
         y[i] = yi;
     }
     if (du) {
-        const double v = block_sum((i < n) ? yi * u[i] : 0.0);
+        const double v = block_sum((i < n) ? yi * (COHERENT ? __ldcg(u + i) : u[i]) : 0.0);
         if (threadIdx.x == 0) du[rb] = v;
     }
     if (dw) {
-        const double v = block_sum((i < n) ? yi * w[i] : 0.0);
+        const double v = block_sum((i < n) ? yi * (COHERENT ? __ldcg(w + i) : w[i]) : 0.0);
         if (threadIdx.x == 0) dw[rb] = v;
     }
     if (threadIdx.x == 0) cnt[rb] = 0u;
+}
+
+// y = A x; A column-major (T = double or float), x and y FP64.  grid (row blocks of GV_ROWS rows,
+// column splits of `chunk` columns, a multiple of GV_UNR).  One row per thread; GV_UNR columns are
+// loaded before they are used.  The column-split partials are summed in a fixed order by the last
+// CTA of each row block (ticket counter), so the result is deterministic.
+// Optional fused dots of the result: d1 = y.u, d2 = y.w partials per row block.
+// y, u and w are not __restrict__: callers pass u == y to get y.y.  With cvec != null the result is
+// y = cvec + sgn * (A x) (residuals b - A x, accumulations x + X r); cvec may alias y.
+// Measured on B200 at n = 4002, back to back as in the refinement loop: one FP64 and one FP32 GEMV
+// take 45 us together (256 rows x 64 column splits; wider vector loads per thread and TMA-staged
+// columns were both slower, and the serial tail of the split sum cost 5-7 us before its loads were
+// batched).
+template <typename T>
+__global__ void __launch_bounds__(GV_ROWS) k_gemv(int n, int chunk, const T* __restrict__ A,
+                                                  const double* __restrict__ x, double* y,
+                                                  double* __restrict__ part, unsigned* __restrict__ cnt,
+                                                  const int* __restrict__ gate, int gate_val, const double* u,
+                                                  double* __restrict__ du, const double* w, double* __restrict__ dw,
+                                                  const double* cvec, double sgn) {
+    if (gate && *gate != gate_val) return;
+    gemv_tile<T, false>(n, chunk, gridDim.y, blockIdx.x, blockIdx.y, A, x, y, part, cnt, u, du, w, dw, cvec, sgn);
 }
 
 // Column splits: enough CTAs for about eight per SM, at most 64 (the partials buffer holds 64 n).
@@ -1129,6 +1152,84 @@ static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cu
     return bicgstab(c, A, b, x, s);
 }
 
+// One round of the refinement as one cooperative kernel: for k < K, r = b - A x (its row-block norms
+// into pr[k]; skipped for k = 0 when the assembly already left that residual) and x += X r, then the
+// final r = b - A x (norms into pr[K]).  The GEMV tiles are k_gemv's (gemv_tile: the same split count,
+// per-thread order and split sums), spread over co-resident CTAs and separated by grid barriers, so the
+// result equals the multi-kernel round's bit for bit without its 2K+1 launches, their ramps and tails.
+// A barrier wait that runs out sets *err and ends the kernel (grid_barrier); the host then repeats
+// the round with separate launches.
+struct RFArgs {
+    int n, chunk, ncs, K, skip_first;
+    const double* A;
+    const float* X;
+    const double* b;
+    double *x, *r, *part, *pr;
+    unsigned* cnt;
+    unsigned* bar;
+    int* err;
+    long long wait_limit;
+};
+
+__global__ void __launch_bounds__(GV_ROWS) k_refine_round(RFArgs a) {
+    const int n = a.n, nrb = (n + GV_ROWS - 1) / GV_ROWS, ntiles = nrb * a.ncs;
+    for (int k = 0; k <= a.K; ++k) {
+        if (!(k == 0 && a.skip_first)) {
+            for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+                gemv_tile<double, true>(n, a.chunk, a.ncs, t % nrb, t / nrb, a.A, a.x, a.r, a.part, a.cnt, a.r,
+                                        a.pr + (size_t)k * nrb, nullptr, nullptr, a.b, -1.0);
+            if (k == a.K) break;
+            if (!grid_barrier(a.bar, a.err, a.wait_limit)) return;
+        }
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+            gemv_tile<float, true>(n, a.chunk, a.ncs, t % nrb, t / nrb, a.X, a.r, a.x, a.part, a.cnt, nullptr, nullptr,
+                                   nullptr, nullptr, a.x, 1.0);
+        if (!grid_barrier(a.bar, a.err, a.wait_limit)) return;
+    }
+}
+
+// Launches k_refine_round; BEM_ERR_CUDA when a cooperative launch of it is not possible (the caller
+// uses separate launches).  Its error word is c.rf_bar[2], cleared on first use.
+static int refine_round_persistent(Ctx& c, const double* A, const double* b, double* x, double* pr, int K,
+                                   bool skip_first, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    if (!c.rf_bar) return BEM_ERR_CUDA;
+    int sms = 0, coop = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.device);
+    if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_round, GV_ROWS, 0) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    RFArgs a{};
+    a.n = n;
+    a.ncs = gemv_splits(n);
+    a.chunk = ((n + a.ncs - 1) / a.ncs + GV_UNR - 1) / GV_UNR * GV_UNR;
+    a.K = K;
+    a.skip_first = skip_first ? 1 : 0;
+    a.A = A;
+    a.X = c.Xinv;
+    a.b = b;
+    a.x = x;
+    a.r = c.r;
+    a.part = c.part;
+    a.pr = pr;
+    a.cnt = c.cnt;
+    a.bar = reinterpret_cast<unsigned*>(c.rf_bar);
+    a.err = c.rf_bar + 2;
+    a.wait_limit = c.wait_limit;
+    const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
+    const int grid = std::min(nrb * a.ncs, per_sm * sms);
+    void* args[] = {&a};
+    KLAUNCH();
+    if (cudaLaunchCooperativeKernel((void*)k_refine_round, grid, GV_ROWS, args, 0, s) != cudaSuccess) {
+        cudaGetLastError();
+        return BEM_ERR_CUDA;
+    }
+    return BEM_OK;
+}
+
 int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s, SolveTail* tail) {
     const int n = (int)c.topo.N;
     const double tol = c.prm.mixed_tol > 0 ? c.prm.mixed_tol : 1e-12;
@@ -1154,7 +1255,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     else
         KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb);
     // the norms come back through pinned memory: a direct DMA the host sees as soon as it lands
-    const size_t nh = (size_t)(KMAX + 2) * nrb;
+    const size_t nh = (size_t)(KMAX + 2) * nrb + 2;  // norms, then the round kernel's error word
     if (c.h_red_cap < nh) {
         cudaFreeHost(c.h_red);
         c.h_red = nullptr;
@@ -1172,17 +1273,28 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     double rho = 1.0, rel = 1.0, rel0 = -1.0;
     bool converged = false;
     int rounds = 0;
+    int* herr = reinterpret_cast<int*>(host + (size_t)(KMAX + 2) * nrb);
     for (int round = 0; round < 4; ++round) {
         ++rounds;
         tail_valid = false;  // a round changes x
-        for (int k = 0; k < K; ++k) {
-            if (!(round == 0 && k == 0 && r0_ready))  // else the residual and its norms are there
-                gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr, nullptr, b,
-                               -1.0);
-            gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, nullptr, 0, nullptr, nullptr, nullptr, nullptr, x, 1.0);
+        const bool skip_first = round == 0 && r0_ready;  // the residual and its norms are there
+        bool persistent = c.refine_ok && !(c.prm.flags & BEM_FLAG_REFINE_MULTIKERNEL) &&
+                          refine_round_persistent(c, A, b, x, pr, K, skip_first, s) == BEM_OK;
+        if (!persistent) {
+            if (!(c.prm.flags & BEM_FLAG_REFINE_MULTIKERNEL)) c.refine_ok = false;
+            for (int k = 0; k < K; ++k) {
+                if (!(k == 0 && skip_first))
+                    gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr,
+                                   nullptr, b, -1.0);
+                gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, nullptr, 0, nullptr, nullptr, nullptr, nullptr, x,
+                              1.0);
+            }
+            gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b,
+                           -1.0);
         }
-        gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b, -1.0);
         BEM_CUDA(c, cudaMemcpyAsync(host, c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
+        *herr = 0;
+        if (persistent) BEM_CUDA(c, cudaMemcpyAsync(herr, c.rf_bar + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
         if (round == 0 && tail) {  // the solution's consumers, speculatively: x is final if this round converges
             if (!c.solve_ev) BEM_CUDA(c, cudaEventCreateWithFlags(&c.solve_ev, cudaEventDisableTiming));
             BEM_CUDA(c, cudaEventRecord(c.solve_ev, s));
@@ -1192,6 +1304,21 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
             BEM_CUDA(c, cudaEventSynchronize(c.solve_ev));
         } else {
             BEM_CUDA(c, cudaStreamSynchronize(s));
+        }
+        if (*herr) {
+            // a barrier wait of the round kernel ran out: x holds some rows of this round's update and
+            // r is incomplete.  Any x is a valid refinement iterate, so the round is repeated from x
+            // with separate launches, which the context keeps from now on.
+            // CTAs that had passed the last completed barrier may have drawn tickets of the next GEMV's
+            // row blocks: clear them for the separate launches
+            BEM_CUDA(c, cudaMemsetAsync(c.cnt, 0, sizeof(unsigned) * (size_t)(nrb + 1), s));
+            c.stats.wait_expired++;
+            c.refine_ok = false;
+            r0_ready = false;
+            tail_valid = false;
+            --round;
+            --rounds;
+            continue;
         }
         c.stats.last_iters += K;
         double bb = 0.0;

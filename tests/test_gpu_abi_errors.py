@@ -137,3 +137,22 @@ def test_expired_barrier_wait_falls_back_to_the_multikernel_bicgstab():
         assert st.last_rel_residual <= 1e-14
         assert np.max(np.abs(psi - psi_lu)) <= 1e-10 * np.max(np.abs(psi_lu))
     s.close()
+
+
+def test_expired_barrier_wait_in_the_refinement_round_repeats_it_with_separate_launches():
+    # The mixed solve runs each round of refinement steps as one cooperative kernel with grid
+    # barriers.  With a one-cycle bound its first barrier wait runs out: the kernel sets its error word
+    # and ends, the host counts the expired wait, clears the GEMV tickets and repeats the round with
+    # separate GEMV launches (kept for the rest of the context); psi still matches LU.
+    v, f = mesh.bubble(8, 1.0, (2.0, 0.0, 0.0))
+    phi = 0.1 * np.sin(3 * v[:, 2]) + 0.05 * v[:, 0]
+    lu = ColocSim(v, f, solver="lu")
+    _, psi_lu = lu.position_t(phi, return_psi=True)
+    lu.close()
+    s = ColocSim(v, f, solver="mixed")
+    assert s._L.bem_set_wait_limit(s._h, 1) == L.BEM_OK
+    for k in range(2):
+        _, psi = s.position_t(phi, return_psi=True)
+        assert s.stats().wait_expired == 1, k
+        assert np.max(np.abs(psi - psi_lu)) <= 1e-10 * np.max(np.abs(psi_lu))
+    s.close()

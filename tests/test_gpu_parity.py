@@ -400,3 +400,24 @@ def test_exterior_potential_grid_matches_oracle():
     sim = ColocSim(v, f)
     got = sim.exterior_potential(pts, phi=phi, psi=psi)
     assert rel(got, O.exterior_pot(v, f, phi, psi, pts)) <= 1e-12
+
+
+def test_refinement_round_kernel_equals_separate_launches():
+    # the mixed solve's refinement round as one cooperative kernel and as separate GEMV launches: the
+    # same tiles, per-thread order and split sums, so whole RK4 trajectories agree bit for bit
+    from bem_b200 import _lib as L
+    v, f = mesh.bubble(12, 1.0, (2.0, 0.0, 0.0))
+    rng = np.random.default_rng(3)
+    v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None]
+    out = []
+    for flags in (0, L.FLAG_REFINE_MULTIKERNEL):
+        sim = ColocSim(v, f, pressurefield=(-0.8, 2 * np.pi / 5, 0.0), solver="mixed", p_inf=1.0, epsilon=1.0,
+                       gamma=1.4)
+        sim._update(flags=flags)
+        sim.set_phi(0.0)
+        for _ in range(4):
+            sim.evolve_system_RK4(5e-3, fixdt=True)
+        x, p, s, t = sim.get_state()
+        out.append((x.tobytes(), p.tobytes(), s.tobytes(), t, sim.stats().total_iters))
+        sim.close()
+    assert out[0] == out[1]
