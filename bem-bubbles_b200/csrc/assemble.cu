@@ -759,8 +759,10 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
 // The patch's triangle records are contiguous (patch order) and arrive in shared memory by one bulk
 // copy (cp.async.bulk, completion counted on an mbarrier) while the threads clear their accumulators.
 // A column whose vertex has all its triangles in the patch is complete and goes straight to G; the
-// columns of vertices shared with other patches go to halo columns, which k_halo_reduce sums into G in
-// increasing patch order.  The singular pairs and b's 4 pi term follow in k_singular_diag<., true>.
+// columns of vertices shared with other patches go to halo columns.  For each shared vertex and row
+// tile, the patch CTA that finishes last (a ticket counter) sums the halo slices in increasing patch
+// order, while they are still in L2, and writes the G column.  The singular pairs and b's 4 pi term
+// follow in k_singular_diag<., true>.
 // Per G entry the order is: the regular pairs of each patch in increasing triangle order, the patches
 // in increasing order, then the singular pairs; no atomics, so results are bit-reproducible.
 
@@ -862,12 +864,13 @@ __global__ void __launch_bounds__(ROWS, MINB)
                      const long long* __restrict__ patch_dst, const double* __restrict__ x,
                      const double* __restrict__ phi, double* __restrict__ G, double* __restrict__ halo,
                      double* __restrict__ bp, const double* __restrict__ x0, double* __restrict__ gp,
-                     int* __restrict__ err) {
+                     int* __restrict__ err, const int* __restrict__ patch_pk, const PartialCol* __restrict__ pcol,
+                     unsigned* __restrict__ halo_tick) {
     extern __shared__ __align__(16) double psmem[];
     double* srec = psmem;                  // [PT_MAX][PREC], the patch's records
     double* acc = psmem + PT_MAX * PREC;   // [PCOLS][ROWS], this CTA's rows of the patch's columns
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_col[PCOLS];
+    __shared__ int s_col[PCOLS], s_pk[PCOLS], s_fin[PCOLS];
     __shared__ long long s_dst[PCOLS];
     const int tid = threadIdx.x;
     const int2 wk = work[blockIdx.x];
@@ -880,6 +883,7 @@ __global__ void __launch_bounds__(ROWS, MINB)
     if (tid < PCOLS) {
         s_col[tid] = patch_col[p * PCOLS + tid];
         s_dst[tid] = patch_dst[p * PCOLS + tid];
+        s_pk[tid] = patch_pk[p * PCOLS + tid];
     }
 #pragma unroll 8
     for (int s = 0; s < PCOLS; ++s) acc[s * ROWS + tid] = 0.0;
@@ -900,9 +904,8 @@ __global__ void __launch_bounds__(ROWS, MINB)
         }
         return;
     }
-    if (!row) return;
     double hb = 0.0;  // sum over this patch's regular pairs of sum_k H_k (phi_k - phi_i)
-    for (int t = 0; t < P.nt; ++t) {
+    for (int t = 0; t < (row ? P.nt : 0); ++t) {
         const double* r = srec + t * PREC;
         const long long ids = __double_as_longlong(r[31]);
         if (i == (int)(ids & 0x1FFFFF) || i == (int)((ids >> 21) & 0x1FFFFF) || i == (int)(ids >> 42))
@@ -919,33 +922,51 @@ __global__ void __launch_bounds__(ROWS, MINB)
         if (MIRROR) hb = fma(fma(ps.m[0], e0, fma(ps.m[1], e1, __dmul_rn(ps.m[2], e2))), ps.sm, hb);
     }
     const int il = i - P.vbase;
-    double gs = 0.0;
-    for (int s = 0; s < PCOLS; ++s) {
-        const int v = s_col[s];
-        if (v < 0) break;
-        const double gv = acc[s * ROWS + tid];
-        const long long h = s_dst[s];
-        if (h < 0)
-            G[P.mbase + (long long)(v - P.vbase) * P.n + il] = gv;
-        else
-            halo[h + il] = gv;
-        if (x0) gs = fma(gv, x0[v], gs);
+    if (row) {
+        double gs = 0.0;
+        for (int s = 0; s < PCOLS; ++s) {
+            const int v = s_col[s];
+            if (v < 0) break;
+            const double gv = acc[s * ROWS + tid];
+            const long long h = s_dst[s];
+            if (h < 0)
+                G[P.mbase + (long long)(v - P.vbase) * P.n + il] = gv;
+            else
+                halo[h + il] = gv;
+            if (x0) gs = fma(gv, x0[v], gs);
+        }
+        const long long po = P.pbase + (long long)il * P.np + P.lp;  // the row's partials are contiguous
+        bp[po] = hb;
+        if (x0) gp[po] = gs;
     }
-    const long long po = P.pbase + (long long)il * P.np + P.lp;  // the row's partials are contiguous
-    bp[po] = hb;
-    if (x0) gp[po] = gs;
-}
-
-// G column of each partial vertex: its halo columns summed in increasing patch order.
-__global__ void k_halo_reduce(const PartialCol* __restrict__ pcol, const double* __restrict__ halo,
-                              double* __restrict__ G) {
-    const PartialCol pc = pcol[blockIdx.x];
-    const int i = blockIdx.y * blockDim.x + threadIdx.x;
-    if (i >= pc.n) return;
-    const double* h = halo + pc.hpos + i;
-    double s = h[0];
-    for (int c = 1; c < pc.cnt; ++c) s += h[(size_t)c * pc.n];
-    G[pc.gpos + i] = s;
+    // shared vertices: one ticket per (vertex, row tile); the CTA drawing the last one sums the halo
+    // slices of this row tile in increasing patch order (every slice was written before its ticket)
+    const int rt = (wk.y - P.vbase) / ROWS;
+    __threadfence();
+    __syncthreads();
+    if (tid < PCOLS) {
+        const int k = s_pk[tid];
+        int fin = -1;
+        if (k >= 0) {
+            const PartialCol pc = pcol[k];
+            if (atomicAdd(&halo_tick[pc.tick + rt], 1u) == (unsigned)(pc.cnt - 1)) fin = k;
+        }
+        s_fin[tid] = fin;
+    }
+    __syncthreads();
+    for (int s = 0; s < PCOLS; ++s) {
+        const int k = s_fin[s];
+        if (k < 0) continue;
+        __threadfence();
+        const PartialCol pc = pcol[k];
+        if (row) {
+            const double* h = halo + pc.hpos + il;
+            double sum = __ldcg(h);
+            for (int c2 = 1; c2 < pc.cnt; ++c2) sum += __ldcg(h + (size_t)c2 * pc.n);
+            G[pc.gpos + il] = sum;
+        }
+        if (tid == 0) halo_tick[pc.tick + rt] = 0u;  // for the next assembly
+    }
 }
 
 // The G-only singular pass of a batch: rows of block vblk[i], its patches' row partials.
@@ -999,13 +1020,11 @@ void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cu
     if (c.prm.mirror)
         KLAUNCH(), k_assemble_patch<true, PATCH_ROWS, 3><<<T.nwork, PATCH_ROWS, sm, s>>>(
                        T.pwork, T.pinfo, c.prec, T.patch_col, T.patch_dst, x, phi, c.G, c.halo, c.bp, x0, c.gp,
-                       c.asm_err);
+                       c.asm_err, T.patch_pk, T.pcol, T.halo_tick);
     else
         KLAUNCH(), k_assemble_patch<false, PATCH_ROWS, 3><<<T.nwork, PATCH_ROWS, sm, s>>>(
                        T.pwork, T.pinfo, c.prec, T.patch_col, T.patch_dst, x, phi, c.G, c.halo, c.bp, x0, c.gp,
-                       c.asm_err);
-    if (T.npartial > 0)
-        KLAUNCH(), k_halo_reduce<<<dim3(T.npartial, (T.max_block_n + 255) / 256), 256, 0, s>>>(T.pcol, c.halo, c.G);
+                       c.asm_err, T.patch_pk, T.pcol, T.halo_tick);
     const int nbs = (N + SD_WARPS - 1) / SD_WARPS, nt = 32 * SD_WARPS;
     if (c.batch) {
         if (c.prm.mirror)
@@ -1021,7 +1040,7 @@ void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cu
         KLAUNCH(), k_singular_diag<false, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
                                                                    T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
     }
-    if (c.prof) {  // the profile's assembly time: tiles, halo reduction, singular pairs and the 4 pi rule
+    if (c.prof) {  // the profile's assembly time: tiles (with the shared columns' sums), singular pairs, 4 pi rule
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }

@@ -83,7 +83,7 @@ __device__ double dot_total(const PBArgs& a, int k) {
     return out;
 }
 
-__device__ __forceinline__ bool grid_sync(const PBArgs& a) { return grid_barrier(a.bar, a.err, a.wait_limit); }
+__device__ __forceinline__ bool grid_sync(const PBArgs& a) { return grid_barrier(a.bar, a.bar + 1, a.err, a.wait_limit); }
 
 // out = A in (column-major A), tiles (row block, column split) spread over the CTAs; the last CTA
 // of a row block sums the splits in order, writes out and the row block's dots out.u0 -> dots[k0],

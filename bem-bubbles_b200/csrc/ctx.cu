@@ -102,7 +102,9 @@ struct HostTopo {
     std::vector<PatchInfo> pinfo;
     std::vector<int> patch_tri, patch_slot, patch_col;
     std::vector<long long> patch_dst;
+    std::vector<int> patch_pk;
     std::vector<PartialCol> pcol;
+    int nticks = 0;
     std::vector<int> blk_npatch;  // patches of each block
     long long halo_elems = 0;
     int max_block_n = 0;
@@ -219,24 +221,31 @@ static void build_patches(int64_t N, int64_t M, const double* verts, HostTopo& h
     }
     // halo columns of the partial vertices: vertex by vertex, each vertex's in increasing patch order
     std::vector<long long> hbase((size_t)N, -1);
-    std::vector<int> hnext((size_t)N, 0);
+    std::vector<int> hnext((size_t)N, 0), kof((size_t)N, -1);
     h.pcol.clear();
     long long pos = 0;
+    int ticks = 0;
     for (int64_t v = 0; v < N; ++v)
         if (touch_cnt[(size_t)v] > 1) {
             const int b = blk_of_vert[(size_t)v];
             const int vb = (int)blocks[(size_t)b], n = (int)(blocks[(size_t)b + 1] - blocks[(size_t)b]);
             hbase[(size_t)v] = pos;
-            h.pcol.push_back(PartialCol{pos, mbase[(size_t)b] + (long long)(v - vb) * n, touch_cnt[(size_t)v], n});
+            kof[(size_t)v] = (int)h.pcol.size();
+            h.pcol.push_back(PartialCol{pos, mbase[(size_t)b] + (long long)(v - vb) * n, touch_cnt[(size_t)v], n, ticks, 0});
             pos += (long long)touch_cnt[(size_t)v] * n;
+            ticks += (n + PATCH_ROWS - 1) / PATCH_ROWS;
         }
     h.halo_elems = pos;
+    h.nticks = ticks;
     h.patch_dst.assign(h.patch_col.size(), -1);
+    h.patch_pk.assign(h.patch_col.size(), -1);
     for (size_t p = 0; p < h.pinfo.size(); ++p)
         for (int s = 0; s < PCOLS; ++s) {
             const int v = h.patch_col[p * PCOLS + s];
-            if (v >= 0 && hbase[(size_t)v] >= 0)
+            if (v >= 0 && hbase[(size_t)v] >= 0) {
                 h.patch_dst[p * PCOLS + s] = hbase[(size_t)v] + (long long)(hnext[(size_t)v]++) * h.pinfo[p].n;
+                h.patch_pk[p * PCOLS + s] = kof[(size_t)v];
+            }
         }
 }
 
@@ -650,9 +659,11 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     if (t.npatch > 0 &&
         ((rc = upload(c, &t.pinfo, h.pinfo)) || (rc = upload(c, &t.patch_tri, h.patch_tri)) ||
          (rc = upload(c, &t.patch_slot, h.patch_slot)) || (rc = upload(c, &t.patch_col, h.patch_col)) ||
-         (rc = upload(c, &t.patch_dst, h.patch_dst)) || (t.npartial > 0 && (rc = upload(c, &t.pcol, h.pcol))) ||
-         (rc = upload(c, &t.pwork, work))))
+         (rc = upload(c, &t.patch_dst, h.patch_dst)) || (rc = upload(c, &t.patch_pk, h.patch_pk)) ||
+         (t.npartial > 0 && (rc = upload(c, &t.pcol, h.pcol))) || (rc = upload(c, &t.pwork, work)) ||
+         (rc = dalloc(c, &t.halo_tick, (size_t)std::max(1, h.nticks)))))
         return rc;
+    if (t.npatch > 0) BEM_CUDA(c, cudaMemset(t.halo_tick, 0, sizeof(unsigned) * (size_t)std::max(1, h.nticks)));
     const size_t n = (size_t)N, m = (size_t)M;
     // dense N x N, or the packed blocks of a batch
     const size_t nn = c.batch ? (size_t)c.blk_elems : n * n;
@@ -688,9 +699,9 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
     if (c.psih_t) BEM_CUDA(c, cudaMemset(c.psih_t, 0, sizeof(double) * (PRED_CNT + 1)));
     if (t.npatch > 0) {
         // the step path writes no H: its storage holds the halo columns when they fit
-        if ((rc = dalloc(c, &c.prec, m * PREC)) || (rc = dalloc(c, &c.asm_err, 4)) || (rc = dalloc(c, &c.rf_bar, 4)))
+        if ((rc = dalloc(c, &c.prec, m * PREC)) || (rc = dalloc(c, &c.asm_err, 4)) || (rc = dalloc(c, &c.rf_bar, RF_WORDS)))
             return rc;
-        BEM_CUDA(c, cudaMemset(c.rf_bar, 0, sizeof(int) * 4));
+        BEM_CUDA(c, cudaMemset(c.rf_bar, 0, sizeof(int) * RF_WORDS));
         if ((size_t)h.halo_elems <= nn)
             c.halo = c.H;
         else if ((rc = dalloc(c, &c.halo, (size_t)h.halo_elems)))

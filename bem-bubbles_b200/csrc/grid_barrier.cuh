@@ -12,20 +12,25 @@ namespace bemb {
 
 constexpr long long GRID_WAIT_CYCLES = 2000000000LL;
 
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, long long limit) {
+// genw: the generation word; callers whose CTAs are many keep it on another cache line than the
+// arrival count (bar[0]), so that the polling does not queue behind the arrivals' atomics, and poll
+// with a short sleep (sleep_ns > 0).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned* genw, int* err, long long limit,
+                                             unsigned sleep_ns = 0) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* gen = bar + 1;
+        volatile unsigned* gen = genw;
         const unsigned g = *gen;
         __threadfence();
         if (atomicAdd(bar, 1u) == gridDim.x - 1) {
             atomicExch(bar, 0u);
             __threadfence();
-            atomicAdd(bar + 1, 1u);
+            atomicAdd(genw, 1u);
         } else {
             const long long t0 = clock64();
             while (*gen == g) {
+                if (sleep_ns) __nanosleep(sleep_ns);
                 if (clock64() - t0 > limit) {
                     atomicExch(err, 1);
                     break;

@@ -55,6 +55,7 @@ constexpr int PT_MAX = 32;
 constexpr int PCOLS = 32;
 constexpr int PREC = 34;
 constexpr int PATCH_ROWS = 256;  // rows per CTA of the patch tiles
+constexpr int RF_WORDS = 96;     // ints of Ctx::rf_bar (the refinement round kernel's barrier and error words)
 // A patch: its triangles [t0, t0 + nt) of Topology::patch_tri, and the sub-system (block) it lies in:
 // first vertex vbase and n vertices, G block at element mbase, row partials at pbase + row*np + lp
 // (np patches in the block, lp this patch's index among them).
@@ -64,9 +65,11 @@ struct PatchInfo {
 };
 // A vertex whose G column sums the halo columns of several patches: cnt columns of n elements from
 // element hpos of the halo buffer, in increasing patch order; its G column starts at element gpos.
+// tick: its first ticket counter, one per row tile of its block (the patch CTA that draws the last
+// ticket of a row tile sums that tile's rows).
 struct PartialCol {
     long long hpos, gpos;
-    int cnt, n;
+    int cnt, n, tick, pad;
 };
 // Fixed block count of the vector kernels, so reductions have a fixed, deterministic shape.
 constexpr int VBLK = 128;
@@ -99,6 +102,8 @@ struct Topology {
     int* patch_slot = nullptr;      // M: the column slots of the triangle's 3 vertices, 8 bits each
     int* patch_col = nullptr;       // npatch*PCOLS: vertex of each column slot, -1 padding
     long long* patch_dst = nullptr; // npatch*PCOLS: element offset of a partial slot's halo column, -1 complete
+    int* patch_pk = nullptr;        // npatch*PCOLS: the partial vertex (index into pcol) of a slot, -1 complete
+    unsigned* halo_tick = nullptr;  // ticket counters of the partial vertices' row tiles (zero between uses)
     int npartial = 0;               // vertices shared between patches
     PartialCol* pcol = nullptr;     // npartial
     int max_block_n = 0;            // rows of the largest block (the halo reduction's grid)

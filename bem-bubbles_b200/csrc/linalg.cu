@@ -109,9 +109,19 @@ template <typename T, bool COHERENT>
 __device__ __forceinline__ void gemv_tile(int n, int chunk, int ncs, int rb, int cs, const T* __restrict__ A,
                                           const double* x, double* y, double* __restrict__ part,
                                           unsigned* __restrict__ cnt, const double* u, double* __restrict__ du,
-                                          const double* w, double* __restrict__ dw, const double* cvec, double sgn) {
+                                          const double* w, double* __restrict__ dw, const double* cvec, double sgn,
+                                          double* sx = nullptr) {
     const int i = rb * GV_ROWS + threadIdx.x;
     const int c0 = min(n, cs * chunk), c1 = min(n, c0 + chunk);
+    if (COHERENT) {
+        // the tile's slice of x, once through L2 into shared memory; the loop below reads it back as
+        // broadcasts (sx - c0 + j is x[j])
+        __syncthreads();
+        for (int j = c0 + (int)threadIdx.x; j < c1; j += GV_ROWS) sx[j - c0] = __ldcg(x + j);
+        __syncthreads();
+    }
+    const int xo = COHERENT ? c0 : 0;  // x[j] is xv[j - xo]
+    const double* xv = COHERENT ? sx : x;
     if (i < n) {
         const uint64_t pol = l2_policy(sizeof(T) == 4);
         double acc0 = 0.0, acc1 = 0.0;
@@ -123,13 +133,13 @@ __device__ __forceinline__ void gemv_tile(int n, int chunk, int ncs, int rb, int
             for (int q = 0; q < GV_UNR; ++q) a[q] = ld_mat(col + (size_t)q * n, pol);
 #pragma unroll
             for (int q = 0; q < GV_UNR; q += 2) {
-                acc0 = fma(a[q], COHERENT ? __ldcg(x + j + q) : __ldg(x + j + q), acc0);
-                acc1 = fma(a[q + 1], COHERENT ? __ldcg(x + j + q + 1) : __ldg(x + j + q + 1), acc1);
+                acc0 = fma(a[q], COHERENT ? xv[j + q - xo] : __ldg(xv + j + q), acc0);
+                acc1 = fma(a[q + 1], COHERENT ? xv[j + q + 1 - xo] : __ldg(xv + j + q + 1), acc1);
             }
             col += (size_t)GV_UNR * n;
         }
         for (; j < c1; ++j) {
-            acc0 = fma(ld_mat(col, pol), COHERENT ? __ldcg(x + j) : __ldg(x + j), acc0);
+            acc0 = fma(ld_mat(col, pol), COHERENT ? xv[j - xo] : __ldg(xv + j), acc0);
             col += n;
         }
         part[(size_t)cs * n + i] = acc0 + acc1;
@@ -1159,6 +1169,12 @@ static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cu
 // result equals the multi-kernel round's bit for bit without its 2K+1 launches, their ramps and tails.
 // A barrier wait that runs out sets *err and ends the kernel (grid_barrier); the host then repeats
 // the round with separate launches.
+// Ctx::rf_bar: the arrival count at word 0, the generation at RF_GEN and the error word at RF_ERR,
+// each on its own 128-byte line (RF_WORDS ints)
+constexpr int RF_GEN = 32, RF_ERR = 64;
+static_assert(RF_ERR < RF_WORDS, "Ctx::rf_bar holds RF_WORDS ints");
+constexpr unsigned RF_SLEEP_NS = 32;  // polling interval of the waiting CTAs
+constexpr int RF_CHUNK_MAX = 4096;    // columns of one tile's staged slice of the input vector
 struct RFArgs {
     int n, chunk, ncs, K, skip_first;
     const double* A;
@@ -1172,24 +1188,25 @@ struct RFArgs {
 };
 
 __global__ void __launch_bounds__(GV_ROWS) k_refine_round(RFArgs a) {
+    extern __shared__ double rf_x[];  // the current tile's slice of the input vector
     const int n = a.n, nrb = (n + GV_ROWS - 1) / GV_ROWS, ntiles = nrb * a.ncs;
     for (int k = 0; k <= a.K; ++k) {
         if (!(k == 0 && a.skip_first)) {
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
                 gemv_tile<double, true>(n, a.chunk, a.ncs, t % nrb, t / nrb, a.A, a.x, a.r, a.part, a.cnt, a.r,
-                                        a.pr + (size_t)k * nrb, nullptr, nullptr, a.b, -1.0);
+                                        a.pr + (size_t)k * nrb, nullptr, nullptr, a.b, -1.0, rf_x);
             if (k == a.K) break;
-            if (!grid_barrier(a.bar, a.err, a.wait_limit)) return;
+            if (!grid_barrier(a.bar, a.bar + RF_GEN, a.err, a.wait_limit, RF_SLEEP_NS)) return;
         }
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
             gemv_tile<float, true>(n, a.chunk, a.ncs, t % nrb, t / nrb, a.X, a.r, a.x, a.part, a.cnt, nullptr, nullptr,
-                                   nullptr, nullptr, a.x, 1.0);
-        if (!grid_barrier(a.bar, a.err, a.wait_limit)) return;
+                                   nullptr, nullptr, a.x, 1.0, rf_x);
+        if (!grid_barrier(a.bar, a.bar + RF_GEN, a.err, a.wait_limit, RF_SLEEP_NS)) return;
     }
 }
 
 // Launches k_refine_round; BEM_ERR_CUDA when a cooperative launch of it is not possible (the caller
-// uses separate launches).  Its error word is c.rf_bar[2], cleared on first use.
+// uses separate launches).  Its barrier and error words are c.rf_bar (cleared with the mesh).
 static int refine_round_persistent(Ctx& c, const double* A, const double* b, double* x, double* pr, int K,
                                    bool skip_first, cudaStream_t s) {
     const int n = (int)c.topo.N;
@@ -1197,7 +1214,9 @@ static int refine_round_persistent(Ctx& c, const double* A, const double* b, dou
     int sms = 0, coop = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.device);
-    if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_round, GV_ROWS, 0) != cudaSuccess ||
+    const int ncs0 = gemv_splits(n);
+    const size_t smem0 = sizeof(double) * (size_t)(((n + ncs0 - 1) / ncs0 + GV_UNR - 1) / GV_UNR * GV_UNR);
+    if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_round, GV_ROWS, smem0) != cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
         return BEM_ERR_CUDA;
@@ -1206,6 +1225,7 @@ static int refine_round_persistent(Ctx& c, const double* A, const double* b, dou
     a.n = n;
     a.ncs = gemv_splits(n);
     a.chunk = ((n + a.ncs - 1) / a.ncs + GV_UNR - 1) / GV_UNR * GV_UNR;
+    if (a.chunk > RF_CHUNK_MAX) return BEM_ERR_CUDA;
     a.K = K;
     a.skip_first = skip_first ? 1 : 0;
     a.A = A;
@@ -1217,13 +1237,14 @@ static int refine_round_persistent(Ctx& c, const double* A, const double* b, dou
     a.pr = pr;
     a.cnt = c.cnt;
     a.bar = reinterpret_cast<unsigned*>(c.rf_bar);
-    a.err = c.rf_bar + 2;
+    a.err = c.rf_bar + RF_ERR;
     a.wait_limit = c.wait_limit;
     const int nrb = (n + GV_ROWS - 1) / GV_ROWS;
     const int grid = std::min(nrb * a.ncs, per_sm * sms);
     void* args[] = {&a};
     KLAUNCH();
-    if (cudaLaunchCooperativeKernel((void*)k_refine_round, grid, GV_ROWS, args, 0, s) != cudaSuccess) {
+    const size_t smem = sizeof(double) * (size_t)a.chunk;
+    if (cudaLaunchCooperativeKernel((void*)k_refine_round, grid, GV_ROWS, args, smem, s) != cudaSuccess) {
         cudaGetLastError();
         return BEM_ERR_CUDA;
     }
@@ -1294,7 +1315,7 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         }
         BEM_CUDA(c, cudaMemcpyAsync(host, c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
         *herr = 0;
-        if (persistent) BEM_CUDA(c, cudaMemcpyAsync(herr, c.rf_bar + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (persistent) BEM_CUDA(c, cudaMemcpyAsync(herr, c.rf_bar + RF_ERR, sizeof(int), cudaMemcpyDeviceToHost, s));
         if (round == 0 && tail) {  // the solution's consumers, speculatively: x is final if this round converges
             if (!c.solve_ev) BEM_CUDA(c, cudaEventCreateWithFlags(&c.solve_ev, cudaEventDisableTiming));
             BEM_CUDA(c, cudaEventRecord(c.solve_ev, s));

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(LP_THREADS) k_lu_panel_rows(LPArgs a) {
             for (int c = tid; c < nb; c += LP_THREADS) mine[2 + c] = sp[(bi - r0) * ld + c];
         if (rowj >= r0 && rowj < r1)
             for (int c = tid; c < nb; c += LP_THREADS) diag[c] = sp[(rowj - r0) * ld + c];
-        if (!grid_barrier(a.bar, a.err, a.wait_limit)) return;
+        if (!grid_barrier(a.bar, a.bar + 1, a.err, a.wait_limit)) return;
         // the pivot, the same in every CTA: largest |entry| over the candidates, then smallest row (an
         // order-independent rule, reduced over the threads)
         double pv = -1.0;
