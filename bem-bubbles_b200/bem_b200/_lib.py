@@ -26,7 +26,7 @@ SOLVER_MIXED = 2
 FLAG_BICGSTAB_MULTIKERNEL = 1
 FLAG_NO_STAGE_PREDICTOR = 2
 FLAG_STEP_ASSEMBLE_H = 4
-FLAG_REFINE_MULTIKERNEL = 8
+FLAG_REFINE_PERSISTENT = 8
 
 _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)

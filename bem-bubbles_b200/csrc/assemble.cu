@@ -944,20 +944,25 @@ __global__ void __launch_bounds__(ROWS, MINB)
     const int rt = (wk.y - P.vbase) / ROWS;
     __threadfence();
     __syncthreads();
+    __shared__ int s_nfin;
+    static_assert(PCOLS == 32, "the finishing slots are drawn by one warp");
     if (tid < PCOLS) {
         const int k = s_pk[tid];
-        int fin = -1;
+        bool fin = false;
         if (k >= 0) {
             const PartialCol pc = pcol[k];
-            if (atomicAdd(&halo_tick[pc.tick + rt], 1u) == (unsigned)(pc.cnt - 1)) fin = k;
+            fin = atomicAdd(&halo_tick[pc.tick + rt], 1u) == (unsigned)(pc.cnt - 1);
         }
-        s_fin[tid] = fin;
+        // the finishing slots, compacted in slot order
+        const unsigned m = __ballot_sync(0xffffffffu, fin);
+        if (fin) s_fin[__popc(m & ((1u << tid) - 1u))] = k;
+        if (tid == 0) s_nfin = __popc(m);
     }
     __syncthreads();
-    for (int s = 0; s < PCOLS; ++s) {
-        const int k = s_fin[s];
-        if (k < 0) continue;
-        __threadfence();
+    const int nfin = s_nfin;
+    if (nfin > 0) __threadfence();  // the other patches' slices, written before their tickets
+    for (int f = 0; f < nfin; ++f) {
+        const int k = s_fin[f];
         const PartialCol pc = pcol[k];
         if (row) {
             const double* h = halo + pc.hpos + il;

@@ -1162,7 +1162,8 @@ static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cu
     return bicgstab(c, A, b, x, s);
 }
 
-// One round of the refinement as one cooperative kernel: for k < K, r = b - A x (its row-block norms
+// One round of the refinement as one cooperative kernel (BEM_FLAG_REFINE_PERSISTENT; the separate
+// launches below are the default, measured faster): for k < K, r = b - A x (its row-block norms
 // into pr[k]; skipped for k = 0 when the assembly already left that residual) and x += X r, then the
 // final r = b - A x (norms into pr[K]).  The GEMV tiles are k_gemv's (gemv_tile: the same split count,
 // per-thread order and split sums), spread over co-resident CTAs and separated by grid barriers, so the
@@ -1299,10 +1300,10 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         ++rounds;
         tail_valid = false;  // a round changes x
         const bool skip_first = round == 0 && r0_ready;  // the residual and its norms are there
-        bool persistent = c.refine_ok && !(c.prm.flags & BEM_FLAG_REFINE_MULTIKERNEL) &&
-                          refine_round_persistent(c, A, b, x, pr, K, skip_first, s) == BEM_OK;
+        const bool want = c.refine_ok && (c.prm.flags & BEM_FLAG_REFINE_PERSISTENT);
+        const bool persistent = want && refine_round_persistent(c, A, b, x, pr, K, skip_first, s) == BEM_OK;
         if (!persistent) {
-            if (!(c.prm.flags & BEM_FLAG_REFINE_MULTIKERNEL)) c.refine_ok = false;
+            if (want) c.refine_ok = false;
             for (int k = 0; k < K; ++k) {
                 if (!(k == 0 && skip_first))
                     gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr,

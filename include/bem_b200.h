@@ -75,9 +75,11 @@ typedef struct {
  * kernel of bem_assemble, instead of the G-only triangle-patch kernel that forms b = H phi without
  * H.  Both give the same G and b to rounding; for comparison. */
 #define BEM_FLAG_STEP_ASSEMBLE_H 4
-/* bem_params.flags: run each round of BEM_SOLVER_MIXED's refinement steps as separate GEMV launches
- * instead of one cooperative kernel (same tiles and summation order: bit-identical results). */
-#define BEM_FLAG_REFINE_MULTIKERNEL 8
+/* bem_params.flags: run each round of BEM_SOLVER_MIXED's refinement steps as one cooperative kernel
+ * with grid barriers instead of separate GEMV launches (the same tiles and summation order:
+ * bit-identical results).  Measured slower than the separate launches on B200 (0.36 against
+ * 0.27 ms per solve at N = 4002), so it is not the default. */
+#define BEM_FLAG_REFINE_PERSISTENT 8
 
 /* Fill *p with the reference's defaults. */
 void bem_default_params(bem_params* p);

@@ -140,8 +140,8 @@ def test_expired_barrier_wait_falls_back_to_the_multikernel_bicgstab():
 
 
 def test_expired_barrier_wait_in_the_refinement_round_repeats_it_with_separate_launches():
-    # The mixed solve runs each round of refinement steps as one cooperative kernel with grid
-    # barriers.  With a one-cycle bound its first barrier wait runs out: the kernel sets its error word
+    # With BEM_FLAG_REFINE_PERSISTENT the mixed solve runs each round of refinement steps as one
+    # cooperative kernel with grid barriers.  With a one-cycle bound its first barrier wait runs out: the kernel sets its error word
     # and ends, the host counts the expired wait, clears the GEMV tickets and repeats the round with
     # separate GEMV launches (kept for the rest of the context); psi still matches LU.
     v, f = mesh.bubble(8, 1.0, (2.0, 0.0, 0.0))
@@ -150,6 +150,7 @@ def test_expired_barrier_wait_in_the_refinement_round_repeats_it_with_separate_l
     _, psi_lu = lu.position_t(phi, return_psi=True)
     lu.close()
     s = ColocSim(v, f, solver="mixed")
+    s._update(flags=L.FLAG_REFINE_PERSISTENT)
     assert s._L.bem_set_wait_limit(s._h, 1) == L.BEM_OK
     for k in range(2):
         _, psi = s.position_t(phi, return_psi=True)

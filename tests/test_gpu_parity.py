@@ -410,7 +410,7 @@ def test_refinement_round_kernel_equals_separate_launches():
     rng = np.random.default_rng(3)
     v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None]
     out = []
-    for flags in (0, L.FLAG_REFINE_MULTIKERNEL):
+    for flags in (0, L.FLAG_REFINE_PERSISTENT):
         sim = ColocSim(v, f, pressurefield=(-0.8, 2 * np.pi / 5, 0.0), solver="mixed", p_inf=1.0, epsilon=1.0,
                        gamma=1.4)
         sim._update(flags=flags)
