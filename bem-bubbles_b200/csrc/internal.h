@@ -191,8 +191,16 @@ int bicgstab_persistent(Ctx& c, const double* A, const double* b, double* x, cud
 size_t pbicg_words(int64_t n);  // doubles of the persistent BiCGSTAB's dot and barrier scratch
 
 // lu_panel.cu
-int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s);
-int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s);
+// The panel of another column-major n x n matrix (only its columns [k0, k0+nb) are touched); piv and
+// sing as c.piv and c.flag for c.LU.
+struct PanelTarget {
+    double* A;
+    int n;
+    int* piv;
+    int* sing;
+};
+int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* tgt = nullptr);
+int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* tgt = nullptr);
 void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s);  // the panel's interchanges, other columns
 size_t lu_panel_words();   // doubles of Ctx::lu_aux
 int* lu_panel_err(Ctx& c); // device error word of the row-distributed panels
@@ -213,9 +221,23 @@ struct NSJob {
 };
 int ns_step(Ctx& c, const NSJob& j, cudaStream_t s, double* eres, int terms = 3);
 int ns_from_scratch(Ctx& c, const NSJob& j, cudaStream_t s, bool classical);
+// gj_inverse.cu: j.X ~ A^-1 by blocked Gauss-Jordan with tensor-core rank-64 updates (j.T as work)
+int gj_inverse(Ctx& c, const NSJob& j, cudaStream_t s);
 void to_f32(int64_t nn, const double* a, float* b, cudaStream_t s);
 
 // tc_gemm.cu
+// An operand of the general split-precision GEMM: S(r, k) = src[r*sr + k*sk] for r < rows, k < cols,
+// times sign, zero for r in [zr0, zr1) or k in [zk0, zk1).
+struct TcOperand {
+    const float* src;
+    long long sr, sk;
+    int rows, cols;
+    int zr0 = 0, zr1 = 0, zk0 = 0, zk1 = 0;
+    float sign = 1.f;
+};
+void tc_split_op(const TcOperand& o, int rpad, int kpad, void* hi, void* lo, cudaStream_t s);
+int tc_gemm_planes(Ctx& c, int m, int n, int mpad, int npad, int kpad, const void* ah, const void* al, const void* bh,
+                   const void* bl, float* C, int ldc, bool acc, int* err, cudaStream_t s);
 int tc_pad(int n);
 int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* planes, int* err, cudaStream_t s,
             int terms = 3);

@@ -929,6 +929,27 @@ void to_f32(int64_t nn, const double* a, float* b, cudaStream_t s) {
     KLAUNCH(), k_to_f32<<<4 * 148, 256, 0, s>>>(nn, a, b);
 }
 
+// X from scratch by the tensor-core Gauss-Jordan elimination, then Newton-Schulz steps against G
+// until ||I - G X|| is below 1e-2 before the last step (about 1e-4 after it, as the set-up by
+// Newton-Schulz alone ends).
+static int gj_polished(Ctx& c, const NSJob& j, cudaStream_t s) {
+    int rc = gj_inverse(c, j, s);
+    if (rc) return rc;
+    for (int it = 0; it < 8; ++it) {
+        double e = 1.0;
+        if ((rc = ns_step(c, j, s, &e, 3))) return rc;
+        if (!(e < 0.9)) break;
+        if (e < 1e-2) return BEM_OK;
+    }
+    return c.fail(BEM_ERR_NOT_CONVERGED, "Gauss-Jordan inverse: Newton-Schulz polish did not converge");
+}
+
+static bool use_gj(const Ctx& c, int n) {
+    if (c.prm.flags & BEM_FLAG_INVERSE_NS) return false;
+    if (c.prm.flags & BEM_FLAG_INVERSE_GJ) return true;
+    return n >= BEM_GJ_MIN_N;
+}
+
 static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_scratch) {
     const int n = (int)c.topo.N;
     const int64_t nn = (int64_t)n * n;
@@ -937,7 +958,9 @@ static int refresh_inverse(Ctx& c, const double* A, cudaStream_t s, bool from_sc
     to_f32(nn, A, c.G32, s);
     if (from_scratch || !c.xinv_valid) {
         c.xinv_valid = false;
-        int rc = ns_from_scratch(c, j, s, false);
+        int rc = BEM_ERR_CUDA;
+        if (use_gj(c, n)) rc = gj_polished(c, j, s);
+        if (rc != BEM_OK) rc = ns_from_scratch(c, j, s, false);  // the set-up without the elimination
         if (rc) return rc;
         c.xinv_valid = true;
     } else {

@@ -430,8 +430,11 @@ void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s) {
 
 // The panel on one thread-block cluster when its rows fit; BEM_ERR_CUDA when they do not or the
 // cluster launch is unavailable.
-int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s) {
-    const int n = (int)c.topo.N;
+int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* tgt) {
+    const int n = tgt ? tgt->n : (int)c.topo.N;
+    double* A = tgt ? tgt->A : c.LU;
+    int* piv = tgt ? tgt->piv : c.piv;
+    int* sing = tgt ? tgt->sing : c.flag;
     const int P = n - k0;
     if (nb > LP_NBMAX) return BEM_ERR_CUDA;
     const int C = std::max(1, std::min(LC_MAX, (P + 127) / 128));
@@ -466,7 +469,7 @@ int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s) {
         return BEM_ERR_CUDA;
     }
     KLAUNCH();
-    if (cudaLaunchKernelEx(&cfg, k_lu_panel_cluster, n, k0, nb, rows_per, c.LU, c.piv, c.flag) != cudaSuccess) {
+    if (cudaLaunchKernelEx(&cfg, k_lu_panel_cluster, n, k0, nb, rows_per, A, piv, sing) != cudaSuccess) {
         cudaGetLastError();
         return BEM_ERR_CUDA;
     }
@@ -475,11 +478,11 @@ int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s) {
 
 int* lu_panel_err(Ctx& c) { return reinterpret_cast<int*>(lp_bar(c) + 2); }
 
-// Factor panel [k0, k0+nb) of c.LU over rows k0..n-1.  Returns BEM_ERR_CUDA when the cooperative
+// Factor panel [k0, k0+nb) of c.LU (or of tgt's matrix) over rows k0..n-1.  Returns BEM_ERR_CUDA when the cooperative
 // launch is unavailable or a barrier wait expired (the caller falls back to the single-CTA panel,
 // from a fresh copy of the matrix).
-int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s) {
-    const int n = (int)c.topo.N;
+int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* tgt) {
+    const int n = tgt ? tgt->n : (int)c.topo.N;
     int sms = 0, coop = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.device);
@@ -507,9 +510,9 @@ int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s) {
     a.k0 = k0;
     a.nb = nb;
     a.rows_per = rows_per;
-    a.A = c.LU;
-    a.piv = c.piv;
-    a.sing = c.flag;
+    a.A = tgt ? tgt->A : c.LU;
+    a.piv = tgt ? tgt->piv : c.piv;
+    a.sing = tgt ? tgt->sing : c.flag;
     a.cand = c.lu_aux;
     a.diag = lp_diag(c);
     a.bar = lp_bar(c);

@@ -81,11 +81,12 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-template <int BN, int STAGES, int TERMS>
+// C (rows < m, columns < n, column-major with leading dimension ldc) = A B, or += A B with ACC.
+template <int BN, int STAGES, int TERMS, bool ACC = false>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                   const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                  float* __restrict__ C, int n, int ldc, int kblocks, int* __restrict__ err) {
+                  float* __restrict__ C, int m, int n, int ldc, int kblocks, int* __restrict__ err) {
     constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     constexpr uint32_t STAGE_TX = TERMS == 1 ? A_BYTES + B_BYTES : STAGE_BYTES;
@@ -188,11 +189,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                   "=r"(r[15])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < n) {
+            if (row < m) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int col = n0 + c0 + j;
-                    if (col < n) C[(size_t)col * ldc + row] = __uint_as_float(r[j]);
+                    if (col < n) {
+                        float* p = C + (size_t)col * ldc + row;
+                        *p = ACC ? *p + __uint_as_float(r[j]) : __uint_as_float(r[j]);
+                    }
                 }
             }
         }
@@ -239,6 +243,36 @@ __global__ void k_split_bf16(int n, int npad, const float* __restrict__ src, __n
     }
 }
 
+// An operand plane of the general GEMM: plane[r * kpad + k] = sign * S(r, k), bf16 hi/lo split, for
+// r < rows and k < cols, zero in the padding (rpad x kpad) and for r in [zr0, zr1) or k in [zk0, zk1).
+// S(r, k) = src[r * sr + k * sk]: (sr, sk) = (1, ld) reads an A operand stored column-major, (ld, 1) a
+// B operand stored column-major (K x N; the plane's rows are its columns).  32 x 32 tiles, staged
+// through shared memory when the plane's inner index is not the source's contiguous one.
+__global__ void k_split_op(int rows, int cols, int rpad, int kpad, const float* __restrict__ src, long long sr,
+                           long long sk, int zr0, int zr1, int zk0, int zk1, float sign,
+                           __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    __shared__ float tile[32][33];
+    const int k0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    auto value = [&](int r, int k) -> float {
+        if (r >= rows || k >= cols || (r >= zr0 && r < zr1) || (k >= zk0 && k < zk1)) return 0.f;
+        return sign * src[(long long)r * sr + (long long)k * sk];
+    };
+    auto put = [&](int r, int k, float v) {
+        if (r < rpad && k < kpad) {
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            hi[(size_t)r * kpad + k] = h;
+            lo[(size_t)r * kpad + k] = __float2bfloat16_rn(v - __bfloat162float(h));
+        }
+    };
+    if (sr == 1) {  // contiguous along r: read along r, write along k through the tile
+        for (int q = threadIdx.y; q < 32; q += blockDim.y) tile[q][threadIdx.x] = value(r0 + threadIdx.x, k0 + q);
+        __syncthreads();
+        for (int q = threadIdx.y; q < 32; q += blockDim.y) put(r0 + q, k0 + threadIdx.x, tile[threadIdx.x][q]);
+    } else {  // contiguous along k (or neither): both along k
+        for (int q = threadIdx.y; q < 32; q += blockDim.y) put(r0 + q, k0 + threadIdx.x, value(r0 + q, k0 + threadIdx.x));
+    }
+}
+
 // ---------------------------------------------------------------- host side
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -254,6 +288,19 @@ static EncodeTiledFn encode_fn() {
             fn = reinterpret_cast<EncodeTiledFn>(p);
     }
     return fn;
+}
+
+// 2-D bf16 plane of `rows` rows x kpad (K innermost), box {64, box_rows}, 128-byte swizzle
+static bool make_map_rows(CUtensorMap* m, const void* base, int kpad, int rows, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kpad * 2};
+    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // 2-D bf16 plane npad x npad (K innermost), box {64, rows}, 128-byte swizzle
@@ -304,11 +351,50 @@ int tc_gemm(Ctx& c, int n, const float* A, const float* B, float* C, void* plane
     }
     dim3 grid(npad / TC_BN, npad / TC_BM);
     if (terms == 1)
-        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 1><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 1><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, n, npad / TC_BK, err);
     else
-        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, npad / TC_BK, err);
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, n, n, n, npad / TC_BK, err);
     // a launch refused for its configuration (shared memory, grid) leaves C unwritten: report it here,
     // since a later stream synchronisation does not
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return c.fail(BEM_ERR_CUDA, std::string("tensor-core GEMM launch: ") + cudaGetErrorString(le));
+    return BEM_OK;
+}
+
+void tc_split_op(const TcOperand& o, int rpad, int kpad, void* hi, void* lo, cudaStream_t s) {
+    dim3 g((kpad + 31) / 32, (rpad + 31) / 32), b(32, 8);
+    KLAUNCH(), k_split_op<<<g, b, 0, s>>>(o.rows, o.cols, rpad, kpad, o.src, o.sr, o.sk, o.zr0, o.zr1, o.zk0, o.zk1,
+                                          o.sign, static_cast<__nv_bfloat16*>(hi), static_cast<__nv_bfloat16*>(lo));
+}
+
+// C (m x n, column-major, ldc) = A B, or += A B (acc), from operand planes made by tc_split_op:
+// A planes mpad x kpad, B planes npad x kpad (mpad a multiple of 128, npad of 256, kpad of 64).
+int tc_gemm_planes(Ctx& c, int m, int n, int mpad, int npad, int kpad, const void* ah, const void* al, const void* bh,
+                   const void* bl, float* C, int ldc, bool acc, int* err, cudaStream_t s) {
+    if (mpad % TC_BM || npad % TC_BN || kpad % TC_BK || m > mpad || n > npad)
+        return c.fail(BEM_ERR_ARG, "tc_gemm_planes: plane shape");
+    CUtensorMap mAh, mAl, mBh, mBl;
+    if (!make_map_rows(&mAh, ah, kpad, mpad, TC_BM) || !make_map_rows(&mAl, al, kpad, mpad, TC_BM) ||
+        !make_map_rows(&mBh, bh, kpad, npad, TC_BN) || !make_map_rows(&mBl, bl, kpad, npad, TC_BN))
+        return c.fail(BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    const size_t sm = tc_smem_bytes();
+    static std::atomic<uint64_t> attr{0};
+    if (!once_per_device(attr, [sm] {
+            return cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess;
+        })) {
+        cudaGetLastError();
+        return c.fail(BEM_ERR_CUDA, "cudaFuncSetAttribute failed for the tensor-core GEMM");
+    }
+    dim3 grid(npad / TC_BN, mpad / TC_BM);
+    if (acc)
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3, true><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc,
+                                                                                   kpad / TC_BK, err);
+    else
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3, false><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc,
+                                                                                    kpad / TC_BK, err);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return c.fail(BEM_ERR_CUDA, std::string("tensor-core GEMM launch: ") + cudaGetErrorString(le));
     return BEM_OK;

@@ -80,6 +80,13 @@ typedef struct {
  * bit-identical results).  Measured slower than the separate launches on B200 (0.36 against
  * 0.27 ms per solve at N = 4002), so it is not the default. */
 #define BEM_FLAG_REFINE_PERSISTENT 8
+/* bem_params.flags: how BEM_SOLVER_MIXED builds its approximate inverse from scratch.  By default
+ * (neither flag) large systems (N >= BEM_GJ_MIN_N) use blocked Gauss-Jordan elimination with row
+ * partial pivoting in FP32, its rank-64 updates as split-precision tcgen05 GEMMs, polished by
+ * Newton-Schulz steps; smaller ones use Newton-Schulz from a scaled identity.  The flags force one. */
+#define BEM_FLAG_INVERSE_GJ 16
+#define BEM_FLAG_INVERSE_NS 32
+#define BEM_GJ_MIN_N 8192
 
 /* Fill *p with the reference's defaults. */
 void bem_default_params(bem_params* p);
@@ -265,6 +272,8 @@ typedef struct {
                                  the mixed path, including its GMRES hand-overs; BiCGSTAB iterations) */
     int64_t wait_expired;     /* bounded grid-barrier waits of the persistent kernels (BiCGSTAB, LU
                                  panel) that gave up; each sent the context to the multi-kernel form */
+    int64_t gj_inverses;      /* approximate inverses of the mixed path built by the tensor-core
+                                 Gauss-Jordan elimination (the rest by Newton-Schulz from scratch) */
 } bem_stats;
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 

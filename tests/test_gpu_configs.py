@@ -143,5 +143,6 @@ def test_large_pair_mixed_step_matches_fp64():
     _, psi64 = sim.position_t(ph, return_psi=True)
     st = sim.stats()
     sim.close()
+    assert st.gj_inverses == 1  # the set-up of the inverse at this size: tensor-core Gauss-Jordan
     assert st.last_rel_residual <= 1e-14
     assert rel(psi_mix, psi64) <= 1e-8
