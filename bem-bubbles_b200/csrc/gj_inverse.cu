@@ -6,7 +6,7 @@
 //     lu_panel.cu on an FP64 copy of the panel), the same row choice as unblocked Gauss-Jordan;
 //   * the interchanges applied to whole rows of A, and to the permutation perm;
 //   * with B the panel's rows and O the others, b the panel's columns and o the others:
-//       W = A_Bb^-1                       (from the panel's L and U, FP64, one CTA)
+//       W = A_Bb^-1                       (in-place Gauss-Jordan of the pivoted block, FP64, one CTA)
 //       P = -A_Ob W                       (tcgen05 GEMM, n x nb x nb)
 //       R' = W A_Bo                       (tcgen05 GEMM, nb x n x nb)
 //       A_Oo += P A_Bo                    (tcgen05 GEMM, n x n x nb, accumulating into A)
@@ -66,35 +66,41 @@ __global__ void k_gj_swap(int n, int k0, int nb, const int* __restrict__ piv, fl
         }
 }
 
-// W = (L U)^-1 of the factored panel's leading nb x nb block (unit lower L and upper U packed in Pm,
-// leading dimension m), FP64: column c by thread c, forward substitution on e_c, then back substitution.
-__global__ void __launch_bounds__(GJ_NB) k_gj_block_inverse(int m, int nb, const double* __restrict__ Pm,
-                                                            float* __restrict__ W, int* __restrict__ sing) {
-    extern __shared__ double gj_smem[];  // LU and Y, GJ_NB x (GJ_NB + 1) each
-    double (*LU)[GJ_NB + 1] = reinterpret_cast<double (*)[GJ_NB + 1]>(gj_smem);
-    double (*Y)[GJ_NB + 1] = reinterpret_cast<double (*)[GJ_NB + 1]>(gj_smem + GJ_NB * (GJ_NB + 1));
-    const int c = threadIdx.x;
-    if (c < nb)
-        for (int r = 0; r < nb; ++r) LU[r][c] = Pm[(size_t)c * m + r];
+// W = A_Bb^-1 for the panel's nb x nb block of A after its interchanges, by in-place Gauss-Jordan
+// without further pivoting in FP64 (the rows are already the partial-pivoting choice over the whole
+// panel, so every pivot is the largest entry left in its column of the block): step k scales row k
+// by 1/p and takes f_i times it from every other row i, all elements of a step in parallel.
+__global__ void __launch_bounds__(1024) k_gj_block_inverse(int n, int k0, int nb, const float* __restrict__ A,
+                                                           float* __restrict__ W, int* __restrict__ sing) {
+    __shared__ double M[GJ_NB][GJ_NB + 1];
+    __shared__ double s_f[GJ_NB];
+    __shared__ double s_p;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < nb * nb; e += nt) {
+        const int c = e / nb, r = e - c * nb;
+        M[r][c] = (double)A[(size_t)(k0 + c) * n + k0 + r];
+    }
     __syncthreads();
-    if (c >= nb) return;
-    for (int r = 0; r < nb; ++r) {
-        double v = (r == c) ? 1.0 : 0.0;
-        for (int q = 0; q < r; ++q) v -= LU[r][q] * Y[q][c];
-        Y[r][c] = v;
-    }
-    for (int r = nb - 1; r >= 0; --r) {
-        double v = Y[r][c];
-        for (int q = r + 1; q < nb; ++q) v -= LU[r][q] * Y[q][c];
-        const double d = LU[r][r];
-        if (d == 0.0) {
-            atomicExch(sing, 1);
-            Y[r][c] = 0.0;
-        } else {
-            Y[r][c] = v / d;
+    for (int k = 0; k < nb; ++k) {
+        if (tid < nb) s_f[tid] = M[tid][k];
+        if (tid == 0) {
+            s_p = M[k][k];
+            if (s_p == 0.0) atomicExch(sing, 1);
         }
+        __syncthreads();
+        const double ip = s_p != 0.0 ? 1.0 / s_p : 0.0;
+        if (tid < nb) M[k][tid] = (tid == k ? 1.0 : M[k][tid]) * ip;
+        __syncthreads();
+        for (int e = tid; e < nb * nb; e += nt) {
+            const int i = e / nb, j = e - i * nb;
+            if (i != k) M[i][j] = (j == k ? 0.0 : M[i][j]) - s_f[i] * M[k][j];
+        }
+        __syncthreads();
     }
-    for (int r = 0; r < nb; ++r) W[(size_t)c * nb + r] = (float)Y[r][c];
+    for (int e = tid; e < nb * nb; e += nt) {
+        const int c = e / nb, r = e - c * nb;
+        W[(size_t)c * nb + r] = (float)M[r][c];
+    }
 }
 
 // After the accumulating GEMM: the panel's columns take P (zero in the panel's rows) and W in the
@@ -129,7 +135,7 @@ __global__ void k_iota(int n, int* __restrict__ v) {
 
 inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-constexpr size_t GJ_BLOCK_SMEM = sizeof(double) * 2 * GJ_NB * (GJ_NB + 1);
+
 
 }  // namespace
 
@@ -167,14 +173,6 @@ int gj_inverse(Ctx& c, const NSJob& j, cudaStream_t s) {
     __nv_bfloat16 *Bh = Al + (size_t)mpad * kpad, *Bl = Bh + (size_t)npad * kpad;
     __nv_bfloat16 *Wah = Bl + (size_t)npad * kpad, *Wal = Wah + 128 * kpad;
     __nv_bfloat16 *Wbh = Wal + 128 * kpad, *Wbl = Wbh + 256 * kpad;
-    static std::atomic<uint64_t> attr{0};
-    if (!once_per_device(attr, [] {
-            return cudaFuncSetAttribute(k_gj_block_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)GJ_BLOCK_SMEM) == cudaSuccess;
-        })) {
-        cudaGetLastError();
-        return BEM_ERR_CUDA;
-    }
     KLAUNCH(), k_iota<<<(n + 255) / 256, 256, 0, s>>>(n, perm);
     BEM_CUDA(c, cudaMemsetAsync(sing, 0, sizeof(int), s));
     BEM_CUDA(c, cudaMemsetAsync(lu_panel_err(c), 0, sizeof(int), s));
@@ -186,7 +184,7 @@ int gj_inverse(Ctx& c, const NSJob& j, cudaStream_t s) {
         if (lu_panel_cluster(c, 0, nb, s, &tgt) != BEM_OK && lu_panel_rows(c, 0, nb, s, &tgt) != BEM_OK)
             return BEM_ERR_CUDA;
         KLAUNCH(), k_gj_swap<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, piv, A, perm);
-        KLAUNCH(), k_gj_block_inverse<<<1, NB, GJ_BLOCK_SMEM, s>>>(m, nb, Pm, W, sing);
+        KLAUNCH(), k_gj_block_inverse<<<1, 1024, 0, s>>>(n, k0, nb, A, W, sing);
         // P = -A_Ob W: A operand the panel's columns with its rows masked, B operand W (K x N = nb x nb)
         TcOperand a1{A + (size_t)k0 * n, 1, (long long)n, n, nb, k0, k1, 0, 0, -1.f};
         TcOperand b1{W, (long long)nb, 1, nb, nb};

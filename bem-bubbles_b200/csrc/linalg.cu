@@ -929,12 +929,50 @@ void to_f32(int64_t nn, const double* a, float* b, cudaStream_t s) {
     KLAUNCH(), k_to_f32<<<4 * 148, 256, 0, s>>>(nn, a, b);
 }
 
-// X from scratch by the tensor-core Gauss-Jordan elimination, then Newton-Schulz steps against G
-// until ||I - G X|| is below 1e-2 before the last step (about 1e-4 after it, as the set-up by
-// Newton-Schulz alone ends).
+// v[i] in [-1, 1), a fixed hash of i
+__global__ void k_fill_hash(int n, double* __restrict__ v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)i * 2654435761u + 0x9e3779b9u;
+        h ^= h >> 16;
+        h *= 0x85ebca6bu;
+        h ^= h >> 13;
+        v[i] = (double)(h >> 8) * (2.0 / 16777216.0) - 1.0;
+    }
+}
+
+__global__ void k_rowblock_norm2(int n, const double* __restrict__ b, double* __restrict__ part);
+
+// ||(I - G X) v|| / ||v|| for a fixed pseudo-random v (two GEMVs): an estimate of how much one
+// refinement step with X contracts the error.
+static int inverse_resid_estimate(Ctx& c, const NSJob& j, cudaStream_t s, double* est) {
+    const int n = j.n, nrb = (n + GV_ROWS - 1) / GV_ROWS;
+    double *v = c.r0, *w = c.tv, *r = c.yv;
+    KLAUNCH(), k_fill_hash<<<VBLK, VTHR, 0, s>>>(n, v);
+    gemv_t<float>(n, j.X, v, w, s, c.part, c.cnt);                                              // w = X v
+    gemv_t<double>(n, j.A, w, r, s, c.part, c.cnt, nullptr, 0, r, c.red, nullptr, nullptr, v, -1.0);  // r = v - G w
+    KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, v, c.red + nrb);
+    std::vector<double> h((size_t)2 * nrb);
+    BEM_CUDA(c, cudaMemcpyAsync(h.data(), c.red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+    BEM_CUDA(c, cudaStreamSynchronize(s));
+    double rr = 0.0, vv = 0.0;
+    for (int q = 0; q < nrb; ++q) {
+        rr += h[(size_t)q];
+        vv += h[(size_t)nrb + q];
+    }
+    *est = vv > 0.0 ? sqrt(rr / vv) : 1.0;
+    return BEM_OK;
+}
+
+// X from scratch by the tensor-core Gauss-Jordan elimination.  When the estimate of ||(I - G X) v||
+// is already below 1e-3 X is kept as it is; otherwise Newton-Schulz steps against G follow until
+// ||I - G X|| is below 1e-2 before the last step (about 1e-4 after it, as the set-up by Newton-Schulz
+// alone ends).
 static int gj_polished(Ctx& c, const NSJob& j, cudaStream_t s) {
     int rc = gj_inverse(c, j, s);
     if (rc) return rc;
+    double est = 1.0;
+    if ((rc = inverse_resid_estimate(c, j, s, &est))) return rc;
+    if (est < 1e-3) return BEM_OK;
     for (int it = 0; it < 8; ++it) {
         double e = 1.0;
         if ((rc = ns_step(c, j, s, &e, 3))) return rc;

@@ -178,25 +178,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     if (have && !abort_flag) {
         const int row = m0 + warp * 32 + lane;
+        // 32 columns per round; with ACC the round's 32 values of C are loaded first, all in flight
+        // together before the tensor-memory read (one memory latency per round, not one per element)
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(taddr));
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            float cv[32];
+            if (ACC) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = n0 + c0 + j;
+                    cv[j] = (row < m && col < n) ? C[(size_t)col * ldc + row] : 0.f;
+                }
+            }
+            uint32_t r[32];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c0 + 16 * h);
+                uint32_t* q = r + 16 * h;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                    : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+                      "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]),
+                      "=r"(q[15])
+                    : "r"(taddr));
+            }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (row < m) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
+                for (int j = 0; j < 32; ++j) {
                     const int col = n0 + c0 + j;
-                    if (col < n) {
-                        float* p = C + (size_t)col * ldc + row;
-                        *p = ACC ? *p + __uint_as_float(r[j]) : __uint_as_float(r[j]);
-                    }
+                    if (col < n) C[(size_t)col * ldc + row] = ACC ? cv[j] + __uint_as_float(r[j]) : __uint_as_float(r[j]);
                 }
             }
         }
@@ -320,7 +331,10 @@ constexpr int TC_BN = 256, TC_STAGES = 2;
 
 int tc_pad(int n) { return (n + 255) / 256 * 256; }
 
-size_t tc_smem_bytes() { return (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 2 + 2 * TC_BN * TC_BK * 2) + 1024; }
+size_t tc_smem_bytes(int stages = TC_STAGES, int bn = TC_BN) {
+    return (size_t)stages * (2 * TC_BM * TC_BK * 2 + 2 * bn * TC_BK * 2) + 1024;
+}
+constexpr int TC_BN_ACC = 128;  // the accumulating GEMM's tile width: three CTAs per SM with one stage
 
 // C = A * B (all FP32, column-major n x n, leading dimension n).  Work buffers: four bf16 planes
 // of tc_pad(n)^2 elements each (ah, al, bh, bl); err: device int (non-zero after a timeout).
@@ -373,28 +387,48 @@ int tc_gemm_planes(Ctx& c, int m, int n, int mpad, int npad, int kpad, const voi
                    const void* bl, float* C, int ldc, bool acc, int* err, cudaStream_t s) {
     if (mpad % TC_BM || npad % TC_BN || kpad % TC_BK || m > mpad || n > npad)
         return c.fail(BEM_ERR_ARG, "tc_gemm_planes: plane shape");
+    const int kb = kpad / TC_BK;
+    const bool narrow = acc && kb == 1;  // the accumulating rank-64 update: 128-column tiles
     CUtensorMap mAh, mAl, mBh, mBl;
+    const int bn = narrow ? TC_BN_ACC : TC_BN;
     if (!make_map_rows(&mAh, ah, kpad, mpad, TC_BM) || !make_map_rows(&mAl, al, kpad, mpad, TC_BM) ||
-        !make_map_rows(&mBh, bh, kpad, npad, TC_BN) || !make_map_rows(&mBl, bl, kpad, npad, TC_BN))
+        !make_map_rows(&mBh, bh, kpad, npad, bn) || !make_map_rows(&mBl, bl, kpad, npad, bn))
         return c.fail(BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    const size_t sm = tc_smem_bytes();
+    const size_t sm2 = tc_smem_bytes(2), sm1 = tc_smem_bytes(1), smn = tc_smem_bytes(1, TC_BN_ACC);
     static std::atomic<uint64_t> attr{0};
-    if (!once_per_device(attr, [sm] {
-            return cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3, false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess &&
-                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, TC_STAGES, 3, true>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess;
+    if (!once_per_device(attr, [sm1, sm2, smn] {
+            return cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, 2, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm2) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, 2, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm2) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, 1, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm1) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN, 1, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sm1) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_gemm_bf16x3<TC_BN_ACC, 1, 3, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smn) == cudaSuccess;
         })) {
         cudaGetLastError();
         return c.fail(BEM_ERR_CUDA, "cudaFuncSetAttribute failed for the tensor-core GEMM");
     }
     dim3 grid(npad / TC_BN, mpad / TC_BM);
-    if (acc)
-        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3, true><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc,
-                                                                                   kpad / TC_BK, err);
-    else
-        KLAUNCH(), k_gemm_bf16x3<TC_BN, TC_STAGES, 3, false><<<grid, TC_THREADS, sm, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc,
-                                                                                    kpad / TC_BK, err);
+    if (narrow) {
+        dim3 gn(npad / TC_BN_ACC, mpad / TC_BM);
+        KLAUNCH(), k_gemm_bf16x3<TC_BN_ACC, 1, 3, true><<<gn, TC_THREADS, smn, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc, kb,
+                                                                                 err);
+    } else if (kb == 1) {  // one k-block: a one-stage ring, half the shared memory, two CTAs per SM
+        if (acc)
+            KLAUNCH(), k_gemm_bf16x3<TC_BN, 1, 3, true><<<grid, TC_THREADS, sm1, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc, kb,
+                                                                                 err);
+        else
+            KLAUNCH(), k_gemm_bf16x3<TC_BN, 1, 3, false><<<grid, TC_THREADS, sm1, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc, kb,
+                                                                                  err);
+    } else if (acc) {
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, 2, 3, true><<<grid, TC_THREADS, sm2, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc, kb, err);
+    } else {
+        KLAUNCH(), k_gemm_bf16x3<TC_BN, 2, 3, false><<<grid, TC_THREADS, sm2, s>>>(mAh, mAl, mBh, mBl, C, m, n, ldc, kb,
+                                                                              err);
+    }
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return c.fail(BEM_ERR_CUDA, std::string("tensor-core GEMM launch: ") + cudaGetErrorString(le));
     return BEM_OK;
