@@ -97,6 +97,9 @@ public:
 
     // mixed precision (FP64 refinement on a low-precision inverse) instead of the FP64 solver
     void set_mixed_precision(bool value) { mixed = value; }
+    // the GPU solver's counters since the context was created (bem_stats; all zero before the first step)
+    void gpu_stats(int64_t* solves, int64_t* iterations, int64_t* ns_steps, int64_t* refreshes,
+                   int64_t* fp64_fallbacks, int64_t* gmres_fallbacks) const;
 
 protected:
     real get_dt(real dp, std::vector<vec3> const& gradients, std::vector<real> const& grad_potential) const;

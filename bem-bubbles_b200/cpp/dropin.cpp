@@ -88,6 +88,18 @@ bem_ctx* Simulation::device_ctx() const {
     return ctx_;
 }
 
+void Simulation::gpu_stats(int64_t* solves, int64_t* iterations, int64_t* ns_steps, int64_t* refreshes,
+                           int64_t* fp64_fallbacks, int64_t* gmres_fallbacks) const {
+    bem_stats st{};
+    if (ctx_) check(bem_get_stats(ctx_, &st));
+    *solves = st.solves;
+    *iterations = st.total_iters;
+    *ns_steps = st.ns_steps;
+    *refreshes = st.precond_refresh;
+    *fp64_fallbacks = st.fp64_fallbacks;
+    *gmres_fallbacks = st.gmres_fallbacks;
+}
+
 bem_ctx* Simulation::context(Mesh const& m) const {
     device_ctx();
     bem_params p;

@@ -54,10 +54,22 @@ int main(int argc, char* argv[]) {
         const auto t1 = clk::now();
         sim.remesh(0.12);
         const auto t2 = clk::now();
+#ifdef CYCLE_DROPIN
+        int64_t s0[6], s1[6];
+        sim.gpu_stats(&s0[0], &s0[1], &s0[2], &s0[3], &s0[4], &s0[5]);
+#endif
         for (int j = 0; j < 4; ++j) sim.evolve_system(0.02);
         const auto t3 = clk::now();
-        std::printf("iteration %d verts %zu export_ms %.2f remesh_ms %.2f steps_ms %.2f\n", i, sim.mesh.verts.size(),
+        std::printf("iteration %d verts %zu export_ms %.2f remesh_ms %.2f steps_ms %.2f", i, sim.mesh.verts.size(),
                     ms(t0, t1), ms(t1, t2), ms(t2, t3));
+#ifdef CYCLE_DROPIN
+        // the GPU solver's work in this iteration's four steps
+        sim.gpu_stats(&s1[0], &s1[1], &s1[2], &s1[3], &s1[4], &s1[5]);
+        std::printf(" solves %lld iters %lld ns_steps %lld refreshes %lld fp64_fallbacks %lld gmres_fallbacks %lld",
+                    (long long)(s1[0] - s0[0]), (long long)(s1[1] - s0[1]), (long long)(s1[2] - s0[2]),
+                    (long long)(s1[3] - s0[3]), (long long)(s1[4] - s0[4]), (long long)(s1[5] - s0[5]));
+#endif
+        std::printf("\n");
         if (i > 0) {
             te += ms(t0, t1);
             tr += ms(t1, t2);
