@@ -761,10 +761,15 @@ void launch_assemble(Ctx& c, const double* x, const double* phi, double* G, doub
 // A column whose vertex has all its triangles in the patch is complete and goes straight to G; the
 // columns of vertices shared with other patches go to halo columns.  For each shared vertex and row
 // tile, the patch CTA that finishes last (a ticket counter) sums the halo slices in increasing patch
-// order, while they are still in L2, and writes the G column.  The singular pairs and b's 4 pi term
-// follow in k_singular_diag<., true>.
-// Per G entry the order is: the regular pairs of each patch in increasing triangle order, the patches
-// in increasing order, then the singular pairs; no atomics, so results are bit-reproducible.
+// order, while they are still in L2, and writes the G column.
+// Without the wall image the singular pairs (3 per triangle, the polar rule of Integrator.cpp:13-41)
+// are evaluated beside the records, one thread per (triangle, corner), and the tile loop adds them
+// where the row is a vertex of the triangle; k_rhs_finish then sums each row's patch partials of b
+// and adds the 4 pi term.  Per G entry the order is: the pairs of each patch, regular and singular,
+// in increasing triangle order (for a column inside one patch, the reference's per-column order),
+// then the patches in increasing order.  With the wall image the singular pairs carry an H part too;
+// k_singular_diag<true, true> adds them after the tiles, with the 4 pi term.  No atomics on values,
+// so results are bit-reproducible.
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -804,11 +809,32 @@ constexpr int COPY_WAIT_POLLS = 1 << 22;  // each poll may suspend the thread fo
 
 // Patch-order triangle records (PREC doubles): the k_triangle_records layout (0-27), the potential
 // at the three vertices (28-30), the vertex ids (31, 21 bits each, as the bits of a double) and the
-// column slots of the three vertices in the patch (32, 8 bits each); 33 is padding.
+// column slots of the three vertices in the patch (32, 8 bits each).  Without the wall image the
+// image points (16-22) are unused, and those doubles with 33-34 hold the triangle's singular pairs:
+// for row = vertex k of the triangle, the G entry of the column of vertex v at sing_slot(3 k + v).
+// 35 is padding.
+__device__ __forceinline__ int sing_slot(int e) { return e < 7 ? 16 + e : 26 + e; }
+
+// Threads [0, M): the records; without the wall image threads [M, 4M) also evaluate the singular
+// pairs, one (triangle, corner) each (Integrator.cpp:13-41), into the record's singular slots.
+template <bool MIRROR>
 __global__ void k_patch_records(int M, const double* __restrict__ x, const double* __restrict__ phi,
                                 const int* __restrict__ tri, const int* __restrict__ ptri,
                                 const int* __restrict__ pslot, double* __restrict__ prec) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!MIRROR && q >= M) {
+        if (q >= 4 * M) return;
+        const int p = (q - M) / 3, k = (q - M) - 3 * p;
+        const int t = ptri[p];
+        const int ta = tri[3 * t], tb = tri[3 * t + 1], tc = tri[3 * t + 2];
+        double gg[3], hh[3];
+        singular_sums<false>(x, ta, tb, tc, k, gg, hh);  // gg[m]: the column of vertex (m + k) % 3
+        double* r = prec + (size_t)p * PREC;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) r[sing_slot(3 * k + (m + k) % 3)] = gg[m];
+        return;
+    }
+    const int p = q;
     if (p >= M) return;
     const int t = ptri[p];
     const int ia = tri[3 * t], ib = tri[3 * t + 1], ic = tri[3 * t + 2];
@@ -829,11 +855,11 @@ __global__ void k_patch_records(int M, const double* __restrict__ x, const doubl
     r[7] = 2.0 * bcy;
     r[8] = 2.0 * bcz;
 #pragma unroll
-    for (int q = 0; q < 7; ++q) {
-        const double u = c_quv[q][0], v = c_quv[q][1];
+    for (int q2 = 0; q2 < 7; ++q2) {
+        const double u = c_quv[q2][0], v = c_quv[q2][1];
         const double wx = u * abx + v * bcx, wy = u * aby + v * bcy, wz = u * abz + v * bcz;
-        r[9 + q] = wx * wx + wy * wy + wz * wz;
-        r[16 + q] = ax + wx;
+        r[9 + q2] = wx * wx + wy * wy + wz * wz;
+        if (MIRROR) r[16 + q2] = ax + wx;
     }
     const double unx = nx * ia_, uny = ny * ia_, unz = nz * ia_;
     r[23] = unx;
@@ -846,7 +872,11 @@ __global__ void k_patch_records(int M, const double* __restrict__ x, const doubl
     r[30] = phi[ic];
     r[31] = __longlong_as_double((long long)ia | ((long long)ib << 21) | ((long long)ic << 42));
     r[32] = __longlong_as_double((long long)pslot[p]);
-    r[33] = 0.0;
+    if (MIRROR) {
+        r[33] = 0.0;
+        r[34] = 0.0;
+    }
+    r[35] = 0.0;
 }
 
 template <int ROWS>
@@ -870,7 +900,7 @@ __global__ void __launch_bounds__(ROWS, MINB)
     double* srec = psmem;                  // [PT_MAX][PREC], the patch's records
     double* acc = psmem + PT_MAX * PREC;   // [PCOLS][ROWS], this CTA's rows of the patch's columns
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_col[PCOLS], s_pk[PCOLS], s_fin[PCOLS];
+    __shared__ int s_col[PCOLS], s_pk[PCOLS];
     __shared__ long long s_dst[PCOLS];
     const int tid = threadIdx.x;
     const int2 wk = work[blockIdx.x];
@@ -908,12 +938,21 @@ __global__ void __launch_bounds__(ROWS, MINB)
     for (int t = 0; t < (row ? P.nt : 0); ++t) {
         const double* r = srec + t * PREC;
         const long long ids = __double_as_longlong(r[31]);
-        if (i == (int)(ids & 0x1FFFFF) || i == (int)((ids >> 21) & 0x1FFFFF) || i == (int)(ids >> 42))
-            continue;  // singular pair: k_singular_diag
-        PairSums ps;
-        regular_pair<MIRROR>(r, xi0, xi1, xi2, ps);
         const int code = (int)__double_as_longlong(r[32]);
         const int s0 = code & 255, s1 = (code >> 8) & 255, s2 = (code >> 16) & 255;
+        const int ka = i == (int)(ids & 0x1FFFFF) ? 0 : (i == (int)((ids >> 21) & 0x1FFFFF) ? 1 : 2);
+        if (ka < 2 || i == (int)(ids >> 42)) {
+            // singular pair: without the wall image its G entries come with the records (the double
+            // layer of the flat own triangle vanishes); with it, k_singular_diag<true, true> adds both
+            if (!MIRROR) {
+                acc[s0 * ROWS + tid] += r[sing_slot(3 * ka)];
+                acc[s1 * ROWS + tid] += r[sing_slot(3 * ka + 1)];
+                acc[s2 * ROWS + tid] += r[sing_slot(3 * ka + 2)];
+            }
+            continue;
+        }
+        PairSums ps;
+        regular_pair<MIRROR>(r, xi0, xi1, xi2, ps);
         acc[s0 * ROWS + tid] = fma(ps.g[0], ps.area, acc[s0 * ROWS + tid]);
         acc[s1 * ROWS + tid] = fma(ps.g[1], ps.area, acc[s1 * ROWS + tid]);
         acc[s2 * ROWS + tid] = fma(ps.g[2], ps.area, acc[s2 * ROWS + tid]);
@@ -946,32 +985,50 @@ __global__ void __launch_bounds__(ROWS, MINB)
     __syncthreads();
     __shared__ int s_nfin;
     static_assert(PCOLS == 32, "the finishing slots are drawn by one warp");
+    static_assert(PT_MAX * PREC * sizeof(double) >= PCOLS * sizeof(PartialCol), "finishing slots fit the records");
+    PartialCol* s_pc = reinterpret_cast<PartialCol*>(srec);  // the records are no longer read
     if (tid < PCOLS) {
         const int k = s_pk[tid];
         bool fin = false;
+        PartialCol pc;
         if (k >= 0) {
-            const PartialCol pc = pcol[k];
+            pc = pcol[k];
             fin = atomicAdd(&halo_tick[pc.tick + rt], 1u) == (unsigned)(pc.cnt - 1);
         }
-        // the finishing slots, compacted in slot order
+        // the finishing columns, compacted in slot order
         const unsigned m = __ballot_sync(0xffffffffu, fin);
-        if (fin) s_fin[__popc(m & ((1u << tid) - 1u))] = k;
+        if (fin) s_pc[__popc(m & ((1u << tid) - 1u))] = pc;
         if (tid == 0) s_nfin = __popc(m);
     }
     __syncthreads();
     const int nfin = s_nfin;
     if (nfin > 0) __threadfence();  // the other patches' slices, written before their tickets
-    for (int f = 0; f < nfin; ++f) {
-        const int k = s_fin[f];
-        const PartialCol pc = pcol[k];
-        if (row) {
+    // four columns at a time, the first four slices of each loaded before any is summed (the slices
+    // sit in L2: one round trip per four columns instead of one per column)
+    constexpr int FC = 4, FS = 4;
+    for (int f0 = 0; f0 < (row ? nfin : 0); f0 += FC) {
+        double v[FC][FS];
+#pragma unroll
+        for (int f = 0; f < FC; ++f) {
+            const PartialCol& pc = s_pc[f0 + f < nfin ? f0 + f : f0];
             const double* h = halo + pc.hpos + il;
-            double sum = __ldcg(h);
-            for (int c2 = 1; c2 < pc.cnt; ++c2) sum += __ldcg(h + (size_t)c2 * pc.n);
+#pragma unroll
+            for (int c2 = 0; c2 < FS; ++c2) v[f][c2] = (f0 + f < nfin && c2 < pc.cnt) ? __ldcg(h + (size_t)c2 * pc.n) : 0.0;
+        }
+#pragma unroll
+        for (int f = 0; f < FC; ++f) {
+            if (f0 + f >= nfin) break;
+            const PartialCol& pc = s_pc[f0 + f];
+            double sum = v[f][0];
+#pragma unroll
+            for (int c2 = 1; c2 < FS; ++c2)
+                if (c2 < pc.cnt) sum += v[f][c2];
+            const double* h = halo + pc.hpos + il;
+            for (int c2 = FS; c2 < pc.cnt; ++c2) sum += __ldcg(h + (size_t)c2 * pc.n);
             G[pc.gpos + il] = sum;
         }
-        if (tid == 0) halo_tick[pc.tick + rt] = 0u;  // for the next assembly
     }
+    if (tid < nfin) halo_tick[s_pc[tid].tick + rt] = 0u;  // for the next assembly
 }
 
 // The G-only singular pass of a batch: rows of block vblk[i], its patches' row partials.
@@ -986,6 +1043,49 @@ __global__ void __launch_bounds__(32 * SD_WARPS)
     const BlockInfo B = blk[vblk[i]];
     singular_diag_row<MIRROR, true>(i, i - B.vbase, B.n, B.mbase, B.vbase, B.npatch, nullptr, bp + B.ppbase, x, tri,
                                     csr_off, csr_idx, phi, G, nullptr, b, nullptr, nullptr, nullptr);
+}
+
+// b_i (and r0_i = b_i - (G x0)_i) of the G-only assembly without the wall image, one warp per row:
+// the tiles already hold every pair of the row, so what is left is the sum of the row's patch partials
+// (lane l takes patches l, l + 32, ..., the lanes add in a fixed butterfly order) and the 4 pi term,
+// b_i = sum_j H(i, j) (phi_j - phi_i) - 4 pi phi_i (ColocSim.cpp:85-97).
+__device__ __forceinline__ void rhs_finish_row(int i, int il, int np, const double* __restrict__ bp,
+                                               const double* __restrict__ phi, double* __restrict__ b,
+                                               const double* __restrict__ x0, const double* __restrict__ gp,
+                                               double* __restrict__ r0) {
+    const int lane = threadIdx.x & 31;
+    const size_t pr = (size_t)il * np;  // the row's partials, contiguous
+    double bs = 0.0, gx = 0.0;
+    for (int g = lane; g < np; g += 32) bs += bp[pr + g];
+    if (x0)
+        for (int g = lane; g < np; g += 32) gx += gp[pr + g];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        bs += __shfl_xor_sync(0xffffffffu, bs, o);
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+    }
+    if (lane) return;
+    const double bi = fma(-4.0 * 3.14159265358979323846, phi[i], bs);
+    if (b) b[i] = bi;
+    if (x0) r0[i] = bi - gx;
+}
+
+__global__ void __launch_bounds__(32 * SD_WARPS)
+    k_rhs_finish(int N, int np, const double* __restrict__ bp, const double* __restrict__ phi,
+                 double* __restrict__ b, const double* __restrict__ x0, const double* __restrict__ gp,
+                 double* __restrict__ r0) {
+    const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
+    if (i >= N) return;
+    rhs_finish_row(i, i, np, bp, phi, b, x0, gp, r0);
+}
+
+__global__ void __launch_bounds__(32 * SD_WARPS)
+    k_rhs_finish_batch(int N, const int* __restrict__ vblk, const BlockInfo* __restrict__ blk,
+                       const double* __restrict__ bp, const double* __restrict__ phi, double* __restrict__ b) {
+    const int i = blockIdx.x * SD_WARPS + (threadIdx.x >> 5);
+    if (i >= N) return;
+    const BlockInfo B = blk[vblk[i]];
+    rhs_finish_row(i, i - B.vbase, B.npatch, bp + B.ppbase, phi, b, nullptr, nullptr, nullptr);
 }
 
 template <bool MIRROR>
@@ -1014,13 +1114,19 @@ void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cu
     const int N = (int)T.N, M = (int)T.M;
     if (!r0 || c.batch) x0 = nullptr;
     prepare_assemble_g(c);
-    KLAUNCH(), k_patch_records<<<(M + 127) / 128, 128, 0, s>>>(M, x, phi, T.tri, T.patch_tri, T.patch_slot, c.prec);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c.prof) {
         e0 = c.take_event();
         e1 = c.take_event();
         cudaEventRecord(e0, s);
     }
+    // records (and, without the wall image, the singular pairs)
+    if (c.prm.mirror)
+        KLAUNCH(), k_patch_records<true><<<(M + 127) / 128, 128, 0, s>>>(M, x, phi, T.tri, T.patch_tri,
+                                                                          T.patch_slot, c.prec);
+    else
+        KLAUNCH(), k_patch_records<false><<<(4 * M + 127) / 128, 128, 0, s>>>(M, x, phi, T.tri, T.patch_tri,
+                                                                               T.patch_slot, c.prec);
     constexpr size_t sm = patch_smem<PATCH_ROWS>();
     if (c.prm.mirror)
         KLAUNCH(), k_assemble_patch<true, PATCH_ROWS, 3><<<T.nwork, PATCH_ROWS, sm, s>>>(
@@ -1036,16 +1142,14 @@ void launch_assemble_g(Ctx& c, const double* x, const double* phi, double* b, cu
             KLAUNCH(), k_singular_diag_batch_g<true><<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.bp, x, T.tri, T.csr_off,
                                                                         T.csr_idx, phi, c.G, b);
         else
-            KLAUNCH(), k_singular_diag_batch_g<false><<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.bp, x, T.tri, T.csr_off,
-                                                                         T.csr_idx, phi, c.G, b);
+            KLAUNCH(), k_rhs_finish_batch<<<nbs, nt, 0, s>>>(N, c.vblk, c.blk, c.bp, phi, b);
     } else if (c.prm.mirror) {
         KLAUNCH(), k_singular_diag<true, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
                                                                   T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
     } else {
-        KLAUNCH(), k_singular_diag<false, true><<<nbs, nt, 0, s>>>(N, T.npatch, nullptr, c.bp, x, T.tri, T.csr_off,
-                                                                   T.csr_idx, phi, c.G, nullptr, b, x0, c.gp, r0);
+        KLAUNCH(), k_rhs_finish<<<nbs, nt, 0, s>>>(N, T.npatch, c.bp, phi, b, x0, c.gp, r0);
     }
-    if (c.prof) {  // the profile's assembly time: tiles (with the shared columns' sums), singular pairs, 4 pi rule
+    if (c.prof) {  // the profile's assembly time: records, tiles (with the shared columns' sums), singular pairs, 4 pi rule
         cudaEventRecord(e1, s);
         c.ev_asm.emplace_back(e0, e1);
     }

@@ -655,6 +655,13 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         const PatchInfo& P = h.pinfo[(size_t)p];
         for (int r0 = P.vbase; r0 < P.vbase + P.n; r0 += PATCH_ROWS) work.push_back(make_int2(p, r0));
     }
+    // tiles with more rows first, patch order kept among equals: the CTAs that start last are the
+    // short ones, which shortens the kernel's tail (the results do not depend on the order)
+    auto tile_rows = [&](const int2& w) {
+        const PatchInfo& P = h.pinfo[(size_t)w.x];
+        return std::min(PATCH_ROWS, P.vbase + P.n - w.y);
+    };
+    std::stable_sort(work.begin(), work.end(), [&](const int2& a, const int2& b) { return tile_rows(a) > tile_rows(b); });
     t.nwork = (int)work.size();
     if (t.npatch > 0 &&
         ((rc = upload(c, &t.pinfo, h.pinfo)) || (rc = upload(c, &t.patch_tri, h.patch_tri)) ||

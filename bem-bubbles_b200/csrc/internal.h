@@ -50,10 +50,10 @@ constexpr int ASM_TC = 40;
 constexpr int REC = 28;
 // Triangle patches of the G-only assembly (the step path): every triangle belongs to exactly one
 // patch of at most PT_MAX triangles touching at most PCOLS vertices (the patch's columns); a patch
-// record of PREC doubles per triangle (272 bytes, a multiple of 16 for the bulk copy).
+// record of PREC doubles per triangle (288 bytes, a multiple of 16 for the bulk copy).
 constexpr int PT_MAX = 32;
 constexpr int PCOLS = 32;
-constexpr int PREC = 34;
+constexpr int PREC = 36;
 constexpr int PATCH_ROWS = 256;  // rows per CTA of the patch tiles
 constexpr int RF_WORDS = 96;     // ints of Ctx::rf_bar (the refinement round kernel's barrier and error words)
 // A patch: its triangles [t0, t0 + nt) of Topology::patch_tri, and the sub-system (block) it lies in:

@@ -532,7 +532,7 @@ def run_ours(args):
                                "refreshes": int(st1.precond_refresh - st0.precond_refresh)},
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(prof.kernel_launches),
-        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble_patch + k_halo_reduce + k_singular_diag (G-only assembly: regular pairs by triangle patch, shared columns summed, then singular pairs and the 4 pi rule); traffic: the tile kernel", "achieved": achieved,
+        "roofline": {"bound": "fp64-fma", "kernel": "k_patch_records + k_assemble_patch + k_rhs_finish (G-only assembly: records with the singular pairs, triangle-patch tiles with the shared columns summed, row partials of b with the 4 pi term); traffic: the tile kernel", "achieved": achieved,
                      "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
                      "peak_source": "measured live: FP64 FMA-loop kernel (bem_measure_fma_peaks)",
                      "flops_per_launch": flops, "avg_launch_ms": avg_asm_ms,
@@ -750,7 +750,7 @@ def run_sweep(args):
         "e2e": {"value": e2e_value, "unit": "bubble-steps/s", "h2d_bytes_per_step": 40 * N,
                 "d2h_bytes_per_step": 40 * N},
         "gpu_launches": launches,
-        "roofline": {"bound": "fp64-fma", "kernel": "k_assemble_patch + k_halo_reduce + k_singular_diag_batch_g (G-only assembly of every bubble)",
+        "roofline": {"bound": "fp64-fma", "kernel": "k_patch_records + k_assemble_patch + k_rhs_finish_batch (G-only assembly of every bubble)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "flops_per_launch": flops, "avg_launch_ms": avg_asm_ms,
                      "peak_source": "measured live: FP64 FMA-loop kernel (bem_measure_fma_peaks)"},
