@@ -697,7 +697,7 @@ static int alloc_mesh(Ctx& c, int64_t N, int64_t M, const HostTopo& h) {
         (rc = dalloc(c, &c.bp, nrow_part)) || (!c.batch && (rc = dalloc(c, &c.gp, nrow_part))) || (rc = dalloc(c, &c.vol, (size_t)h.nparts + 1)) ||
         (rc = dalloc(c, &c.vol_part, (size_t)h.nparts * 64)) || (rc = dalloc(c, &c.vol_cnt, (size_t)h.nparts)) ||
         (rc = dalloc(c, &c.part, (size_t)ncs * n)) || (rc = dalloc(c, &c.cnt, (n + 255) / 256 + 1)) ||
-        (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) ||
+        (rc = dalloc(c, &c.red, (size_t)(c.gmres_m + 8) * VBLK + 4096)) || (rc = dalloc(c, &c.piv, n)) || (rc = dalloc(c, &c.lu_perm, n)) ||
         (rc = dalloc(c, &c.hcol, (size_t)2 * (c.gmres_m + 2) + 8)) || (rc = dalloc(c, &c.pbicg, pbicg_words(N))) ||
         (!c.batch && (rc = dalloc(c, &c.lu_aux, lu_panel_words()))) ||
         (!c.batch && (rc = dalloc(c, &c.psih, (size_t)PRED_DEPTH * 4 * n))) ||

@@ -82,6 +82,7 @@ struct Ctx {
     // LU
     double* LU = nullptr;  // N*N
     int* piv = nullptr;    // N
+    int* lu_perm = nullptr;  // N: the factorisation's composed row permutation (row i of P A is row lu_perm[i])
     double* lu_aux = nullptr;  // row-distributed panels: candidates, diagonal rows, barrier and error words
     bool lu_rows_ok = true;    // the row-distributed panel is usable (cleared after a failed launch or wait)
     // mixed: approximate inverse (FP32), Krylov basis

@@ -48,7 +48,7 @@ __global__ void k_gj_swap(int n, int k0, int nb, const int* __restrict__ piv, fl
         float* col = A + (size_t)j * n + k0;
         for (int t = 0; t < nb; ++t) {
             const int p = piv[t];
-            if (p != t) {
+            if (p != t && p > t && p < n - k0) {  // a partner outside the panel's rows only after an expired wait
                 const float v = col[t];
                 col[t] = col[p];
                 col[p] = v;
@@ -58,7 +58,7 @@ __global__ void k_gj_swap(int n, int k0, int nb, const int* __restrict__ piv, fl
     if (j == 0)
         for (int t = 0; t < nb; ++t) {
             const int p = piv[t];
-            if (p != t) {
+            if (p != t && p > t && p < n - k0) {
                 const int v = perm[k0 + t];
                 perm[k0 + t] = perm[k0 + p];
                 perm[k0 + p] = v;

@@ -201,7 +201,12 @@ struct PanelTarget {
 };
 int lu_panel_rows(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* tgt = nullptr);
 int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* tgt = nullptr);
-void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s);  // the panel's interchanges, other columns
+// the panel's interchanges on the other columns of c.LU and on c.lu_perm; built: the (cluster) panel
+// kernel composed them already
+void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s, bool built);
+void lu_perm_init(Ctx& c, cudaStream_t s);  // c.lu_perm = identity, before the first panel
+// lu_update.cu: A22 -= L21 U12 after the panel [k0, k0 + nb) of the column-major n x n A (FP64 tensor cores)
+int lu_update(Ctx& c, int n, int k0, int nb, double* A, cudaStream_t s);
 size_t lu_panel_words();   // doubles of Ctx::lu_aux
 int* lu_panel_err(Ctx& c); // device error word of the row-distributed panels
 

@@ -522,79 +522,53 @@ __global__ void k_lu_laswp(int n, int k0, int nb, double* __restrict__ A, const 
 }
 
 // U12 = L11^-1 A12: one warp per column right of the panel, two panel rows per lane.
-__global__ void k_lu_trsm(int n, int k0, int nb, double* __restrict__ A) {
+__global__ void __launch_bounds__(256) k_lu_trsm(int n, int k0, int nb, double* __restrict__ A) {
     __shared__ double L[LU_NB][LU_NB + 1];
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        int r = e % nb, c = e / nb;
-        L[r][c] = A[(size_t)(k0 + c) * n + k0 + r];
+    {
+        // L11, all 16 loads of the thread in flight together
+        double v[LU_NB * LU_NB / 256];
+#pragma unroll
+        for (int u = 0; u < LU_NB * LU_NB / 256; ++u) {
+            const int e = threadIdx.x + 256 * u, r = e % LU_NB, c = e / LU_NB;
+            v[u] = (r < nb && c < nb) ? A[(size_t)(k0 + c) * n + k0 + r] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < LU_NB * LU_NB / 256; ++u) {
+            const int e = threadIdx.x + 256 * u;
+            L[e % LU_NB][e / LU_NB] = v[u];
+        }
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int col = k0 + nb + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (col >= n) return;
-    double* a = A + (size_t)col * n + k0;
-    double v0 = (lane < nb) ? a[lane] : 0.0, v1 = (lane + 32 < nb) ? a[lane + 32] : 0.0;
-    for (int k = 0; k < nb; ++k) {
-        double xk = (k < 32) ? __shfl_sync(0xffffffffu, v0, k) : __shfl_sync(0xffffffffu, v1, k - 32);
-        if (lane > k && lane < nb) v0 -= L[lane][k] * xk;
-        if (lane + 32 > k && lane + 32 < nb) v1 -= L[lane + 32][k] * xk;
-    }
-    if (lane < nb) a[lane] = v0;
-    if (lane + 32 < nb) a[lane + 32] = v1;
-}
-
-// A22 -= L21 * U12 with 64x64 output tiles, K = nb <= 64 in chunks of 32, FP64 FMA (SIMT).
-__global__ void __launch_bounds__(256) k_lu_gemm(int n, int k0, int nb, double* __restrict__ A) {
-    __shared__ double sa[32][64 + 1];  // [k][row]
-    __shared__ double sb[32][64 + 1];  // [k][col]
-    const int r0 = k0 + nb + blockIdx.x * 64, c0 = k0 + nb + blockIdx.y * 64;
-    const int tid = threadIdx.x;
-    const int tr = (tid % 16) * 4, tc = (tid / 16) * 4;
-    double acc[4][4] = {};
-    for (int kc = 0; kc < nb; kc += 32) {
-        const int kn = min(32, nb - kc);
-        __syncthreads();
-        for (int e = tid; e < kn * 64; e += 256) {
-            int k = e / 64, r = e % 64;
-            int gr = r0 + r;
-            sa[k][r] = (gr < n) ? A[(size_t)(k0 + kc + k) * n + gr] : 0.0;
-            int gc = c0 + r;
-            sb[k][r] = (gc < n) ? A[(size_t)gc * n + k0 + kc + k] : 0.0;
+    // each warp takes columns right of the panel, strided over the grid
+    for (int col = k0 + nb + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); col < n;
+         col += gridDim.x * (blockDim.x >> 5)) {
+        double* a = A + (size_t)col * n + k0;
+        double v0 = (lane < nb) ? a[lane] : 0.0, v1 = (lane + 32 < nb) ? a[lane + 32] : 0.0;
+        for (int k = 0; k < nb; ++k) {
+            double xk = (k < 32) ? __shfl_sync(0xffffffffu, v0, k) : __shfl_sync(0xffffffffu, v1, k - 32);
+            if (lane > k && lane < nb) v0 -= L[lane][k] * xk;
+            if (lane + 32 > k && lane + 32 < nb) v1 -= L[lane + 32][k] * xk;
         }
-        __syncthreads();
-        for (int k = 0; k < kn; ++k) {
-            double a[4], b[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[q] = sa[k][tr + q];
-                b[q] = sb[k][tc + q];
-            }
-#pragma unroll
-            for (int x = 0; x < 4; ++x)
-#pragma unroll
-                for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-        }
-    }
-#pragma unroll
-    for (int y = 0; y < 4; ++y) {
-        int gc = c0 + tc + y;
-        if (gc >= n) continue;
-#pragma unroll
-        for (int x = 0; x < 4; ++x) {
-            int gr = r0 + tr + x;
-            if (gr < n) A[(size_t)gc * n + gr] -= acc[x][y];
-        }
+        if (lane < nb) a[lane] = v0;
+        if (lane + 32 < nb) a[lane + 32] = v1;
     }
 }
 
 // Triangular solves of the factored system (x = P b, L y = x with unit L, U x = y) in blocks of TS_B
 // columns, with the operations of the column-oriented substitution in the same order per element:
 // each row subtracts the contributions of the columns in increasing order going forward and in
-// decreasing order going back.  A small kernel solves the block's diagonal part; a row-parallel
-// kernel subtracts the block's columns from the other rows.
+// decreasing order going back.  One launch per block: every CTA loads the block's diagonal part into
+// shared memory and solves it with one warp (two rows per lane, the solved entry broadcast by a
+// shuffle), CTA 0 writes the block's solution, and every CTA subtracts the block's columns from its
+// rows outside the block.  The block's right-hand side is read, never written, in its own launch.
+// Going back, each entry is multiplied by the reciprocal of its diagonal entry (formed before the
+// sweep) instead of divided by it.
 constexpr int TS_B = 64;
+constexpr int TS_LD = TS_B + 1;
 
-// y = P b: the recorded interchanges in order (one CTA, the vector in shared memory)
+// y = P b: the recorded interchanges in order (one CTA, the vector in shared memory); the fallback
+// when the factorisation kept no composed row permutation
 __global__ void __launch_bounds__(1024) k_lu_permute(int n, const int* __restrict__ piv, const double* __restrict__ b,
                                                      double* __restrict__ y) {
     extern __shared__ double sy[];
@@ -613,98 +587,176 @@ __global__ void __launch_bounds__(1024) k_lu_permute(int n, const int* __restric
     for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = sy[i];
 }
 
-// forward: unit lower L on rows [k0, k1)
-__global__ void k_trsv_fwd_diag(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
-    __shared__ double s[TS_B];
-    const int t = threadIdx.x, i = k0 + t;
-    if (i < k1) s[t] = y[i];
-    for (int j = k0; j < k1; ++j) {
-        __syncthreads();
-        const double xj = s[j - k0];
-        if (i > j && i < k1) s[t] -= A[(size_t)j * n + i] * xj;
+// y = P b with the composed row permutation (row i of P A is row perm[i] of A)
+__global__ void k_lu_gather(int n, const int* __restrict__ perm, const double* __restrict__ b, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = b[perm[i]];
+}
+
+// forward: unit lower L on rows [k0, k0 + kb); y the running right-hand side (rows >= k0 + kb are
+// updated), z the solution
+__global__ void __launch_bounds__(256) k_trsv_fwd(int n, int k0, int kb, const double* __restrict__ A,
+                                                  double* __restrict__ y, double* __restrict__ z) {
+    __shared__ double sL[TS_B * TS_LD];  // [c][r]
+    __shared__ double sx[TS_B];
+    const int tid = threadIdx.x, k1 = k0 + kb;
+    {
+        // the diagonal block, all 16 loads of the thread in flight together
+        double v[TS_B * TS_B / 256];
+#pragma unroll
+        for (int u = 0; u < TS_B * TS_B / 256; ++u) {
+            const int e = tid + 256 * u, c = e / TS_B, r = e - c * TS_B;
+            v[u] = (c < kb && r < kb) ? A[(size_t)(k0 + c) * n + k0 + r] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < TS_B * TS_B / 256; ++u) {
+            const int e = tid + 256 * u, c = e / TS_B;
+            sL[c * TS_LD + (e - c * TS_B)] = v[u];
+        }
     }
     __syncthreads();
-    if (i < k1) y[i] = s[t];
-}
-__global__ void k_trsv_fwd_rest(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
-    __shared__ double xs[TS_B];
-    if (threadIdx.x < k1 - k0) xs[threadIdx.x] = y[k0 + threadIdx.x];
+    if (tid < 32) {
+        const int lane = tid;
+        double v0 = lane < kb ? y[k0 + lane] : 0.0, v1 = lane + 32 < kb ? y[k0 + 32 + lane] : 0.0;
+        for (int j = 0; j < kb; ++j) {
+            const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+            if (lane > j && lane < kb) v0 -= sL[j * TS_LD + lane] * xj;
+            if (lane + 32 > j && lane + 32 < kb) v1 -= sL[j * TS_LD + lane + 32] * xj;
+        }
+        if (lane < kb) sx[lane] = v0;
+        if (lane + 32 < kb) sx[lane + 32] = v1;
+    }
     __syncthreads();
-    const int i = k1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && tid < kb) z[k0 + tid] = sx[tid];
+    const int i = k1 + blockIdx.x * 256 + tid;
     if (i >= n) return;
     double acc = y[i];
-    for (int j = k0; j < k1; ++j) acc -= A[(size_t)j * n + i] * xs[j - k0];
-    y[i] = acc;
-}
-// backward: upper U on rows [k0, k1), columns from the last
-__global__ void k_trsv_bwd_diag(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
-    __shared__ double s[TS_B];
-    const int t = threadIdx.x, i = k0 + t;
-    if (i < k1) s[t] = y[i];
-    for (int j = k1 - 1; j >= k0; --j) {
-        __syncthreads();
-        if (i == j) s[t] /= A[(size_t)j * n + j];
-        __syncthreads();
-        const double xj = s[j - k0];
-        if (i < j) s[t] -= A[(size_t)j * n + i] * xj;
+    for (int j0 = 0; j0 < kb; j0 += 16) {  // 16 loads in flight, the subtractions in column order
+        double lv[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) lv[u] = j0 + u < kb ? A[(size_t)(k0 + j0 + u) * n + i] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+            if (j0 + u < kb) acc -= lv[u] * sx[j0 + u];
     }
-    __syncthreads();
-    if (i < k1) y[i] = s[t];
-}
-__global__ void k_trsv_bwd_rest(int n, int k0, int k1, const double* __restrict__ A, double* __restrict__ y) {
-    __shared__ double xs[TS_B];
-    if (threadIdx.x < k1 - k0) xs[threadIdx.x] = y[k0 + threadIdx.x];
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= k0) return;
-    double acc = y[i];
-    for (int j = k1 - 1; j >= k0; --j) acc -= A[(size_t)j * n + i] * xs[j - k0];
     y[i] = acc;
 }
 
-static void lu_substitute_blocked(Ctx& c, const double* b, double* x, cudaStream_t s) {
-    const int n = (int)c.topo.N;
-    static std::atomic<uint64_t> attr{0};
-    once_per_device(attr, [] {
-        return cudaFuncSetAttribute(k_lu_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
-               cudaSuccess;
-    });
-    KLAUNCH(), k_lu_permute<<<1, 1024, sizeof(double) * (size_t)n, s>>>(n, c.piv, b, x);
-    for (int k0 = 0; k0 < n; k0 += TS_B) {
-        const int k1 = std::min(n, k0 + TS_B);
-        KLAUNCH(), k_trsv_fwd_diag<<<1, TS_B, 0, s>>>(n, k0, k1, c.LU, x);
-        if (k1 < n) KLAUNCH(), k_trsv_fwd_rest<<<(n - k1 + 255) / 256, 256, 0, s>>>(n, k0, k1, c.LU, x);
+// backward: upper U on rows [k0, k0 + kb), columns from the last; y the running right-hand side
+// (rows < k0 are updated), x the solution
+__global__ void __launch_bounds__(256) k_trsv_bwd(int n, int k0, int kb, const double* __restrict__ A,
+                                                  double* __restrict__ y, double* __restrict__ x) {
+    __shared__ double sU[TS_B * TS_LD];  // [c][r]
+    __shared__ double sx[TS_B];
+    const int tid = threadIdx.x;
+    {
+        // the diagonal block, all 16 loads of the thread in flight together
+        double v[TS_B * TS_B / 256];
+#pragma unroll
+        for (int u = 0; u < TS_B * TS_B / 256; ++u) {
+            const int e = tid + 256 * u, c = e / TS_B, r = e - c * TS_B;
+            v[u] = (c < kb && r < kb) ? A[(size_t)(k0 + c) * n + k0 + r] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < TS_B * TS_B / 256; ++u) {
+            const int e = tid + 256 * u, c = e / TS_B;
+            sU[c * TS_LD + (e - c * TS_B)] = v[u];
+        }
     }
+    __syncthreads();
+    if (tid < 32) {
+        const int lane = tid;
+        double v0 = lane < kb ? y[k0 + lane] : 0.0, v1 = lane + 32 < kb ? y[k0 + 32 + lane] : 0.0;
+        // reciprocals of the lane's two diagonal entries, formed before the sweep: a division per
+        // step would sit on the sweep's critical path
+        const double q0 = lane < kb ? 1.0 / sU[lane * TS_LD + lane] : 0.0;
+        const double q1 = lane + 32 < kb ? 1.0 / sU[(lane + 32) * TS_LD + lane + 32] : 0.0;
+        for (int j = kb - 1; j >= 0; --j) {
+            if (lane == j) v0 *= q0;
+            if (lane + 32 == j) v1 *= q1;
+            const double xj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+            if (lane < j) v0 -= sU[j * TS_LD + lane] * xj;
+            if (lane + 32 < j) v1 -= sU[j * TS_LD + lane + 32] * xj;
+        }
+        if (lane < kb) sx[lane] = v0;
+        if (lane + 32 < kb) sx[lane + 32] = v1;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0 && tid < kb) x[k0 + tid] = sx[tid];
+    const int i = blockIdx.x * 256 + tid;
+    if (i >= k0) return;
+    double acc = y[i];
+    for (int j1 = kb - 1; j1 >= 0; j1 -= 16) {  // 16 loads in flight, the subtractions from the last column
+        double lv[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) lv[u] = j1 - u >= 0 ? A[(size_t)(k0 + j1 - u) * n + i] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+            if (j1 - u >= 0) acc -= lv[u] * sx[j1 - u];
+    }
+    y[i] = acc;
+}
+
+// x = U^-1 L^-1 P b with c.LU, c.piv (and c.lu_perm when the factorisation composed it); c.yv and
+// c.zv are the work vectors
+static void lu_substitute_blocked(Ctx& c, const double* b, double* x, cudaStream_t s, bool composed) {
+    const int n = (int)c.topo.N;
+    double* y = c.yv;
+    double* z = c.zv;
+    if (composed) {
+        KLAUNCH(), k_lu_gather<<<(n + 255) / 256, 256, 0, s>>>(n, c.lu_perm, b, y);
+    } else {
+        static std::atomic<uint64_t> attr{0};
+        once_per_device(attr, [] {
+            return cudaFuncSetAttribute(k_lu_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+                   cudaSuccess;
+        });
+        KLAUNCH(), k_lu_permute<<<1, 1024, sizeof(double) * (size_t)n, s>>>(n, c.piv, b, y);
+    }
+    for (int k0 = 0; k0 < n; k0 += TS_B) {
+        const int kb = std::min(TS_B, n - k0);
+        const int rows = n - k0 - kb;
+        KLAUNCH(), k_trsv_fwd<<<std::max(1, (rows + 255) / 256), 256, 0, s>>>(n, k0, kb, c.LU, y, z);
+    }
+    // z is now L^-1 P b; the backward sweep runs on it in place of y
     for (int k1 = n; k1 > 0; k1 -= TS_B) {
         const int k0 = std::max(0, k1 - TS_B);
-        KLAUNCH(), k_trsv_bwd_diag<<<1, TS_B, 0, s>>>(n, k0, k1, c.LU, x);
-        if (k0 > 0) KLAUNCH(), k_trsv_bwd_rest<<<(k0 + 255) / 256, 256, 0, s>>>(n, k0, k1, c.LU, x);
+        KLAUNCH(), k_trsv_bwd<<<std::max(1, (k0 + 255) / 256), 256, 0, s>>>(n, k0, k1 - k0, c.LU, z, x);
     }
 }
 
 // Blocked right-looking factorisation of c.LU (a copy of A).  rows: each panel on one thread-block
 // cluster when its rows fit in the cluster's shared memory, else spread over the SMs with grid
-// barriers (lu_panel.cu); otherwise the single-CTA panel.
-static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
+// barriers (lu_panel.cu); the interchanges are composed per panel and applied to the other columns
+// and to the row permutation c.lu_perm (*composed = true).  Otherwise the single-CTA panel and one
+// interchange at a time.  The trailing update runs on the FP64 tensor cores (lu_update.cu).
+static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows, bool* composed) {
     const int n = (int)c.topo.N;
+    *composed = false;
     BEM_CUDA(c, cudaMemcpyAsync(c.LU, A, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemsetAsync(c.flag, 0, sizeof(int), s));
-    if (rows) BEM_CUDA(c, cudaMemsetAsync(lu_panel_err(c), 0, sizeof(int), s));
+    if (rows) {
+        BEM_CUDA(c, cudaMemsetAsync(lu_panel_err(c), 0, sizeof(int), s));
+        lu_perm_init(c, s);
+    }
     for (int k0 = 0; k0 < n; k0 += LU_NB) {
         const int nb = std::min(LU_NB, n - k0);
-        if (!rows || (lu_panel_cluster(c, k0, nb, s) != BEM_OK && lu_panel_rows(c, k0, nb, s) != BEM_OK)) {
-            if (rows) return BEM_ERR_CUDA;
+        bool built = false;
+        if (rows) {
+            if (lu_panel_cluster(c, k0, nb, s) == BEM_OK)
+                built = true;
+            else if (lu_panel_rows(c, k0, nb, s) != BEM_OK)
+                return BEM_ERR_CUDA;
+            lu_panel_swap_rest(c, k0, nb, s, built);
+        } else {
             KLAUNCH(), k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
-        }
-        if (c.lu_aux)
-            lu_panel_swap_rest(c, k0, nb, s);
-        else
             KLAUNCH(), k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
+        }
         const int rest = n - k0 - nb;
         if (rest > 0) {
-            KLAUNCH(), k_lu_trsm<<<(rest + 7) / 8, 256, 0, s>>>(n, k0, nb, c.LU);
-            dim3 g((rest + 63) / 64, (rest + 63) / 64);
-            KLAUNCH(), k_lu_gemm<<<g, 256, 0, s>>>(n, k0, nb, c.LU);
+            KLAUNCH(), k_lu_trsm<<<std::min((rest + 7) / 8, 2 * 148), 256, 0, s>>>(n, k0, nb, c.LU);
+            int rc = lu_update(c, n, k0, nb, c.LU, s);
+            if (rc) return rc;
         }
     }
     if (rows) {
@@ -715,24 +767,27 @@ static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows) {
             c.stats.wait_expired++;
             return BEM_ERR_CUDA;
         }
+        *composed = true;
     }
     return BEM_OK;
 }
 
 int lu_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_t s) {
     const int n = (int)c.topo.N;
-    if ((size_t)n * sizeof(double) > 200 * 1024)
-        return c.fail(BEM_ERR_ARG, "LU solver: N too large for the in-shared-memory interchange of b (N <= 25600)");
     int rc = BEM_ERR_CUDA;
+    bool composed = false;
     if (c.lu_rows_ok && c.lu_aux) {
-        rc = lu_factor(c, A, s, true);
+        rc = lu_factor(c, A, s, true, &composed);
         if (rc == BEM_ERR_CUDA) c.lu_rows_ok = false;  // factor again with the single-CTA panel
     }
     if (rc != BEM_OK) {
-        rc = lu_factor(c, A, s, false);
+        if ((size_t)n * sizeof(double) > 200 * 1024)
+            return c.fail(BEM_ERR_ARG,
+                          "LU solver: N too large for the in-shared-memory interchange of b (N <= 25600)");
+        rc = lu_factor(c, A, s, false, &composed);
         if (rc) return rc;
     }
-    lu_substitute_blocked(c, b, x, s);
+    lu_substitute_blocked(c, b, x, s, composed);
     int sing = 0;
     BEM_CUDA(c, cudaMemcpyAsync(&sing, c.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     BEM_CUDA(c, cudaStreamSynchronize(s));

@@ -209,48 +209,154 @@ __global__ void __launch_bounds__(LP_THREADS) k_lu_panel_rows(LPArgs a) {
     }
 }
 
-// The same panel step on one thread-block cluster (up to 16 CTAs): the candidates, the diagonal row
-// and the pivot row are read from the other CTAs' shared memory (distributed shared memory), and a
-// column step is one hardware cluster barrier.  For panels whose rows fit in the cluster's shared
-// memory (about 6000 rows of a 64-column panel).
-constexpr int LC_MAX = 16;
+// One warp: tab_r[q] is a touched row, tab_s[q] the source row whose entries now sit there (both in
+// shared memory, at most 2 nb entries).  Each transposition swaps the sources of its two rows; the
+// lanes look a row up in parallel.  pairs[0] = m, then m (destination, source) pairs.
+// A transposition whose partner row is not in (k0 + j, n) is skipped: it can only come from a panel
+// whose bounded wait expired (an error the host reports), and skipping keeps every access in bounds.
+__device__ void lu_build_pairs_warp(int n, int k0, int nb, const int* pj, int* tab_r, int* tab_s, int* pairs) {
+    const int lane = threadIdx.x & 31;
+    int cnt = 0;
+    auto slot = [&](int r) {
+        int found = -1;
+        for (int q0 = 0; q0 < cnt && found < 0; q0 += 32) {
+            const unsigned m = __ballot_sync(0xffffffffu, q0 + lane < cnt && tab_r[q0 + lane] == r);
+            if (m) found = q0 + __ffs(m) - 1;
+        }
+        if (found >= 0) return found;
+        if (lane == 0) {
+            tab_r[cnt] = r;
+            tab_s[cnt] = r;
+        }
+        __syncwarp();
+        return cnt++;
+    };
+    for (int j = 0; j < nb; ++j) {
+        const int rj = k0 + j, p = pj[j];
+        if (p <= rj || p >= n) continue;
+        const int a = slot(rj), b = slot(p);
+        if (lane == 0) {
+            const int t = tab_s[a];
+            tab_s[a] = tab_s[b];
+            tab_s[b] = t;
+        }
+        __syncwarp();
+    }
+    int m = 0;
+    for (int q0 = 0; q0 < cnt; q0 += 32) {
+        const int q = q0 + lane;
+        const bool moved = q < cnt && tab_s[q] != tab_r[q];
+        const unsigned bal = __ballot_sync(0xffffffffu, moved);
+        if (moved) {
+            const int k = m + __popc(bal & ((1u << lane) - 1u));
+            pairs[1 + 2 * k] = tab_r[q];
+            pairs[2 + 2 * k] = tab_s[q];
+        }
+        m += __popc(bal);
+    }
+    if (lane == 0) pairs[0] = m;
+}
 
+// The same panel on one thread-block cluster (up to 16 CTAs), for panels whose rows fit in the
+// cluster's shared memory (about 5700 rows of a 64-column panel).  The candidates travel by push: a
+// column step is
+//   * each thread already holds the largest |entry| of the column among its rows (found while it
+//     eliminated the previous column); one block barrier reduces them to the CTA's candidate;
+//   * warp 0 writes the candidate (|entry|, row, the whole row) into slot `me` of every CTA's inbox,
+//     the CTA owning the diagonal row writes that row into every CTA's diagonal box, and one lane per
+//     destination arrives on the destination's mbarrier (release at cluster scope);
+//   * warp 0 waits (bounded) on its own mbarrier for all CTAs' arrivals (acquire), then picks the
+//     pivot from its inbox: largest |entry|, then smallest row (the single-CTA kernel's rule); the
+//     pivot row and the diagonal row are already in its own shared memory; one block barrier;
+//   * each thread takes its rows: the diagonal row's owner writes the pivot row there, the pivot
+//     row's owner writes the old diagonal row in its place, and every row below the diagonal is
+//     eliminated, l = a_ij * (1 / a_jj), a_ik -= l * a_jk, the next column first, so its candidate
+//     comes with it.
+// Inbox, diagonal box and mbarrier are double-buffered by column parity: a CTA writes column j + 2's
+// candidates only after all CTAs' arrivals for column j + 1, which each CTA makes after it has read
+// its column-j inbox.  A wait that runs out sets *err; the CTA still makes every write and arrival of
+// the remaining columns (so no other CTA waits on it), and the caller factors again without the
+// cluster.
+constexpr int LC_MAX = 16;
+constexpr size_t LC_SMEM = 220 * 1024;  // dynamic shared memory of one cluster CTA, at most
+
+__device__ __forceinline__ uint32_t lp_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Bounded wait for phase `parity` of the local mbarrier `bar` (acquire at cluster scope): polls with
+// the non-blocking test_wait and gives up after `limit` SM clock cycles.
+__device__ __forceinline__ bool lp_bar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > limit) return false;
+    }
+}
+
+// pairs (may be null): CTA 0 also composes the panel's interchanges (lu_build_pairs_warp) at the end.
 __global__ void __launch_bounds__(LP_THREADS) k_lu_panel_cluster(int n, int k0, int nb, int rows_per, double* A,
-                                                                 int* piv, int* sing) {
+                                                                 int* piv, int* sing, int* pairs, int* err,
+                                                                 long long wait_limit) {
     namespace cgx = cooperative_groups;
     cgx::cluster_group cl = cgx::this_cluster();
-    extern __shared__ double sp[];  // [rows_per][ld], then candidates [2][2 + nb] and diagonal rows [2][nb]
-    __shared__ double s_v[LP_THREADS / 32];
-    __shared__ int s_i[LP_THREADS / 32];
-    __shared__ double s_prow[LP_NBMAX];
-    __shared__ int s_pw[2];
+    // dynamic: [rows_per][ld] rows, inbox [2][C][2 + nb], diagonal box [2][nb]
+    extern __shared__ double sp[];
+    constexpr int NW = LP_THREADS / 32;
+    __shared__ double s_v[NW];
+    __shared__ int s_i[NW];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ double s_rcp;
+    __shared__ int s_p, s_w, s_piv[LP_NBMAX], tab_r[2 * LP_NBMAX], tab_s[2 * LP_NBMAX];
     const int C = (int)cl.num_blocks(), me = (int)cl.block_rank(), tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
     const int ld = nb + 1, stride = 2 + nb;
-    double* cand = sp + (size_t)rows_per * ld;
-    double* diag = cand + 2 * stride;
+    double* inbox = sp + (size_t)rows_per * ld;
+    double* dbox = inbox + 2 * C * stride;
     const int r0 = k0 + me * rows_per, r1 = min(n, r0 + rows_per);
     const int nr = max(0, r1 - r0);
-    for (int e = tid; e < nr * nb; e += LP_THREADS) {
-        const int c = e / nr, rr = e - c * nr;
-        sp[rr * ld + c] = A[(size_t)(k0 + c) * n + r0 + rr];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(lp_smem(&s_bar[0])), "r"(C));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(lp_smem(&s_bar[1])), "r"(C));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
+    // the CTA's rows of the panel, 16 loads in flight per thread
+    for (int e0 = tid; e0 < nr * nb; e0 += 16 * LP_THREADS) {
+        double v[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int e = e0 + u * LP_THREADS, c = e / max(nr, 1), rr = e - c * nr;
+            v[u] = e < nr * nb ? A[(size_t)(k0 + c) * n + r0 + rr] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int e = e0 + u * LP_THREADS, c = e / max(nr, 1), rr = e - c * nr;
+            if (e < nr * nb) sp[rr * ld + c] = v[u];
+        }
+    }
+    cl.sync();  // every CTA's mbarriers initialised before anyone arrives on them
+    // this thread's candidate for column 0 (every row of the panel is at or below the diagonal)
+    double best = -1.0;
+    int bi = n;
+    for (int rr = tid; rr < nr; rr += LP_THREADS) {
+        const double v = fabs(sp[rr * ld]);
+        if (v > best) {  // rows increase with rr: the first row wins ties
+            best = v;
+            bi = r0 + rr;
+        }
+    }
+    bool ok = true;
     for (int j = 0; j < nb; ++j) {
         const int rowj = k0 + j, par = j & 1;
         const int owner_j = (rowj - k0) / rows_per;
-        double* mycand = cand + par * stride;
-        double* mydiag = diag + par * nb;
-        double best = -1.0;
-        int bi = n;
-        for (int rr = tid; rr < nr; rr += LP_THREADS) {
-            const int i = r0 + rr;
-            if (i < rowj) continue;
-            const double v = fabs(sp[rr * ld + j]);
-            if (v > best || (v == best && i < bi)) {
-                best = v;
-                bi = i;
-            }
-        }
+        double* box = inbox + (size_t)par * C * stride;  // [C][2 + nb]
+        double* dg = dbox + (size_t)par * nb;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const double ov = __shfl_xor_sync(0xffffffffu, best, o);
@@ -260,154 +366,219 @@ __global__ void __launch_bounds__(LP_THREADS) k_lu_panel_cluster(int n, int k0, 
                 bi = oi;
             }
         }
-        if ((tid & 31) == 0) {
-            s_v[tid >> 5] = best;
-            s_i[tid >> 5] = bi;
+        if (lane == 0) {
+            s_v[wid] = best;
+            s_i[wid] = bi;
         }
         __syncthreads();
-        if (tid < 32) {
-            best = tid < LP_THREADS / 32 ? s_v[tid] : -2.0;
-            bi = tid < LP_THREADS / 32 ? s_i[tid] : n;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (ov > best || (ov == best && oi < bi)) {
-                    best = ov;
-                    bi = oi;
-                }
-            }
-            if (tid == 0) {
-                s_v[0] = best;
-                s_i[0] = bi;
-            }
-        }
-        __syncthreads();
-        best = s_v[0];
-        bi = s_i[0];
-        if (tid == 0) {
-            mycand[0] = best;
-            mycand[1] = (double)bi;
-        }
-        if (bi < n)
-            for (int c = tid; c < nb; c += LP_THREADS) mycand[2 + c] = sp[(bi - r0) * ld + c];
-        if (me == owner_j)
-            for (int c = tid; c < nb; c += LP_THREADS) mydiag[c] = sp[(rowj - r0) * ld + c];
-        cl.sync();
-        // the pivot: the CTAs' candidates, largest |entry| then smallest row (the same in every CTA)
-        if (tid < 32) {
-            double v = -1.0;
-            int i = n, w = -1;
-            if (tid < C) {
-                const double* rc = cl.map_shared_rank(mycand, tid);
-                const int ri = (int)rc[1];
-                if (ri < n) {
-                    v = rc[0];
-                    i = ri;
-                    w = tid;
-                }
-            }
+        if (wid == 0) {
+            double v = lane < NW ? s_v[lane] : -2.0;
+            int i = lane < NW ? s_i[lane] : n;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 const double ov = __shfl_xor_sync(0xffffffffu, v, o);
                 const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-                const int ow = __shfl_xor_sync(0xffffffffu, w, o);
-                if (oi < n && (ov > v || (ov == v && oi < i))) {
+                if (ov > v || (ov == v && oi < i)) {
                     v = ov;
                     i = oi;
-                    w = ow;
                 }
             }
-            if (tid == 0) {
-                s_pw[0] = i;
-                s_pw[1] = w;
+            // the candidate row (two columns per lane) and, from the owner, the diagonal row
+            const bool h0 = lane < nb, h1 = lane + 32 < nb;
+            const double* crow = sp + (size_t)(i < n ? i - r0 : 0) * ld;
+            const double c0v = (i < n && h0) ? crow[lane] : 0.0, c1v = (i < n && h1) ? crow[lane + 32] : 0.0;
+            const bool own = me == owner_j;
+            const double* drow_l = sp + (size_t)(own ? rowj - r0 : 0) * ld;
+            const double d0v = (own && h0) ? drow_l[lane] : 0.0, d1v = (own && h1) ? drow_l[lane + 32] : 0.0;
+            double* slot = box + (size_t)me * stride;
+            for (int t = 0; t < C; ++t) {
+                double* rs = cl.map_shared_rank(slot, t);
+                if (lane == 0) {
+                    rs[0] = v;
+                    rs[1] = (double)i;
+                }
+                if (h0) rs[2 + lane] = c0v;
+                if (h1) rs[2 + lane + 32] = c1v;
+                if (own) {
+                    double* rd = cl.map_shared_rank(dg, t);
+                    if (h0) rd[lane] = d0v;
+                    if (h1) rd[lane + 32] = d1v;
+                }
+            }
+            asm volatile("fence.acq_rel.cluster;" ::: "memory");
+            __syncwarp();
+            if (lane < C) {
+                uint32_t rb;
+                asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(lp_smem(&s_bar[par])), "r"(lane));
+                asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(rb) : "memory");
+            }
+            // all CTAs' candidates for this column, then the pivot (the same in every CTA)
+            if (!lp_bar_wait(lp_smem(&s_bar[par]), (uint32_t)((j >> 1) & 1), wait_limit)) ok = false;
+            double bv = -1.0;
+            int bi2 = n, bw = -1;
+            if (lane < C) {
+                const double* rc = box + (size_t)lane * stride;
+                const int ri = (int)rc[1];
+                if (ri < n) {
+                    bv = rc[0];
+                    bi2 = ri;
+                    bw = lane;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi2, o);
+                const int ow = __shfl_xor_sync(0xffffffffu, bw, o);
+                if (oi < n && (ov > bv || (ov == bv && oi < bi2))) {
+                    bv = ov;
+                    bi2 = oi;
+                    bw = ow;
+                }
+            }
+            if (bw >= 0 && (bi2 < rowj || bi2 >= n)) {  // not a row of this column's candidates: only
+                bw = -1;                                // after an expired wait (garbage), never used
+                bi2 = n;
+                ok = false;
+            }
+            if (lane == 0) {
+                const int p = (bi2 < n) ? bi2 : rowj;  // no candidate: keep the diagonal row
+                const double d = (bw >= 0) ? box[(size_t)bw * stride + 2 + j] : dg[j];
+                s_p = p;
+                s_w = bw;
+                s_rcp = d != 0.0 ? 1.0 / d : 0.0;
+                s_piv[j] = p;
+                if (me == 0) {
+                    piv[rowj] = p;
+                    if (d == 0.0) *sing = 1;
+                }
             }
         }
         __syncthreads();
-        int p = s_pw[0];
-        const int w = s_pw[1];
-        if (p >= n) p = rowj;
-        const double* prow = (w >= 0) ? cl.map_shared_rank(mycand, w) + 2 : cl.map_shared_rank(mydiag, owner_j);
-        const double* drow = cl.map_shared_rank(mydiag, owner_j);
-        for (int c = tid; c < nb; c += LP_THREADS) s_prow[c] = prow[c];
-        if (me == 0 && tid == 0) piv[rowj] = p;
-        __syncthreads();
-        if (p != rowj) {
-            if (rowj >= r0 && rowj < r1)
-                for (int c = tid; c < nb; c += LP_THREADS) sp[(rowj - r0) * ld + c] = s_prow[c];
-            if (p >= r0 && p < r1)
-                for (int c = tid; c < nb; c += LP_THREADS) sp[(p - r0) * ld + c] = drow[c];
-        }
-        __syncthreads();
-        const double d = s_prow[j];
-        if (d == 0.0 && me == 0 && tid == 0) *sing = 1;
+        const int p = s_p, w = s_w;
+        const double rcp = s_rcp;
+        const double* prow = (w >= 0) ? box + (size_t)w * stride + 2 : dg;
+        best = -1.0;
+        bi = n;
         for (int rr = tid; rr < nr; rr += LP_THREADS) {
             const int i = r0 + rr;
-            if (i <= rowj) continue;
-            double l = sp[rr * ld + j];
-            if (d != 0.0) {
-                l /= d;
-                sp[rr * ld + j] = l;
+            if (i < rowj) continue;
+            double* row = sp + rr * ld;
+            // copies and updates go eight columns at a time, their loads before their stores (one
+            // column at a time each load waits behind the previous store: the warp of the one lane
+            // doing it then holds up the column step)
+            if (i == rowj) {  // the pivot row moves here, multipliers of the earlier columns included
+                if (p != rowj)
+                    for (int cb = 0; cb < nb; cb += 8) {
+                        double pv[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                            if (cb + u < nb) pv[u] = prow[cb + u];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                            if (cb + u < nb) row[cb + u] = pv[u];
+                    }
+                continue;
             }
-            for (int c = j + 1; c < nb; ++c) sp[rr * ld + c] -= l * s_prow[c];
+            // the old diagonal row moves to the pivot's place: its earlier multipliers are copied and
+            // the rest is eliminated straight from the diagonal box
+            const double* src = row;
+            if (i == p) {
+                src = dg;
+                for (int cb = 0; cb < j; cb += 8) {
+                    double dv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (cb + u < j) dv[u] = dg[cb + u];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (cb + u < j) row[cb + u] = dv[u];
+                }
+            }
+            double l = src[j];
+            if (rcp != 0.0) l *= rcp;
+            row[j] = l;
+            if (j + 1 < nb) {
+                const double v1 = src[j + 1] - l * prow[j + 1];
+                row[j + 1] = v1;
+                const double a1 = fabs(v1);
+                if (a1 > best) {  // rows increase with rr
+                    best = a1;
+                    bi = i;
+                }
+            }
+            for (int cb = j + 2; cb < nb; cb += 8) {
+                double rv[8], pv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (cb + u < nb) {
+                        rv[u] = src[cb + u];
+                        pv[u] = prow[cb + u];
+                    }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (cb + u < nb) row[cb + u] = rv[u] - l * pv[u];
+            }
         }
-        __syncthreads();
     }
-    cl.sync();  // no CTA leaves while another may still read its shared memory
+    if (!ok && lane == 0) atomicExch(err, 1);
+    cl.sync();  // no CTA leaves while another may still write into its shared memory
     for (int e = tid; e < nr * nb; e += LP_THREADS) {
         const int c = e / nr, rr = e - c * nr;
         A[(size_t)(k0 + c) * n + r0 + rr] = sp[rr * ld + c];
     }
+    if (pairs && me == 0 && wid == 0) lu_build_pairs_warp(n, k0, nb, s_piv, tab_r, tab_s, pairs);
 }
 
 // Row interchanges of a panel applied to the columns outside it, as one permutation: the panel's
-// transpositions (j, piv[j]) composed into (destination, source) row pairs by one thread, then one
+// transpositions (k0 + j, pj[j]) composed into (destination, source) row pairs by one warp, then one
 // warp per column loads every source before storing any destination.
-__global__ void k_lu_perm_build(int k0, int nb, const int* __restrict__ piv, int* __restrict__ pairs) {
-    // rows touched: the panel rows and their partners; content[r] = source row now at r
-    int rows[2 * LP_NBMAX], src[2 * LP_NBMAX], cnt = 0;
-    auto slot = [&](int r) {
-        for (int q = 0; q < cnt; ++q)
-            if (rows[q] == r) return q;
-        rows[cnt] = r;
-        src[cnt] = r;
-        return cnt++;
-    };
-    for (int j = k0; j < k0 + nb; ++j) {
-        const int p = piv[j];
-        if (p == j) continue;
-        const int a = slot(j), b = slot(p);
-        const int t = src[a];
-        src[a] = src[b];
-        src[b] = t;
-    }
-    int m = 0;
-    for (int q = 0; q < cnt; ++q)
-        if (src[q] != rows[q]) {
-            pairs[1 + 2 * m] = rows[q];
-            pairs[2 + 2 * m] = src[q];
-            ++m;
-        }
-    pairs[0] = m;
+__global__ void __launch_bounds__(32) k_lu_perm_build(int n, int k0, int nb, const int* __restrict__ piv,
+                                                      int* __restrict__ pairs) {
+    __shared__ int tab_r[2 * LP_NBMAX], tab_s[2 * LP_NBMAX];
+    lu_build_pairs_warp(n, k0, nb, piv + k0, tab_r, tab_s, pairs);
 }
 
-__global__ void k_lu_perm_apply(int n, int k0, int nb, const int* __restrict__ pairs, double* __restrict__ A) {
+// perm (may be null): the composed row permutation so far, permuted like one more column
+__global__ void k_lu_perm_apply(int n, int k0, int nb, const int* __restrict__ pairs, double* __restrict__ A,
+                                int* __restrict__ perm) {
     const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (col >= n || (col >= k0 && col < k0 + nb)) return;
     const int m = pairs[0];
-    double* a = A + (size_t)col * n;
-    double v[(2 * LP_NBMAX + 31) / 32];
+    constexpr int NQ = (2 * LP_NBMAX + 31) / 32;
+    if (col == n && perm) {
+        int v[NQ];
 #pragma unroll
-    for (int q = 0; q < (2 * LP_NBMAX + 31) / 32; ++q) {
+        for (int q = 0; q < NQ; ++q) {
+            const int k = lane + 32 * q;
+            if (k < m) v[q] = perm[pairs[2 + 2 * k]];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int k = lane + 32 * q;
+            if (k < m) perm[pairs[1 + 2 * k]] = v[q];
+        }
+        return;
+    }
+    if (col >= n || (col >= k0 && col < k0 + nb)) return;
+    double* a = A + (size_t)col * n;
+    double v[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
         const int k = lane + 32 * q;
         if (k < m) v[q] = a[pairs[2 + 2 * k]];
     }
     __syncwarp();
 #pragma unroll
-    for (int q = 0; q < (2 * LP_NBMAX + 31) / 32; ++q) {
+    for (int q = 0; q < NQ; ++q) {
         const int k = lane + 32 * q;
         if (k < m) a[pairs[1 + 2 * k]] = v[q];
     }
+}
+
+__global__ void k_iota_int(int n, int* __restrict__ v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
 }
 
 }  // namespace
@@ -422,10 +593,16 @@ static int* lp_pairs(Ctx& c) { return reinterpret_cast<int*>(lp_bar(c) + 4); }
 
 size_t lu_panel_words() { return (size_t)2 * LP_GMAX * (2 + LP_NBMAX) + (size_t)2 * LP_NBMAX + 8 + 2 * LP_NBMAX + 8; }
 
-void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s) {
+// built: the panel kernel already composed the pairs (the cluster panel of c.LU does)
+void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s, bool built) {
     const int n = (int)c.topo.N;
-    KLAUNCH(), k_lu_perm_build<<<1, 1, 0, s>>>(k0, nb, c.piv, lp_pairs(c));
-    KLAUNCH(), k_lu_perm_apply<<<(n + 7) / 8, 256, 0, s>>>(n, k0, nb, lp_pairs(c), c.LU);
+    if (!built) KLAUNCH(), k_lu_perm_build<<<1, 32, 0, s>>>(n, k0, nb, c.piv, lp_pairs(c));
+    KLAUNCH(), k_lu_perm_apply<<<(n + 1 + 7) / 8, 256, 0, s>>>(n, k0, nb, lp_pairs(c), c.LU, c.lu_perm);
+}
+
+void lu_perm_init(Ctx& c, cudaStream_t s) {
+    const int n = (int)c.topo.N;
+    KLAUNCH(), k_iota_int<<<(n + 255) / 256, 256, 0, s>>>(n, c.lu_perm);
 }
 
 // The panel on one thread-block cluster when its rows fit; BEM_ERR_CUDA when they do not or the
@@ -439,11 +616,11 @@ int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* 
     if (nb > LP_NBMAX) return BEM_ERR_CUDA;
     const int C = std::max(1, std::min(LC_MAX, (P + 127) / 128));
     const int rows_per = (P + C - 1) / C;
-    const size_t smem = sizeof(double) * ((size_t)rows_per * (nb + 1) + 2 * (2 + nb) + 2 * nb);
-    if (smem > 200 * 1024) return BEM_ERR_CUDA;
+    const size_t smem = sizeof(double) * ((size_t)rows_per * (nb + 1) + (size_t)2 * C * (2 + nb) + 2 * nb);
+    if (smem > LC_SMEM) return BEM_ERR_CUDA;
     static std::atomic<uint64_t> attr{0};
     if (!once_per_device(attr, [] {
-            return cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) ==
+            return cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LC_SMEM) ==
                        cudaSuccess &&
                    cudaFuncSetAttribute(k_lu_panel_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
                        cudaSuccess;
@@ -469,7 +646,9 @@ int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* 
         return BEM_ERR_CUDA;
     }
     KLAUNCH();
-    if (cudaLaunchKernelEx(&cfg, k_lu_panel_cluster, n, k0, nb, rows_per, A, piv, sing) != cudaSuccess) {
+    int* pairs = tgt ? nullptr : lp_pairs(c);  // the interchange pairs of c.LU's panel, composed in the kernel
+    if (cudaLaunchKernelEx(&cfg, k_lu_panel_cluster, n, k0, nb, rows_per, A, piv, sing, pairs, lu_panel_err(c),
+                           (long long)c.wait_limit) != cudaSuccess) {
         cudaGetLastError();
         return BEM_ERR_CUDA;
     }

@@ -11,6 +11,8 @@
 #include <cstdlib>
 #include <string>
 
+#include <sys/resource.h>
+
 #include "Bem/Mesh/MeshIO.hpp"
 #include "Bem/Simulation/ColocSim.hpp"
 
@@ -18,6 +20,20 @@ using namespace Bem;
 using clk = std::chrono::steady_clock;
 
 static double ms(clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); }
+
+// the process's CPU time (user + system, ms) and context switches (voluntary, involuntary) so far: a
+// slow iteration whose wall time the CPU time does not explain, with involuntary switches, was
+// waiting for the host's cores, not for its own work
+struct Usage {
+    double cpu_ms;
+    long vcsw, ivcsw;
+};
+static Usage usage() {
+    rusage r{};
+    getrusage(RUSAGE_SELF, &r);
+    const double cpu = (r.ru_utime.tv_sec + r.ru_stime.tv_sec) * 1e3 + (r.ru_utime.tv_usec + r.ru_stime.tv_usec) * 1e-3;
+    return {cpu, r.ru_nvcsw, r.ru_nivcsw};
+}
 
 static real K, Omega, Pa;
 static real waveform(vec3 x, real t) { return Pa * std::sin(K * x.x - Omega * t); }
@@ -49,6 +65,7 @@ int main(int argc, char* argv[]) {
 #endif
     double te = 0, tr = 0, ts = 0;
     for (int i = 0; i < iters; ++i) {
+        const Usage u0 = usage();
         const auto t0 = clk::now();
         sim.export_mesh("cycle-mesh.ply");
         const auto t1 = clk::now();
@@ -60,8 +77,10 @@ int main(int argc, char* argv[]) {
 #endif
         for (int j = 0; j < 4; ++j) sim.evolve_system(0.02);
         const auto t3 = clk::now();
-        std::printf("iteration %d verts %zu export_ms %.2f remesh_ms %.2f steps_ms %.2f", i, sim.mesh.verts.size(),
-                    ms(t0, t1), ms(t1, t2), ms(t2, t3));
+        const Usage u1 = usage();
+        std::printf("iteration %d verts %zu export_ms %.2f remesh_ms %.2f steps_ms %.2f cpu_ms %.2f vcsw %ld ivcsw %ld", i,
+                    sim.mesh.verts.size(), ms(t0, t1), ms(t1, t2), ms(t2, t3), u1.cpu_ms - u0.cpu_ms, u1.vcsw - u0.vcsw,
+                    u1.ivcsw - u0.ivcsw);
 #ifdef CYCLE_DROPIN
         // the GPU solver's work in this iteration's four steps
         sim.gpu_stats(&s1[0], &s1[1], &s1[2], &s1[3], &s1[4], &s1[5]);
