@@ -29,6 +29,7 @@ FLAG_STEP_ASSEMBLE_H = 4
 FLAG_REFINE_PERSISTENT = 8
 FLAG_INVERSE_GJ = 16
 FLAG_INVERSE_NS = 32
+FLAG_NO_IR_GATE = 64
 
 _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)
@@ -47,7 +48,8 @@ class Stats(C.Structure):
     _fields_ = [("solves", C.c_int64), ("last_iters", C.c_int32), ("precond_refresh", C.c_int32),
                 ("last_rel_residual", C.c_double), ("ns_steps", C.c_int64), ("gmres_fallbacks", C.c_int64),
                 ("fp64_fallbacks", C.c_int64),
-                ("total_iters", C.c_int64), ("wait_expired", C.c_int64), ("gj_inverses", C.c_int64)]
+                ("total_iters", C.c_int64), ("wait_expired", C.c_int64), ("gj_inverses", C.c_int64),
+                ("ir_rounds", C.c_int64)]
 
 
 class Profile(C.Structure):

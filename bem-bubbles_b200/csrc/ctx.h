@@ -114,6 +114,9 @@ struct Ctx {
     // behind that round, see SolveTail); solve_stage: the stage of the current solve, or -1
     int ir_steps_stage[4] = {3, 3, 3, 3};
     bool stage_round0[4] = {false, false, false, false};
+    // gated extra steps of the next first round per RK4 stage: 2 after a solve that used an extra step
+    // or a second round, else 1
+    int ir_extra_stage[4] = {2, 2, 2, 2};
     int solve_stage = -1;
     // Stage predictor of the mixed solve (single systems): the solutions of the RK4 stages of the last
     // PRED_DEPTH steps and the stage times, a ring over steps (pred_head: the slot the current step

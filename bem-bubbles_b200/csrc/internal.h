@@ -55,7 +55,8 @@ constexpr int PT_MAX = 32;
 constexpr int PCOLS = 32;
 constexpr int PREC = 36;
 constexpr int PATCH_ROWS = 256;  // rows per CTA of the patch tiles
-constexpr int RF_WORDS = 96;     // ints of Ctx::rf_bar (the refinement round kernel's barrier and error words)
+constexpr int RF_WORDS = 128;    // ints of Ctx::rf_bar (the refinement round kernel's barrier and error words,
+                                 // the refinement's convergence gate)
 // A patch: its triangles [t0, t0 + nt) of Topology::patch_tri, and the sub-system (block) it lies in:
 // first vertex vbase and n vertices, G block at element mbase, row partials at pbase + row*np + lp
 // (np patches in the block, lp this patch's index among them).

@@ -1288,8 +1288,21 @@ static int fp64_fallback(Ctx& c, const double* A, const double* b, double* x, cu
 // the round with separate launches.
 // Ctx::rf_bar: the arrival count at word 0, the generation at RF_GEN and the error word at RF_ERR,
 // each on its own 128-byte line (RF_WORDS ints)
-constexpr int RF_GEN = 32, RF_ERR = 64;
-static_assert(RF_ERR < RF_WORDS, "Ctx::rf_bar holds RF_WORDS ints");
+constexpr int RF_GEN = 32, RF_ERR = 64, RF_GATE = 96;
+static_assert(RF_GATE < RF_WORDS, "Ctx::rf_bar holds RF_WORDS ints");
+
+// The host's convergence rule of the refinement on the device: with the row-block partials of |b|^2
+// (pb) and of |r_k|^2 (prk) summed in the host's order, rel = sqrt(|r_k|^2 / |b|^2); the first k with
+// rel <= tol is stored in *gate (which starts at -1), and the gated GEMVs that follow then return at
+// once.  One thread: the same sums in the same order, so the device and the host decide alike.
+__global__ void k_ir_check(int nrb, const double* __restrict__ pb, const double* __restrict__ prk, double tol,
+                           int k, int* __restrict__ gate) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || *gate >= 0) return;
+    double bb = 0.0, a = 0.0;
+    for (int q = 0; q < nrb; ++q) bb += pb[q];
+    for (int q = 0; q < nrb; ++q) a += prk[q];
+    if (bb != 0.0 && sqrt(a / bb) <= tol) *gate = k;
+}
 constexpr unsigned RF_SLEEP_NS = 32;  // polling interval of the waiting CTAs
 constexpr int RF_CHUNK_MAX = 4096;    // columns of one tile's staged slice of the input vector
 struct RFArgs {
@@ -1392,8 +1405,19 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
         KLAUNCH(), k_rowblock_norm2x2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb, c.r, pr);
     else
         KLAUNCH(), k_rowblock_norm2<<<nrb, GV_ROWS, 0, s>>>(n, b, pb);
+    // The first round runs K steps and then up to IR_EXTRA more whose GEMVs are gated on the device:
+    // a check after each residual from the K-th on stores the step at which the host's convergence
+    // rule holds, and the gated GEMVs after it return at once.  A solve whose step count was guessed
+    // one or two short then still ends in one round, without a second read-back, a recomputed
+    // residual and a second enqueue of the solution's consumers.  A stage whose last solve needed
+    // none of them gets one (a skipped gated GEMV still costs its launch).
+    constexpr int IR_EXTRA = 2;
+    const size_t red_cap = (size_t)(c.gmres_m + 8) * VBLK + 4096;  // doubles of c.red
+    int* gate = (c.rf_bar && !(c.prm.flags & BEM_FLAG_NO_IR_GATE) && (size_t)(KMAX + IR_EXTRA + 2) * nrb <= red_cap)
+                    ? c.rf_bar + RF_GATE
+                    : nullptr;
     // the norms come back through pinned memory: a direct DMA the host sees as soon as it lands
-    const size_t nh = (size_t)(KMAX + 2) * nrb + 2;  // norms, then the round kernel's error word
+    const size_t nh = (size_t)(KMAX + IR_EXTRA + 2) * nrb + 4;  // norms, the round kernel's error word, the gate
     if (c.h_red_cap < nh) {
         cudaFreeHost(c.h_red);
         c.h_red = nullptr;
@@ -1410,16 +1434,21 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
     bool tail_valid = false;  // the tail was enqueued and x has not changed since
     double rho = 1.0, rel = 1.0, rel0 = -1.0;
     bool converged = false;
+    bool r_fresh = false;  // c.r is b - A x for the current x, its relative norm rel (a later round skips it)
     int rounds = 0;
-    int* herr = reinterpret_cast<int*>(host + (size_t)(KMAX + 2) * nrb);
+    int* herr = reinterpret_cast<int*>(host + (size_t)(KMAX + IR_EXTRA + 2) * nrb);
+    int* hgate = herr + 1;
     for (int round = 0; round < 4; ++round) {
         ++rounds;
+        ++c.stats.ir_rounds;
         tail_valid = false;  // a round changes x
-        const bool skip_first = round == 0 && r0_ready;  // the residual and its norms are there
+        const bool skip_first = (round == 0 && r0_ready) || (round > 0 && r_fresh);
         const bool want = c.refine_ok && (c.prm.flags & BEM_FLAG_REFINE_PERSISTENT);
         const bool persistent = want && refine_round_persistent(c, A, b, x, pr, K, skip_first, s) == BEM_OK;
+        const int E = (round == 0 && !persistent && gate) ? (st >= 0 ? c.ir_extra_stage[st] : IR_EXTRA) : 0;
         if (!persistent) {
             if (want) c.refine_ok = false;
+            if (E) BEM_CUDA(c, cudaMemsetAsync(gate, 0xff, sizeof(int), s));  // -1: not converged
             for (int k = 0; k < K; ++k) {
                 if (!(k == 0 && skip_first))
                     gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)k * nrb, nullptr,
@@ -1429,10 +1458,21 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
             }
             gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, nullptr, 0, c.r, pr + (size_t)K * nrb, nullptr, nullptr, b,
                            -1.0);
+            for (int e = 0; e < E; ++e) {
+                KLAUNCH(), k_ir_check<<<1, 32, 0, s>>>(nrb, pb, pr + (size_t)(K + e) * nrb, tol, K + e, gate);
+                gemv_t<float>(n, c.Xinv, c.r, x, s, c.part, c.cnt, gate, -1, nullptr, nullptr, nullptr, nullptr, x,
+                              1.0);
+                gemv_t<double>(n, A, x, c.r, s, c.part, c.cnt, gate, -1, c.r, pr + (size_t)(K + e + 1) * nrb,
+                               nullptr, nullptr, b, -1.0);
+            }
+            if (E) KLAUNCH(), k_ir_check<<<1, 32, 0, s>>>(nrb, pb, pr + (size_t)(K + E) * nrb, tol, K + E, gate);
         }
-        BEM_CUDA(c, cudaMemcpyAsync(host, c.red, sizeof(double) * (size_t)(K + 2) * nrb, cudaMemcpyDeviceToHost, s));
+        BEM_CUDA(c, cudaMemcpyAsync(host, c.red, sizeof(double) * (size_t)(K + E + 2) * nrb, cudaMemcpyDeviceToHost,
+                                    s));
         *herr = 0;
+        *hgate = -1;
         if (persistent) BEM_CUDA(c, cudaMemcpyAsync(herr, c.rf_bar + RF_ERR, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (E) BEM_CUDA(c, cudaMemcpyAsync(hgate, gate, sizeof(int), cudaMemcpyDeviceToHost, s));
         if (round == 0 && tail) {  // the solution's consumers, speculatively: x is final if this round converges
             if (!c.solve_ev) BEM_CUDA(c, cudaEventCreateWithFlags(&c.solve_ev, cudaEventDisableTiming));
             BEM_CUDA(c, cudaEventRecord(c.solve_ev, s));
@@ -1453,12 +1493,16 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
             c.stats.wait_expired++;
             c.refine_ok = false;
             r0_ready = false;
+            r_fresh = false;
             tail_valid = false;
             --round;
             --rounds;
             continue;
         }
-        c.stats.last_iters += K;
+        // the steps this round made: K, or fewer than K + E when the gate closed at an extra step
+        const int steps = (E && *hgate >= K) ? *hgate : K + E;
+        if (round == 0 && E && st >= 0) c.ir_extra_stage[st] = (*hgate == K) ? 1 : IR_EXTRA;
+        c.stats.last_iters += steps;
         double bb = 0.0;
         for (int q = 0; q < nrb; ++q) bb += host[(size_t)q];
         if (bb == 0.0) {
@@ -1468,17 +1512,19 @@ int mixed_solve(Ctx& c, const double* A, const double* b, double* x, cudaStream_
             converged = true;
             break;
         }
-        std::vector<double> rk((size_t)K + 1);
-        for (int k = 0; k <= K; ++k) {
+        std::vector<double> rk((size_t)steps + 1);
+        for (int k = 0; k <= steps; ++k) {
             double a = 0.0;
             for (int q = 0; q < nrb; ++q) a += host[(size_t)(1 + k) * nrb + q];
             rk[(size_t)k] = sqrt(a / bb);
         }
+        if (round > 0 && skip_first) rk[0] = rel;  // the residual was not recomputed: its norm is the last one
         if (rel0 < 0) rel0 = rk[0];
-        rel = rk[(size_t)K];
+        rel = rk[(size_t)steps];
+        r_fresh = true;
         // contraction per step, from the steps still well above the FP64 floor of the residual
         rho = 0.0;
-        for (int k = 0; k < K; ++k)
+        for (int k = 0; k < steps; ++k)
             if (rk[(size_t)k] > 1e3 * tol) rho = std::max(rho, rk[(size_t)k + 1] / rk[(size_t)k]);
         if (rel <= tol) {
             converged = true;

@@ -77,8 +77,8 @@ typedef struct {
 #define BEM_FLAG_STEP_ASSEMBLE_H 4
 /* bem_params.flags: run each round of BEM_SOLVER_MIXED's refinement steps as one cooperative kernel
  * with grid barriers instead of separate GEMV launches (the same tiles and summation order:
- * bit-identical results).  Measured slower than the separate launches on B200 (0.36 against
- * 0.27 ms per solve at N = 4002), so it is not the default. */
+ * bit-identical results, with BEM_FLAG_NO_IR_GATE).  Measured slower than the separate launches on
+ * B200 (0.36 against 0.27 ms per solve at N = 4002), so it is not the default. */
 #define BEM_FLAG_REFINE_PERSISTENT 8
 /* bem_params.flags: how BEM_SOLVER_MIXED builds its approximate inverse from scratch.  By default
  * (neither flag) large systems (N >= BEM_GJ_MIN_N) use blocked Gauss-Jordan elimination with row
@@ -87,6 +87,12 @@ typedef struct {
 #define BEM_FLAG_INVERSE_GJ 16
 #define BEM_FLAG_INVERSE_NS 32
 #define BEM_GJ_MIN_N 8192
+/* bem_params.flags: no gated extra steps in the first round of BEM_SOLVER_MIXED's refinement.  By
+ * default that round issues one or two steps beyond its estimate whose GEMVs a device-side check of
+ * the convergence rule skips once it holds, so a short estimate does not cost a second round (a
+ * read-back of the residual norms by the host and a new enqueue).  With the flag a round issues its
+ * estimate only, as the cooperative round kernel of BEM_FLAG_REFINE_PERSISTENT does. */
+#define BEM_FLAG_NO_IR_GATE 64
 
 /* Fill *p with the reference's defaults. */
 void bem_default_params(bem_params* p);
@@ -274,6 +280,8 @@ typedef struct {
                                  panel) that gave up; each sent the context to the multi-kernel form */
     int64_t gj_inverses;      /* approximate inverses of the mixed path built by the tensor-core
                                  Gauss-Jordan elimination (the rest by Newton-Schulz from scratch) */
+    int64_t ir_rounds;        /* rounds of refinement steps of the mixed path since creation (each ends
+                                 with one read-back of the residual norms by the host) */
 } bem_stats;
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 

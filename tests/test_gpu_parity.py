@@ -404,13 +404,14 @@ def test_exterior_potential_grid_matches_oracle():
 
 def test_refinement_round_kernel_equals_separate_launches():
     # the mixed solve's refinement round as one cooperative kernel and as separate GEMV launches: the
-    # same tiles, per-thread order and split sums, so whole RK4 trajectories agree bit for bit
+    # same tiles, per-thread order and split sums, so whole RK4 trajectories agree bit for bit (the
+    # separate launches without the gated extra steps, which the round kernel does not issue)
     from bem_b200 import _lib as L
     v, f = mesh.bubble(12, 1.0, (2.0, 0.0, 0.0))
     rng = np.random.default_rng(3)
     v = v * (1.0 + 0.01 * rng.standard_normal(len(v)))[:, None]
     out = []
-    for flags in (0, L.FLAG_REFINE_PERSISTENT):
+    for flags in (L.FLAG_NO_IR_GATE, L.FLAG_REFINE_PERSISTENT):
         sim = ColocSim(v, f, pressurefield=(-0.8, 2 * np.pi / 5, 0.0), solver="mixed", p_inf=1.0, epsilon=1.0,
                        gamma=1.4)
         sim._update(flags=flags)
@@ -421,3 +422,27 @@ def test_refinement_round_kernel_equals_separate_launches():
         out.append((x.tobytes(), p.tobytes(), s.tobytes(), t, sim.stats().total_iters))
         sim.close()
     assert out[0] == out[1]
+
+
+def test_mixed_solve_gated_extra_steps_end_in_one_round():
+    # the first round of each refinement appends gated steps (a device check applies the host's
+    # convergence rule and the GEMVs after it return at once): along a smooth trajectory nearly every
+    # solve ends in one round, every solve meets the refinement tolerance, and the trajectory equals
+    # the FP64 BiCGSTAB one
+    v, f = mesh.bubble(10, 1.0, (2.0, 0.0, 0.0))
+    phys = dict(p_inf=1.0, epsilon=1.0, sigma=0.0, gamma=1.4)
+    mix = ColocSim(v, f, solver="mixed", pressurefield=(-0.8, 2.0 * np.pi / 5.0, 0.0), **phys)
+    ref = ColocSim(v, f, solver="bicgstab", pressurefield=(-0.8, 2.0 * np.pi / 5.0, 0.0), **phys)
+    for sim in (mix, ref):
+        sim.set_phi(0.05 * np.cos(v[:, 2]))
+    s0 = mix.stats()
+    for _ in range(10):
+        mix.evolve_system_RK4(5e-3, fixdt=True)
+        ref.evolve_system_RK4(5e-3, fixdt=True)
+        assert mix.stats().last_rel_residual <= 1e-12
+    s1 = mix.stats()
+    solves = s1.solves - s0.solves
+    assert solves == 40
+    assert s1.ir_rounds - s0.ir_rounds <= solves + 4
+    assert rel(mix.get_psi(), ref.get_psi()) <= 1e-8
+    assert rel(mix.get_vertices(), ref.get_vertices()) <= 1e-10
