@@ -72,7 +72,7 @@ __global__ void k_velocity(int N, const int* __restrict__ off, const int* __rest
 // Part volumes (Mesh.cpp:206-218), sum over the part's triangles of (a x b).c / 6, in two levels
 // with a fixed shape: CTA (chunk, part) sums VOL_CHUNK consecutive triangles of the part's list by a
 // tree; the last CTA of the part (completion counter) adds the chunk sums in chunk order.
-constexpr int VOL_CHUNK = 1024, VOL_MAXCH = 64;
+constexpr int VOL_CHUNK = 256, VOL_MAXCH = 64;  // about one triangle per thread: the sum is latency-bound
 __global__ void __launch_bounds__(256) k_part_volume(const double* __restrict__ x, const int* __restrict__ off,
                                                      const int* __restrict__ tidx, const int* __restrict__ ptri,
                                                      double* __restrict__ part_sums, unsigned* __restrict__ cnt,
