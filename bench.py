@@ -405,6 +405,10 @@ def run_ours(args):
     v, f = workload()
     N, M = len(v), len(f)
     sim = ColocSim(v, f, pressurefield=FIELD, solver=args.solver, device=device, **PHYS)
+    if args.inverse != "auto":  # how the mixed solver builds its approximate inverse from scratch
+        from bem_b200 import _lib as L
+
+        sim._update(flags=L.FLAG_INVERSE_GJ if args.inverse == "gj" else L.FLAG_INVERSE_NS)
     sim.set_phi(0.0)
     ext = torch.cuda.ExternalStream(sim.stream_handle(), device=device)
 
@@ -515,7 +519,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (assembly, residual, state) + f32 (preconditioner)",
         "data": "synthetic", "solver": args.solver,
-        "config": headline_config(ws),
+        "config": dict(headline_config(ws), **({"inverse": args.inverse} if args.inverse != "auto" else {})),
         "fp64_gpu": fp64["bicgstab"],
         "fp64_lu_gpu": fp64["lu"],
         "speedup_vs_fp64_gpu": value / ws / fp64["bicgstab"]["steps_per_s"],
@@ -902,6 +906,9 @@ def main():
     ap.add_argument("--no-seq", action="store_true", help="sweep: skip the sequential baseline")
     ap.add_argument("--bubbles", type=int, default=256, help="sweep: number of bubbles")
     ap.add_argument("--dirs", type=int, default=32, help="adjoint: finite-difference directions")
+    ap.add_argument("--inverse", default="auto", choices=["auto", "gj", "ns"],
+                    help="headline, mixed solver: build the approximate inverse by Gauss-Jordan (gj) or "
+                         "Newton-Schulz (ns); auto: Gauss-Jordan from N = 8192")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
