@@ -187,7 +187,8 @@ int bem_pot_t_multi(bem_ctx* ctx, const double* verts, const double* grads, doub
  * *dt_out (may be NULL) receives the step taken.  BEM_ERR_NEGATIVE_X mirrors test_negative. */
 int bem_evolve_rk4(bem_ctx* ctx, double dp, int32_t fixdt, double* dt_out);
 int bem_evolve_euler(bem_ctx* ctx, double dp, int32_t fixdt, double* dt_out);
-/* `steps` RK4 steps with fixed dt without host synchronisation in between. */
+/* `steps` RK4 steps with fixed dt, without the x < 0 check and host synchronisation between steps (the
+ * iterative solvers still read their residual norms back: the mixed solver once per stage). */
 int bem_evolve_rk4_n(bem_ctx* ctx, double dt, int32_t steps);
 
 /* ---- Batches of independent bubbles (a radius x pressure sweep as in the reference's

@@ -94,3 +94,19 @@ def test_lu_cluster_panel_wait_expiry_falls_back():
     # later solves of the context keep the single-CTA panel
     x2 = sim.solve_system(A, b)
     assert np.array_equal(x, x2)
+
+
+def test_lu_panels_taller_than_a_cluster_use_the_grid_barrier_panel():
+    # N = 6762 (icosphere nu = 26): the first panels hold more rows than one thread-block cluster's
+    # shared memory, so they run on co-resident CTAs with grid barriers (their interchanges composed by
+    # a separate kernel), and the later, shorter panels on the cluster
+    sim = _sim(26)
+    n = sim.N
+    assert n == 6762
+    rng = np.random.default_rng(17)
+    A = np.asfortranarray(rng.standard_normal((n, n)))
+    b = rng.standard_normal(n)
+    x = sim.solve_system(A, b)
+    ref = np.linalg.solve(A, b)
+    assert np.max(np.abs(x - ref)) / np.max(np.abs(ref)) <= TOL
+    assert sim.stats().wait_expired == 0
