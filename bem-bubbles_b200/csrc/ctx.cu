@@ -799,6 +799,9 @@ int bem_destroy(bem_ctx* c) {
     cudaFreeHost(c->h_stage);
     if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     if (c->solve_ev) cudaEventDestroy(c->solve_ev);
+    for (cudaEvent_t e : c->lu_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->lu_side) cudaStreamDestroy(c->lu_side);
     cudaFree(c->sc);
     cudaFree(c->flag);
     cudaFreeHost(c->h_sc);

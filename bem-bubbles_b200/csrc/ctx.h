@@ -83,6 +83,9 @@ struct Ctx {
     double* LU = nullptr;  // N*N
     int* piv = nullptr;    // N
     int* lu_perm = nullptr;  // N: the factorisation's composed row permutation (row i of P A is row lu_perm[i])
+    // the LU's look-ahead: the next panel on a high-priority stream beside the current trailing update
+    cudaStream_t lu_side = nullptr;
+    cudaEvent_t lu_ev[2] = {nullptr, nullptr};
     double* lu_aux = nullptr;  // row-distributed panels: candidates, diagonal rows, barrier and error words
     bool lu_rows_ok = true;    // the row-distributed panel is usable (cleared after a failed launch or wait)
     // mixed: approximate inverse (FP32), Krylov basis

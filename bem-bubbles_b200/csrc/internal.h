@@ -207,7 +207,7 @@ int lu_panel_cluster(Ctx& c, int k0, int nb, cudaStream_t s, const PanelTarget* 
 void lu_panel_swap_rest(Ctx& c, int k0, int nb, cudaStream_t s, bool built);
 void lu_perm_init(Ctx& c, cudaStream_t s);  // c.lu_perm = identity, before the first panel
 // lu_update.cu: A22 -= L21 U12 after the panel [k0, k0 + nb) of the column-major n x n A (FP64 tensor cores)
-int lu_update(Ctx& c, int n, int k0, int nb, double* A, cudaStream_t s);
+int lu_update(Ctx& c, int n, int k0, int nb, double* A, cudaStream_t s, int cb = -1, int ce = -1, bool narrow = false);
 size_t lu_panel_words();   // doubles of Ctx::lu_aux
 int* lu_panel_err(Ctx& c); // device error word of the row-distributed panels
 

@@ -735,15 +735,30 @@ static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows, bool* c
     *composed = false;
     BEM_CUDA(c, cudaMemcpyAsync(c.LU, A, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToDevice, s));
     BEM_CUDA(c, cudaMemsetAsync(c.flag, 0, sizeof(int), s));
+    // Look-ahead (row-distributed panels only): after panel k's interchanges and U12, the trailing
+    // update first takes the next panel's columns; that panel is then factored on a high-priority side
+    // stream while the rest of the update runs (in 64-row tiles, so that a panel CTA fits beside an
+    // update CTA on an SM).  The side stream joins the main one before the next interchanges.
+    cudaStream_t s2 = nullptr;
     if (rows) {
         BEM_CUDA(c, cudaMemsetAsync(lu_panel_err(c), 0, sizeof(int), s));
         lu_perm_init(c, s);
+        if (!c.lu_side) {
+            int lo = 0, hi = 0;
+            BEM_CUDA(c, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            BEM_CUDA(c, cudaStreamCreateWithPriority(&c.lu_side, cudaStreamNonBlocking, hi));
+            for (cudaEvent_t& e : c.lu_ev) BEM_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        s2 = c.lu_side;
     }
+    bool ahead = false, ahead_built = false;  // the current panel was factored by the look-ahead
     for (int k0 = 0; k0 < n; k0 += LU_NB) {
         const int nb = std::min(LU_NB, n - k0);
         bool built = false;
         if (rows) {
-            if (lu_panel_cluster(c, k0, nb, s) == BEM_OK)
+            if (ahead)
+                built = ahead_built;
+            else if (lu_panel_cluster(c, k0, nb, s) == BEM_OK)
                 built = true;
             else if (lu_panel_rows(c, k0, nb, s) != BEM_OK)
                 return BEM_ERR_CUDA;
@@ -752,12 +767,30 @@ static int lu_factor(Ctx& c, const double* A, cudaStream_t s, bool rows, bool* c
             KLAUNCH(), k_lu_panel<<<1, 1024, 0, s>>>(n, k0, nb, c.LU, c.piv, c.flag);
             KLAUNCH(), k_lu_laswp<<<(n + 255) / 256, 256, 0, s>>>(n, k0, nb, c.LU, c.piv);
         }
+        ahead = false;
         const int rest = n - k0 - nb;
-        if (rest > 0) {
-            KLAUNCH(), k_lu_trsm<<<std::min((rest + 7) / 8, 2 * 148), 256, 0, s>>>(n, k0, nb, c.LU);
-            int rc = lu_update(c, n, k0, nb, c.LU, s);
-            if (rc) return rc;
+        if (rest <= 0) continue;
+        KLAUNCH(), k_lu_trsm<<<std::min((rest + 7) / 8, 2 * 148), 256, 0, s>>>(n, k0, nb, c.LU);
+        int rc;
+        if (!rows) {
+            if ((rc = lu_update(c, n, k0, nb, c.LU, s))) return rc;
+            continue;
         }
+        const int k1 = k0 + nb, nb2 = std::min(LU_NB, n - k1);
+        if ((rc = lu_update(c, n, k0, nb, c.LU, s, k1, k1 + nb2))) return rc;  // the next panel's columns
+        BEM_CUDA(c, cudaEventRecord(c.lu_ev[0], s));
+        BEM_CUDA(c, cudaStreamWaitEvent(s2, c.lu_ev[0], 0));
+        if (lu_panel_cluster(c, k1, nb2, s2) == BEM_OK)
+            ahead_built = true;
+        else if (lu_panel_rows(c, k1, nb2, s2) == BEM_OK)
+            ahead_built = false;
+        else
+            return BEM_ERR_CUDA;  // nothing was enqueued on the side stream after the wait
+        BEM_CUDA(c, cudaEventRecord(c.lu_ev[1], s2));
+        rc = lu_update(c, n, k0, nb, c.LU, s, k1 + nb2, n, true);  // the rest, beside the next panel
+        BEM_CUDA(c, cudaStreamWaitEvent(s, c.lu_ev[1], 0));
+        if (rc) return rc;
+        ahead = true;
     }
     if (rows) {
         int err = 0;

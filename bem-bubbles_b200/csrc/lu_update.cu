@@ -16,10 +16,13 @@ namespace bemb {
 
 namespace {
 
-constexpr int UB_M = 128, UB_N = 64, UB_K = 64;  // tile of A22, widest panel
-constexpr int UA_LD = UB_M + 4;                  // sA[k][row]: +4 doubles, conflict-free fragment reads
-constexpr int UBB_LD = UB_K + 4;                 // sB[col][k]
-constexpr size_t UPD_SMEM = sizeof(double) * ((size_t)UB_K * UA_LD + (size_t)UB_N * UBB_LD);
+constexpr int UB_N = 64, UB_K = 64;  // tile columns of A22, widest panel
+constexpr int UBB_LD = UB_K + 4;     // sB[col][k]: +4 doubles, conflict-free fragment reads
+// tile rows UB_M = 32 * WM (WM warps along the rows, two along the columns); sA[k][row] with +4 doubles
+template <int WM>
+constexpr size_t upd_smem() {
+    return sizeof(double) * ((size_t)UB_K * (32 * WM + 4) + (size_t)UB_N * UBB_LD);
+}
 
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -27,16 +30,20 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(256, 2) k_lu_update(int n, int k0, int nb, double* __restrict__ A) {
+// columns [cb, ce) of A22 (cb >= k0 + nb)
+template <int WM>
+__global__ void __launch_bounds__(64 * WM, 2) k_lu_update(int n, int k0, int nb, int cb, int ce,
+                                                           double* __restrict__ A) {
+    constexpr int UB_M = 32 * WM, UA_LD = UB_M + 4, NT = 64 * WM;
     extern __shared__ __align__(16) double usm[];
     double* sA = usm;                       // [UB_K][UA_LD]: L21 rows of the tile, k-major
     double* sB = usm + UB_K * UA_LD;        // [UB_N][UBB_LD]: U12 columns of the tile, k contiguous
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int k1 = k0 + nb;
-    const int r0 = k1 + blockIdx.x * UB_M, c0 = k1 + blockIdx.y * UB_N;
+    const int r0 = k1 + blockIdx.x * UB_M, c0 = cb + blockIdx.y * UB_N;
     const int kpad = (nb + 3) & ~3;
     const int g = lane >> 2, t = lane & 3;
-    const int wr = (w & 3) * 32, wc = (w >> 2) * 32;  // the warp's 32 x 32 block in the tile
+    const int wr = (w % WM) * 32, wc = (w / WM) * 32;  // the warp's 32 x 32 block in the tile
     // the accumulators start as the thread's 32 entries of the A22 tile and take -L21 U12 (the staged
     // L21 is negated), so the tile is read once, with every load in flight together
     double acc[4][4][2];
@@ -47,36 +54,36 @@ __global__ void __launch_bounds__(256, 2) k_lu_update(int n, int k0, int nb, dou
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const double* col = tile + (size_t)(ni * 8 + h) * n;
-            const bool cok = gc0 + ni * 8 + h < n;
+            const bool cok = gc0 + ni * 8 + h < ce;
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi) acc[mi][ni][h] = (cok && gr0 + mi * 8 < n) ? col[mi * 8] : 0.0;
         }
     // staging, 8 independent loads of the thread before their stores
 #pragma unroll
-    for (int q = 0; q < UB_K * UB_M / 256; q += 8) {
+    for (int q = 0; q < UB_K * UB_M / NT; q += 8) {
         double v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const int e = tid + 256 * (q + u), k = e / UB_M, gr = r0 + (e - k * UB_M);
+            const int e = tid + NT * (q + u), k = e / UB_M, gr = r0 + (e - k * UB_M);
             v[u] = (k < nb && gr < n) ? -A[(size_t)(k0 + k) * n + gr] : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const int e = tid + 256 * (q + u), k = e / UB_M;
+            const int e = tid + NT * (q + u), k = e / UB_M;
             if (k < kpad) sA[k * UA_LD + (e - k * UB_M)] = v[u];
         }
     }
 #pragma unroll
-    for (int q = 0; q < UB_N * UB_K / 256; q += 8) {
+    for (int q = 0; q < UB_N * UB_K / NT; q += 8) {
         double v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const int e = tid + 256 * (q + u), cc = e / UB_K, k = e - cc * UB_K, gc = c0 + cc;
-            v[u] = (k < nb && gc < n) ? A[(size_t)gc * n + k0 + k] : 0.0;
+            const int e = tid + NT * (q + u), cc = e / UB_K, k = e - cc * UB_K, gc = c0 + cc;
+            v[u] = (k < nb && gc < ce) ? A[(size_t)gc * n + k0 + k] : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const int e = tid + 256 * (q + u), cc = e / UB_K;
+            const int e = tid + NT * (q + u), cc = e / UB_K;
             sB[cc * UBB_LD + (e - cc * UB_K)] = v[u];
         }
     }
@@ -97,7 +104,7 @@ __global__ void __launch_bounds__(256, 2) k_lu_update(int n, int k0, int nb, dou
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             double* col = tile + (size_t)(ni * 8 + h) * n;
-            if (gc0 + ni * 8 + h >= n) continue;
+            if (gc0 + ni * 8 + h >= ce) continue;
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi)
                 if (gr0 + mi * 8 < n) col[mi * 8] = acc[mi][ni][h];
@@ -106,19 +113,34 @@ __global__ void __launch_bounds__(256, 2) k_lu_update(int n, int k0, int nb, dou
 
 }  // namespace
 
-// A22 -= L21 U12 for the panel [k0, k0 + nb) of the column-major n x n matrix A (nb <= 64).
-int lu_update(Ctx& c, int n, int k0, int nb, double* A, cudaStream_t s) {
-    const int rest = n - k0 - nb;
-    if (rest <= 0) return BEM_OK;
-    if (nb > UB_K) return c.fail(BEM_ERR_ARG, "LU trailing update: panel wider than 64 columns");
+template <int WM>
+static bool upd_prepare() {
     static std::atomic<uint64_t> attr{0};
-    if (!once_per_device(attr, [] {
-            return cudaFuncSetAttribute(k_lu_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM) ==
-                   cudaSuccess;
-        }))
-        return c.fail(BEM_ERR_CUDA, "LU trailing update: shared-memory attribute refused");
-    const dim3 grid((rest + UB_M - 1) / UB_M, (rest + UB_N - 1) / UB_N);
-    KLAUNCH(), k_lu_update<<<grid, 256, UPD_SMEM, s>>>(n, k0, nb, A);
+    return once_per_device(attr, [] {
+        return cudaFuncSetAttribute(k_lu_update<WM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)upd_smem<WM>()) == cudaSuccess;
+    });
+}
+
+// A22 -= L21 U12 for the panel [k0, k0 + nb) of the column-major n x n matrix A (nb <= 64), on the
+// columns [cb, ce) of A22 (all of them by default).  narrow: 64-row tiles of 128 threads and 70 KB of
+// shared memory, so that a CTA of the cluster panel fits on the same SM (the look-ahead runs the next
+// panel beside this update); else 128-row tiles of 256 threads and 102 KB.
+int lu_update(Ctx& c, int n, int k0, int nb, double* A, cudaStream_t s, int cb, int ce, bool narrow) {
+    if (cb < 0) cb = k0 + nb;
+    if (ce < 0) ce = n;
+    const int rest = n - k0 - nb, cols = ce - cb;
+    if (rest <= 0 || cols <= 0) return BEM_OK;
+    if (nb > UB_K) return c.fail(BEM_ERR_ARG, "LU trailing update: panel wider than 64 columns");
+    if (narrow) {
+        if (!upd_prepare<2>()) return c.fail(BEM_ERR_CUDA, "LU trailing update: shared-memory attribute refused");
+        const dim3 grid((rest + 63) / 64, (cols + UB_N - 1) / UB_N);
+        KLAUNCH(), k_lu_update<2><<<grid, 128, upd_smem<2>(), s>>>(n, k0, nb, cb, ce, A);
+    } else {
+        if (!upd_prepare<4>()) return c.fail(BEM_ERR_CUDA, "LU trailing update: shared-memory attribute refused");
+        const dim3 grid((rest + 127) / 128, (cols + UB_N - 1) / UB_N);
+        KLAUNCH(), k_lu_update<4><<<grid, 256, upd_smem<4>(), s>>>(n, k0, nb, cb, ce, A);
+    }
     return BEM_OK;
 }
 
