@@ -287,10 +287,11 @@ typedef struct {
 int bem_get_stats(bem_ctx* ctx, bem_stats* s);
 
 /* Bound, in SM clock cycles, of every grid-wide barrier wait of the persistent kernels (the
- * cooperative BiCGSTAB and the row-distributed LU panel).  Default 2e9 (about a second at the
- * B200's clock).  A wait that runs out makes the kernel set its error word and return; the host
- * reads it, counts it in bem_stats.wait_expired and finishes the solve with the multi-kernel form,
- * which the context keeps for the rest of its life.  No counterpart in the reference (its solves
+ * cooperative BiCGSTAB, the cooperative refinement round, the row-distributed LU panel) and of the
+ * LU cluster panel's mbarrier waits.  Default 2e9 (about a second at the B200's clock).  A wait that
+ * runs out makes the kernel set its error word and return; the host reads it, counts it in
+ * bem_stats.wait_expired and finishes the solve with the multi-kernel form (for the LU: the
+ * single-CTA panel), which the context keeps for the rest of its life.  No counterpart in the reference (its solves
  * run on the host); exists so that this failure path can be tested without a GPU fault.
  * cycles <= 0 returns BEM_ERR_ARG. */
 int bem_set_wait_limit(bem_ctx* ctx, int64_t cycles);
